@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the implicit Newton-Raphson time step for growing prism tissue on B200.
+
+Workload (default): the wing-disc-like disc - Delaunay disc of radius 100 um, 2 um ECM layer
+(E=4000 Pa) under a 25 um columnar layer (E=1000 Pa), ~80k prisms, radial Gaussian growth,
+rim clamped, dt = 60 s. One step = one full implicit time step (growth prologue, viscosity
+surfaces, Newton iterations each with assembly + BiCGStab solve) on synthetic seeded input.
+
+Metric: prism assemblies/s = prisms x Newton assemblies / device time (FP64). Newton
+iterations/s are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+
+Under torchrun (N > 1) every rank runs an independent replica of the tissue (the single-tissue
+path does not shard); rank 0 prints one JSON line with the whole-job aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "prism assemblies/s (FP64 implicit Newton step)"
+UNIT = "prisms*assemblies/s"
+
+
+def make_tissue(name: str):
+    from tissueorigami_b200 import mesh
+
+    if name == "wing_disc":
+        return mesh.wing_disc()
+    if name == "small_rectangle":
+        return mesh.small_rectangle()
+    if name == "large_slab":
+        return mesh.large_slab()
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_desc(t) -> dict:
+    return {"workload": f"{t.name}: {t.n_elems} prisms, {t.n_nodes} nodes, dt={t.dt:g}s, "
+                        f"Newton tol {t.newton_tol:g}", "prisms": t.n_elems, "nodes": t.n_nodes,
+            "dt_s": t.dt, "seed": t.seed}
+
+
+# ----------------------------------------------------------------------------------------
+# CPU baseline: the oracle's line-by-line restatement of the reference element loop
+# ----------------------------------------------------------------------------------------
+
+def cpu_assembly_rate(t, seconds: float = 12.0):
+    """Faithful element forces + tangents (the reference's naive D81 loop, OpenMP over
+    elements with every host thread) on a bounded sample of the workload's prisms."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    sub = t.copy()
+    n_cal = min(t.n_elems, 200 * threads)
+    sub.conn = t.conn[:n_cal]
+    sub.xref = t.xref[:n_cal]
+    sub.lam, sub.mu, sub.eta = t.lam[:n_cal], t.mu[:n_cal], t.eta[:n_cal]
+    t0 = time.perf_counter()
+    O.element_forces_and_tangents(sub, t.x, threads=threads)
+    rate0 = n_cal / (time.perf_counter() - t0)
+    n = int(min(t.n_elems, max(n_cal, rate0 * seconds)))
+    sub.conn, sub.xref = t.conn[:n], t.xref[:n]
+    sub.lam, sub.mu, sub.eta = t.lam[:n], t.mu[:n], t.eta[:n]
+    t0 = time.perf_counter()
+    O.element_forces_and_tangents(sub, t.x, threads=threads)
+    el = time.perf_counter() - t0
+    return n / el, threads, n, el
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    t = make_tissue(args.workload)
+    for _ in range(args.warmup):
+        cpu_assembly_rate(t, seconds=1.0)
+    rates, samples, secs = [], [], 0.0
+    threads = os.cpu_count() or 1
+    for _ in range(args.steps):
+        r, threads, n, el = cpu_assembly_rate(t, seconds=args.cpu_seconds)
+        rates.append(r)
+        samples.append(n)
+        secs += el
+    total_units = sum(samples)
+    value = total_units / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": workload_desc(t),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"faithful element forces + 18x18 tangents of the first {samples[0]} "
+                                   f"of {t.n_elems} prisms per step (assembly only: the CPU path's "
+                                   "direct solve is not included, which favours the CPU)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.bus_id = bus_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.bus_id:
+                cmd += ["-i", self.bus_id]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in out.splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 10:
+                continue
+            try:
+                sm.append(float(f[2]))
+                smax.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[6:10]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        mx = max(smax)
+        loaded = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------
+# B200 arm
+# ----------------------------------------------------------------------------------------
+
+def run_b200(args) -> None:
+    import ctypes
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from tissueorigami_b200 import capi
+    from tissueorigami_b200.newton import NewtonRaphsonSolver
+
+    L = capi.load()
+    t = make_tissue(args.workload)
+    s = NewtonRaphsonSolver.from_tissue(t, device=local)
+    sched = s.autotune(t.x, t.dt)
+    n3 = 3 * t.n_nodes
+    x_dev = torch.from_numpy(np.ascontiguousarray(t.x.reshape(-1))).to(f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    def dev_step():
+        st = capi.StepStats()
+        rc = L.tf_time_step_device(s._h, ctypes.c_void_p(x_dev.data_ptr()), float(t.dt),
+                                   ctypes.c_void_p(x_dev.data_ptr()), ctypes.byref(st))
+        capi.check(rc, "tf_time_step_device", s._h)
+        return rc, st
+
+    for _ in range(args.warmup):
+        dev_step()
+
+    bus = None
+    try:
+        bus = torch.cuda.get_device_properties(local).pci_bus_id
+    except Exception:
+        bus = None
+    clocks = ClockSampler(bus)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, iters, kry, launches, worst = 0.0, 0, 0, 0, 0
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the step's event window)
+        torch.cuda.synchronize()
+        rc, st = dev_step()
+        ms += st.ms_total
+        iters += st.newton_iters
+        kry += st.krylov_iters_total
+        launches += st.gpu_launches
+        worst = max(worst, rc)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+
+    # end to end through the public host-pointer call, pinned host buffers
+    x_host = torch.from_numpy(x_dev.cpu().numpy().copy()).pin_memory()
+    x_out = torch.empty_like(x_host).pin_memory()
+    e2e_ms, e2e_iters = 0.0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        st = capi.StepStats()
+        rc = L.tf_time_step(s._h, ctypes.cast(x_host.data_ptr(), ctypes.POINTER(ctypes.c_double)), float(t.dt),
+                            ctypes.cast(x_out.data_ptr(), ctypes.POINTER(ctypes.c_double)), ctypes.byref(st))
+        capi.check(rc, "tf_time_step", s._h)
+        x_host.copy_(x_out)
+        e2e_ms += st.ms_total
+        e2e_iters += st.newton_iters
+
+    # kernel timings for the roofline
+    ms_el, ms_spmv = s.time_kernels(20)
+    nnzb = int(s.pattern()[1].shape[0])
+    E, N = t.n_elems, t.n_nodes
+    bytes_asm = 408.0 * E + 97.0 * N + 72.0 * nnzb        # per assembly (element record, nodes, J written once)
+    bytes_spmv = 76.0 * nnzb + 4.0 * (N + 1) + 48.0 * N    # per SpMV (J + colidx read once, x read, y written)
+    share_el = ms_el * iters
+    share_spmv = ms_spmv * 2 * kry
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = load_traffic()
+
+    def roof(name, b, t_ms):
+        ach = b / (t_ms * 1e-3) / 1e9
+        return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "peak_source": peak_src, "algorithmic_bytes": b, "ms_per_launch": t_ms,
+                "traffic": traffic.get((name, t.name))}
+
+    r_el = roof("element_assemble", bytes_asm, ms_el)
+    r_sp = roof("bsr3_spmv", bytes_spmv, ms_spmv)
+    dominant, other = (r_sp, r_el) if share_spmv >= share_el else (r_el, r_sp)
+
+    units = float(E) * iters
+    t_dev = ms / 1000.0
+    e2e_units = float(E) * e2e_iters
+    t_e2e = e2e_ms / 1000.0
+    if dist:
+        buf = torch.tensor([units, e2e_units, float(iters), float(kry), float(launches)], dtype=torch.float64, device=f"cuda:{local}")
+        tm = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        units, e2e_units, iters_all, kry_all, launches_all = buf.tolist()
+        t_dev, t_e2e = tm.tolist()
+    else:
+        iters_all, kry_all, launches_all = iters, kry, launches
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        r, threads, n, el = cpu_assembly_rate(t, seconds=args.cpu_seconds)
+        cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"faithful element forces + tangents of {n} of {t.n_elems} prisms "
+                         f"({el:.1f} s on {threads} threads; assembly only)"}
+    if rank == 0:
+        value = units / t_dev
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mesh and growth map)",
+            "config": dict(workload_desc(t), l2="flushed (256 MB write) between timed steps",
+                           parallelism=f"{world} independent replica(s), no collective on the data path",
+                           schedule=sched),
+            "newton_iters_per_s": iters_all / t_dev,
+            "newton_iters_per_step": iters_all / (args.steps * world),
+            "krylov_iters_per_newton": kry_all / max(iters_all, 1),
+            "e2e": {"value": e2e_units / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n3,
+                    "d2h_bytes_per_step": 8 * n3},
+            "gpu_launches": int(launches_all),
+            "roofline": dominant, "roofline_other": other,
+            "cpu_baseline": cpu, "clocks": clk, "status_worst": worst,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def load_traffic():
+    """Per-launch DRAM bytes from committed ncu summaries (profiles/traffic.tsv:
+    kernel<TAB>workload<TAB>bytes_per_launch); missing entries read as null."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "traffic.tsv")
+    if os.path.exists(p):
+        for ln in open(p):
+            f = ln.strip().split("\t")
+            if len(f) >= 3 and not ln.startswith("#"):
+                try:
+                    out[(f[0], f[1])] = float(f[2])
+                except ValueError:
+                    pass
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", default="wing_disc")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

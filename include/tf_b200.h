@@ -1,0 +1,199 @@
+/*
+ * tf_b200.h -- C ABI of the B200 implicit Newton-Raphson step for growing prism tissue.
+ *
+ * This is the drop-in boundary for TissueOrigami's Newton path
+ * (TissueFolding/SourceCode: Simulation::updateStepNR -> NewtonRaphsonSolver ->
+ * ShapeBase / Prism). Every entry point takes plain host pointers and sizes; no CUDA or
+ * torch type appears in a signature. Each declaration names the reference interface it
+ * replaces.
+ *
+ * Conventions
+ *   - node DoF index is 3*node + dim, exactly the layout of NewtonRaphsonSolver::un / uk
+ *     (NewtonRaphsonSolver.cpp:106-112).
+ *   - prism node order is the reference's: 0-2 basal triangle, 3-5 apical triangle.
+ *   - the Jacobian exposed by tf_assemble / tf_solve is the TRUE Newton Jacobian
+ *     J = dR/du, which is the transpose of the reference's dense storage K: the reference
+ *     writes the viscous tangent transposed (ShapeBase.cpp:3154-3160, 3193-3199) and asks
+ *     Pardiso for a transposed solve (iparm[11] = 1, NewtonRaphsonSolver.cpp:716-723).
+ *   - return value: 0 ok; > 0 numerical outcome the caller may continue from (the
+ *     reference logs non-convergence and continues, Simulation.cpp:6724-6727); < 0 error.
+ *     No entry point calls exit() or traps the GPU.
+ *   - a context is used from one host thread at a time; its work runs on one CUDA stream.
+ */
+#ifndef TF_B200_H
+#define TF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------------- */
+#define TF_OK 0
+#define TF_NEWTON_NOT_CONVERGED 1 /* hit the Newton cap; positions still updated          */
+#define TF_KRYLOV_MAX_ITERS 2     /* a linear solve stopped at its iteration cap           */
+#define TF_KRYLOV_BREAKDOWN 3     /* BiCGStab breakdown (rho or omega became zero)         */
+#define TF_NONFINITE 4            /* NaN / Inf met in the residual or the update           */
+#define TF_ELEMENT_INVERTED 5     /* det(Fe) <= 0 at some Gauss point                      */
+#define TF_ERR_ARGUMENT (-1)
+#define TF_ERR_CUDA (-2)
+#define TF_ERR_OUT_OF_MEMORY (-3)
+#define TF_ERR_STATE (-4)
+#define TF_ERR_UNSUPPORTED (-5)
+
+/* ---- options ------------------------------------------------------------------------- */
+#define TF_PRECOND_BLOCK_JACOBI 0 /* 3x3 node-block inverse of the diagonal               */
+#define TF_PRECOND_ILU0 1         /* ILU(0) on the BSR3 pattern, multicolour ordered      */
+
+#define TF_SCATTER_AUTO 0     /* pick by the autotuner's cached choice                   */
+#define TF_SCATTER_ATOMIC 1   /* FP64 atomics into the fixed BSR3 pattern                */
+#define TF_SCATTER_COLOURED 2 /* greedy element colouring, plain read-modify-write       */
+
+typedef struct tf_ctx tf_ctx;
+
+/* Mesh handed over once per tissue: the reference's Nodes/Elements after
+ * Simulation::initiateMesh (Simulation.cpp:2969-3014). */
+typedef struct tf_mesh_desc {
+    int32_t n_nodes;
+    int32_t n_elems;
+    const int32_t* conn; /* [n_elems*6]  ShapeBase::NodeIds                                  */
+    const double* xref;  /* [n_elems*18] ReferenceShape->Positions (ReferenceShapeBase.h:21) */
+} tf_mesh_desc;
+
+typedef struct tf_params {
+    int32_t max_newton_iters; /* Simulation.cpp:6615 maxIteration (20)                      */
+    double newton_tol;        /* NewtonRaphsonSolver.cpp:22 threshold on ||du||_2 (1e-8)     */
+    int32_t krylov_max_iters; /* BiCGStab iteration cap per linear solve                    */
+    double krylov_rtol;       /* stop when ||r||_2 <= krylov_rtol * ||g||_2                 */
+    int32_t precond;          /* TF_PRECOND_*                                               */
+    int32_t scatter;          /* TF_SCATTER_*                                               */
+    int32_t elems_per_block;  /* element-kernel teams per CTA: 0 = autotuned                */
+    int32_t device;           /* CUDA device ordinal                                        */
+    int32_t use_graphs;       /* capture the Krylov iteration in a CUDA graph (1) or not    */
+} tf_params;
+
+typedef struct tf_step_stats {
+    int32_t newton_iters;       /* iterations run (reference: iteratorK after the loop)     */
+    int32_t krylov_iters_total; /* BiCGStab iterations summed over the step                 */
+    int32_t krylov_iters_max;   /* largest single solve                                     */
+    int32_t status;             /* worst status seen in the step                            */
+    double du_norm[32];         /* ||du||_2 per Newton iteration (first 32)                 */
+    double krylov_rel_res[32];  /* final relative residual of each linear solve             */
+    double ms_assemble;         /* device time in assembly (element + node kernels)         */
+    double ms_solve;            /* device time in the linear solves                         */
+    double ms_total;            /* device time of the whole call, host copies included      */
+    int64_t gpu_launches;       /* kernels this call launched (graph nodes counted)         */
+} tf_step_stats;
+
+/* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), BiCGStab
+ * rtol 1e-12 with cap 20000, block-Jacobi, autotuned scatter, device 0, graphs on. */
+void tf_default_params(tf_params* p);
+
+/* Library version string. */
+const char* tf_version(void);
+
+/* Replaces NewtonRaphsonSolver::NewtonRaphsonSolver (NewtonRaphsonSolver.cpp:16-41) and the
+ * per-element Prism::calculateElementShapeFunctionDerivatives (Prism.cpp:698-733): builds the
+ * fixed BSR3 pattern, the element-to-block slot map and the element colouring on the host,
+ * and allocates every device buffer of the tissue. */
+int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out);
+
+/* Replaces NewtonRaphsonSolver::~NewtonRaphsonSolver (NewtonRaphsonSolver.cpp:43-71). */
+void tf_destroy(tf_ctx* ctx);
+
+/* Replaces Prism::setElasticProperties / updateElasticProperties (Prism.cpp:464-534) and
+ * ShapeBase::internalViscosity: per-element lambda, mu, eta. */
+int tf_set_material(tf_ctx* ctx, const double* lambda, const double* mu, const double* eta);
+
+/* Replaces ShapeBase::InvFg as growShapeByFg leaves it (ShapeBase.cpp:1452-1506):
+ * per-element inverse growth deformation gradient, [n_elems*9] row-major. */
+int tf_set_inv_fg(tf_ctx* ctx, const double* inv_fg);
+
+/* Replaces Node::FixedPos (Node.h), Node::externalViscosity (Node.cpp:63-110) and
+ * NewtonRaphsonSolver::slaveMasterList (NewtonRaphsonSolver.h:49). fixed [n_nodes*3];
+ * ext_visc [n_nodes*3]; slave_master [n_pairs*2] (slave DoF, master DoF). A master must not
+ * itself be a slave (the reference enforces this in checkMasterUpdate). */
+int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
+                    const int32_t* slave_master, int32_t n_pairs);
+
+/* Replaces Node::viscositySurface as Simulation::updateNodeViscositySurfaces leaves it
+ * (Simulation.cpp:7598-7620): per-node exposed area, [n_nodes]. */
+int tf_set_viscosity_surface(tf_ctx* ctx, const double* visc_surface);
+
+/* Replaces Simulation::updateStepNR (Simulation.cpp:6605-6747) with the surface-based
+ * external viscosity of NewtonRaphsonSolver (externalViscosityVolumeBased = false) and no
+ * packing or lumen terms: x_n [n_nodes*3] host positions at the end of the previous step,
+ * x_out [n_nodes*3] host positions after the step (may alias x_n). stats may be NULL. */
+int tf_newton_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out,
+                   tf_step_stats* stats);
+
+/* tf_newton_step on device-resident buffers (cudaMalloc'd by the caller, same layout), for
+ * callers that keep positions on the GPU between steps. Stream-ordered on the context's
+ * stream; returns after the step completed. */
+int tf_newton_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x_out,
+                          tf_step_stats* stats);
+
+/* Number of 3x3 blocks of the Jacobian pattern, and the pattern itself (rowptr [n_nodes+1],
+ * colidx [nnzb], each may be NULL to query only). */
+int tf_get_pattern(tf_ctx* ctx, int32_t* nnzb, int32_t* rowptr, int32_t* colidx);
+
+/* Parity hook for one Newton iteration's system. Replaces the sequence
+ * calculateDisplacementMatrix, calculateForcesAndJacobianMatrixNR,
+ * writeForcesTogeAndgvInternal, writeImplicitElementalKToJacobian,
+ * calculateExternalViscousForcesForNR, addImplicitKViscousExternalToJacobian,
+ * calculateSumOfInternalForces, calcutateFixedK, calculateBoundKWithSlavesMasterDoF
+ * (NewtonRaphsonSolver.cpp:95-457). uk, un [n_nodes*3]; g_out [n_nodes*3] is gSum;
+ * bsr_vals_out [nnzb*9] (may be NULL) holds J = K^T block-row-major. */
+int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, double* g_out,
+                double* bsr_vals_out);
+
+/* Replaces NewtonRaphsonSolver::solveForDeltaU / solveWithPardiso
+ * (NewtonRaphsonSolver.cpp:461-763) including equateSlaveDisplacementsToMasters: solves
+ * J du = g with preconditioned BiCGStab on the context's pattern. bsr_vals [nnzb*9],
+ * g and du [n_nodes*3]. iters / rel_res may be NULL. */
+int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, int32_t* iters,
+             double* rel_res);
+
+/* Growth state for the per-step prologue on the device: fg [n_elems*9] (ShapeBase::Fg),
+ * rates [n_elems*3] growth rates in 1/s and angles [n_elems] in radians with the uniform
+ * growth function's semantics (GrowthFunctionTypes.h:14-99, ShapeBase.cpp:471-505),
+ * exposed [n_elems] bit0 apical / bit1 basal exposed surface and peripodial [n_elems]
+ * (Prism.cpp:1650-1709). Any pointer may be NULL to keep the current value. */
+int tf_set_growth(tf_ctx* ctx, const double* fg, const double* rates, const double* angles,
+                  const uint8_t* exposed, const uint8_t* peripodial);
+
+/* Read back the device growth state: fg and inv_fg [n_elems*9] (either may be NULL). */
+int tf_get_growth(tf_ctx* ctx, double* fg, double* inv_fg);
+
+/* One full time step of the path, replacing the part of Simulation::runOneStep that feeds
+ * and runs the Newton step (Simulation.cpp:6008-6112): CalculateGrowthRotationByF,
+ * calculateGrowth (uniform-type rates), growShapeByFg, updateNodeViscositySurfaces, then
+ * updateStepNR. Host positions in and out. */
+int tf_time_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out,
+                 tf_step_stats* stats);
+
+/* tf_time_step on device-resident positions. */
+int tf_time_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x_out,
+                        tf_step_stats* stats);
+
+/* Number of element colours and the chosen scatter / teams-per-CTA after autotuning. */
+int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* elems_per_block);
+
+/* Time the assembly variants on the context's current state and keep the fastest
+ * (scatter mode x teams per CTA). Returns the chosen pair through tf_get_schedule. */
+int tf_autotune(tf_ctx* ctx, const double* x_n, double dt);
+
+/* Benchmark hook (no reference counterpart): mean device time in ms over `reps` launches of
+ * the element-assembly kernels of the current schedule, on the positions of the last call, and
+ * of one BSR3 SpMV, each bracketed by CUDA events on the context's stream. Overwrites the
+ * context's Jacobian buffers. */
+int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_spmv);
+
+/* Text of the last error recorded on the context (no reference counterpart). */
+const char* tf_last_error(tf_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,249 @@
+"""ctypes wrapper of the CPU oracle (``oracle/_build/libtf_oracle.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of bench.py. The product never imports this module.
+The oracle restates TissueOrigami's Newton-Raphson path in plain C++ (see tf_oracle.cpp for the
+reference file:line of every function).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libtf_oracle.so")
+_lib = None
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int32)
+_U = ctypes.POINTER(ctypes.c_uint8)
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++ -O3 -fopenmp)."""
+    if force or not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        c_int, c_double = ctypes.c_int, ctypes.c_double
+        L.tfo_shape_derivatives.argtypes = [c_int, _D, _D, _D]
+        L.tfo_element_forces_and_tangents.argtypes = [c_int, _I, _D, _D, _D, _D, _D, _D, _D, c_double, _U, _D, _D, _D, _D, _D, c_int]
+        L.tfo_element_forces_and_tangents.restype = c_int
+        L.tfo_assemble_dense.argtypes = [c_int, c_int, _I, _D, _D, _D, _D, _D, _D, _D, c_double, _U, _D, _D, _I, c_int, _D, _D, c_int]
+        L.tfo_assemble_dense.restype = c_int
+        L.tfo_solve_transposed.argtypes = [c_int, _D, _D, _I, c_int, c_int, _D]
+        L.tfo_solve_transposed.restype = c_int
+        L.tfo_newton_step_dense.argtypes = [c_int, c_int, _I, _D, _D, _D, _D, _D, _D, c_double, c_double, c_int, _U, _D, _D, _I, c_int, _D, _D, c_int]
+        L.tfo_newton_step_dense.restype = c_int
+        L.tfo_block_pattern.argtypes = [c_int, c_int, _I, _I, _I]
+        L.tfo_block_pattern.restype = c_int
+        L.tfo_assemble_bsr.argtypes = [c_int, c_int, _I, _D, _D, _D, _D, _D, _D, _D, c_double, _U, _D, _D, _I, _I, _D, _D, c_int]
+        L.tfo_assemble_bsr.restype = c_int
+        L.tfo_grow.argtypes = [c_int, _I, _D, _D, _D, _D, c_double, _D, _D, _D, _I]
+        L.tfo_viscosity_surfaces.argtypes = [c_int, c_int, _I, _D, _U, _U, _D]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def _i(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_I)
+
+
+def _u(a):
+    if a is None:
+        return None
+    assert a.dtype == np.uint8 and a.flags.c_contiguous
+    return a.ctypes.data_as(_U)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def shape_derivatives(xref):
+    xref = _c(xref, np.float64).reshape(-1, 18)
+    E = xref.shape[0]
+    inv = np.zeros((E, 6, 9))
+    det = np.zeros((E, 6))
+    lib().tfo_shape_derivatives(E, _d(xref), _d(inv), _d(det))
+    return inv, det
+
+
+def element_forces_and_tangents(t, x, v=None, dt=None, inv_fg=None, threads=0, strain=False):
+    """Per-element (f_elastic[E,18], f_viscous[E,18], Ke[E,18,18], Kv[E,18,18]) at positions x
+    and nodal velocity v = (uk-un)/dt, in the reference's storage."""
+    E = t.n_elems
+    conn = _c(t.conn, np.int32)
+    xref = _c(t.xref, np.float64)
+    inv_fg = _c(inv_fg if inv_fg is not None else np.linalg.inv(t.fg.reshape(-1, 3, 3)).reshape(-1, 9), np.float64)
+    x = _c(x, np.float64)
+    v = _c(v if v is not None else np.zeros_like(x), np.float64)
+    fe = np.zeros((E, 18)); fv = np.zeros((E, 18))
+    ke = np.zeros((E, 18, 18)); kv = np.zeros((E, 18, 18))
+    st = np.zeros((E, 6, 6)) if strain else None
+    bad = lib().tfo_element_forces_and_tangents(E, _i(conn), _d(xref), _d(inv_fg), _d(_c(t.lam, np.float64)),
+                                                _d(_c(t.mu, np.float64)), _d(_c(t.eta, np.float64)), _d(x), _d(v),
+                                                float(dt if dt is not None else t.dt), _u(_c(t.fixed, np.uint8)),
+                                                _d(fe), _d(fv), _d(ke), _d(kv), _d(st), int(threads))
+    return fe, fv, ke, kv, st, bad
+
+
+def assemble_dense(t, uk, un, visc_surface, inv_fg, dt=None, threads=0):
+    """Dense reference-storage K[3N,3N] and gSum[3N] after fixed-DoF and slave-master steps."""
+    n = 3 * t.n_nodes
+    K = np.zeros((n, n)); g = np.zeros(n)
+    sm = _c(t.slave_master.reshape(-1), np.int32)
+    lib().tfo_assemble_dense(t.n_nodes, t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(t.xref, np.float64)),
+                             _d(_c(inv_fg, np.float64)), _d(_c(t.lam, np.float64)), _d(_c(t.mu, np.float64)),
+                             _d(_c(t.eta, np.float64)), _d(_c(uk, np.float64)), _d(_c(un, np.float64)),
+                             float(dt if dt is not None else t.dt), _u(_c(t.fixed, np.uint8)),
+                             _d(_c(visc_surface, np.float64)), _d(_c(t.ext_visc, np.float64)),
+                             _i(sm) if sm.size else None, int(t.slave_master.shape[0]), _d(K), _d(g), int(threads))
+    return K, g
+
+
+def solve_transposed(K, g, slave_master=None, n_refine=1):
+    n = g.shape[0]
+    du = np.zeros(n)
+    sm = _c(slave_master.reshape(-1), np.int32) if slave_master is not None and slave_master.size else None
+    st = lib().tfo_solve_transposed(n, _d(_c(K, np.float64)), _d(_c(g, np.float64)), _i(sm),
+                                    0 if sm is None else sm.size // 2, int(n_refine), _d(du))
+    return du, st
+
+
+def newton_step_dense(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0):
+    n = 3 * t.n_nodes
+    x_out = np.zeros((t.n_nodes, 3))
+    norms = np.zeros(max_iter + 2)
+    sm = _c(t.slave_master.reshape(-1), np.int32)
+    it = lib().tfo_newton_step_dense(t.n_nodes, t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(t.xref, np.float64)),
+                                     _d(_c(inv_fg, np.float64)), _d(_c(t.lam, np.float64)), _d(_c(t.mu, np.float64)),
+                                     _d(_c(t.eta, np.float64)), _d(_c(x_n, np.float64)),
+                                     float(dt if dt is not None else t.dt), float(tol if tol is not None else t.newton_tol),
+                                     int(max_iter), _u(_c(t.fixed, np.uint8)), _d(_c(visc_surface, np.float64)),
+                                     _d(_c(t.ext_visc, np.float64)), _i(sm) if sm.size else None,
+                                     int(t.slave_master.shape[0]), _d(x_out), _d(norms), int(threads))
+    del n
+    return x_out, it, norms[:it]
+
+
+def block_pattern(t):
+    conn = _c(t.conn, np.int32)
+    nnzb = lib().tfo_block_pattern(t.n_nodes, t.n_elems, _i(conn), None, None)
+    rowptr = np.zeros(t.n_nodes + 1, np.int32)
+    colidx = np.zeros(nnzb, np.int32)
+    lib().tfo_block_pattern(t.n_nodes, t.n_elems, _i(conn), _i(rowptr), _i(colidx))
+    return rowptr, colidx
+
+
+def assemble_bsr(t, uk, un, visc_surface, inv_fg, rowptr, colidx, dt=None, threads=0):
+    """True Jacobian J = K^T in BSR3 over (rowptr, colidx) and g, without slave-master pairs."""
+    vals = np.zeros((colidx.shape[0], 3, 3))
+    g = np.zeros(3 * t.n_nodes)
+    lib().tfo_assemble_bsr(t.n_nodes, t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(t.xref, np.float64)),
+                           _d(_c(inv_fg, np.float64)), _d(_c(t.lam, np.float64)), _d(_c(t.mu, np.float64)),
+                           _d(_c(t.eta, np.float64)), _d(_c(uk, np.float64)), _d(_c(un, np.float64)),
+                           float(dt if dt is not None else t.dt), _u(_c(t.fixed, np.uint8)),
+                           _d(_c(visc_surface, np.float64)), _d(_c(t.ext_visc, np.float64)),
+                           _i(rowptr), _i(colidx), _d(vals), _d(g), int(threads))
+    return vals, g
+
+
+def grow(t, x, fg, dt=None):
+    """One step of the growth prologue. Returns (fg_new[E,9], inv_fg[E,9], det_fg[E], rotated[E])."""
+    fg = np.array(fg, dtype=np.float64, copy=True).reshape(-1, 9)
+    inv = np.zeros_like(fg)
+    det = np.zeros(t.n_elems)
+    rot = np.zeros(t.n_elems, np.int32)
+    lib().tfo_grow(t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(t.xref, np.float64)), _d(_c(x, np.float64)),
+                   _d(_c(t.rates, np.float64)), _d(_c(t.angles, np.float64)), float(dt if dt is not None else t.dt),
+                   _d(fg), _d(inv), _d(det), _i(rot))
+    return fg, inv, det, rot
+
+
+def viscosity_surfaces(t, x):
+    vs = np.zeros(t.n_nodes)
+    lib().tfo_viscosity_surfaces(t.n_nodes, t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(x, np.float64)),
+                                 _u(_c(t.exposed, np.uint8)), _u(_c(t.peripodial, np.uint8)), _d(vs))
+    return vs
+
+
+def bsr_to_scipy(rowptr, colidx, vals, n_nodes):
+    import scipy.sparse as sp
+
+    return sp.bsr_matrix((np.asarray(vals).reshape(-1, 3, 3), colidx, rowptr), shape=(3 * n_nodes, 3 * n_nodes)).tocsr()
+
+
+def simulate_dense(t, n_steps=None, max_iter=20, tol=None, threads=0):
+    """Run n time steps of the reference path on the CPU with dense assembly and the LU
+    stand-in for Pardiso: growth prologue, viscosity surfaces, Newton step.
+    Returns (x, fg, per-step iteration counts, per-step norm traces)."""
+    x = np.array(t.x, dtype=np.float64, copy=True)
+    fg = np.array(t.fg, dtype=np.float64, copy=True)
+    iters, traces = [], []
+    for _ in range(n_steps if n_steps is not None else t.n_steps):
+        fg, inv, _, _ = grow(t, x, fg)
+        vs = viscosity_surfaces(t, x)
+        x, it, norms = newton_step_dense(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads)
+        iters.append(it)
+        traces.append(norms)
+    return x, fg, iters, traces
+
+
+def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0):
+    """Simulation::updateStepNR with sparse assembly of J = K^T and SuperLU (scipy) as the
+    direct solve standing in for Pardiso. No slave-master pairs. Returns (x, iterations, norms)."""
+    import scipy.sparse.linalg as sla
+
+    rowptr, colidx = block_pattern(t)
+    un = np.array(x_n, dtype=np.float64, copy=True).reshape(-1, 3)
+    uk = un.copy()
+    norms = []
+    it = 0
+    converged = False
+    tol = float(tol if tol is not None else t.newton_tol)
+    while not converged:
+        vals, g = assemble_bsr(t, uk, un, visc_surface, inv_fg, rowptr, colidx, dt=dt, threads=threads)
+        J = bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
+        du = sla.spsolve(J, g)
+        d = float(np.sqrt(np.sum(du * du)))
+        norms.append(d)
+        converged = not (d > tol)
+        uk = uk + du.reshape(-1, 3)
+        it += 1
+        if not converged and it > max_iter:
+            converged = True
+    return uk, it, np.array(norms)
+
+
+def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0):
+    """n time steps with the growth prologue and the sparse Newton step."""
+    x = np.array(t.x, dtype=np.float64, copy=True)
+    fg = np.array(t.fg, dtype=np.float64, copy=True)
+    iters, traces = [], []
+    for _ in range(n_steps if n_steps is not None else t.n_steps):
+        fg, inv, _, _ = grow(t, x, fg)
+        vs = viscosity_surfaces(t, x)
+        x, it, norms = newton_step_sparse(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads)
+        iters.append(it)
+        traces.append(norms)
+    return x, fg, iters, traces

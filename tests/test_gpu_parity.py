@@ -1,0 +1,190 @@
+"""GPU parity of the CUDA path against the oracle, through the C ABI.
+
+Tolerances (written per test):
+  * element forces / residual g and Jacobian entries: 1e-12 relative to the largest entry;
+  * one linear solve (BiCGStab, rtol 1e-13) against the direct solve of the same system:
+    1e-8 relative in ||du|| (the systems have condition numbers ~1e5);
+  * node positions after N implicit steps: 1e-9 of the tissue size (bounding-box diagonal).
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as sla
+
+from oracle import oracle as O
+from tissueorigami_b200 import capi, mesh
+from tissueorigami_b200.newton import NewtonRaphsonSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _state(t, seed=0, amp=0.05, eta=0.0):
+    rng = np.random.default_rng(seed)
+    t = t.copy()
+    t.eta[:] = eta
+    un = t.x.copy()
+    uk = un + rng.normal(0, amp, un.shape)
+    fg = np.tile(np.diag([1.02, 1.01, 0.99]).reshape(1, 9), (t.n_elems, 1))
+    inv = np.linalg.inv(fg.reshape(-1, 3, 3)).reshape(-1, 9)
+    return t, uk, un, inv
+
+
+def _gpu_system(t, uk, un, inv, vs, **kw):
+    with NewtonRaphsonSolver.from_tissue(t, **kw) as s:
+        s.set_inv_fg(inv)
+        s.set_viscosity_surface(vs)
+        g, vals, rowptr, colidx, rc = s.assemble(uk, un, t.dt)
+    return g, O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes), rc
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("eta", [0.0, 4.0])
+@pytest.mark.parametrize("scatter,teams", [(capi.TF_SCATTER_ATOMIC, 16), (capi.TF_SCATTER_COLOURED, 8),
+                                           (capi.TF_SCATTER_ATOMIC, 32), (capi.TF_SCATTER_COLOURED, 32)])
+def test_assembly_matches_oracle(eta, scatter, teams):
+    t, uk, un, inv = _state(mesh.small_rectangle(nx=9, ny=6), eta=eta)
+    vs = O.viscosity_surfaces(t, uk)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g_ref = O.assemble_bsr(t, uk, un, vs, inv, rowptr, colidx)
+    J_ref = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).toarray()
+    g, J, rc = _gpu_system(t, uk, un, inv, vs, scatter=scatter, elems_per_block=teams)
+    assert rc == capi.TF_OK
+    assert _rel(J.toarray(), J_ref) < 1e-12
+    assert _rel(g, g_ref) < 1e-12
+
+
+def test_assembly_disc_matches_oracle():
+    t, uk, un, inv = _state(mesh.wing_disc(n_surface_points=800), amp=0.02)
+    vs = O.viscosity_surfaces(t, uk)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g_ref = O.assemble_bsr(t, uk, un, vs, inv, rowptr, colidx)
+    J_ref = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes)
+    g, J, rc = _gpu_system(t, uk, un, inv, vs)
+    assert rc == capi.TF_OK
+    assert abs(J - J_ref).max() / abs(J_ref).max() < 1e-12
+    assert _rel(g, g_ref) < 1e-12
+
+
+def test_slave_master_assembly_matches_dense_oracle():
+    """calculateBoundKWithSlavesMasterDoF on the fixed pattern: routed scatter == N^T K N + I."""
+    t, uk, un, inv = _state(mesh.small_rectangle(nx=6, ny=4), eta=2.0)
+    # bind x,y of two apical nodes to other apical nodes (both directions untouched by fixing)
+    t.slave_master = np.array([[3 * 9 + 0, 3 * 3 + 0], [3 * 9 + 1, 3 * 3 + 1], [3 * 21 + 0, 3 * 15 + 0]], np.int32)
+    vs = O.viscosity_surfaces(t, uk)
+    K, g_ref = O.assemble_dense(t, uk, un, vs, inv)
+    g, J, rc = _gpu_system(t, uk, un, inv, vs)
+    assert rc == capi.TF_OK
+    assert _rel(J.toarray(), K.T) < 1e-12
+    assert _rel(g, g_ref) < 1e-12
+
+
+def test_solve_matches_direct():
+    t = mesh.small_disc(7, 1500, 1200.0)
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
+    J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
+    du_ref = sla.spsolve(J, g)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13) as s:
+        rp, ci = s.pattern()
+        np.testing.assert_array_equal(rp, rowptr)
+        np.testing.assert_array_equal(ci, colidx)
+        du, rc, iters, rr = s.solveForDeltaU(vals, g)
+    assert rc == capi.TF_OK and rr <= 1e-13
+    assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
+    fixed = t.fixed.reshape(-1) != 0
+    assert np.all(du[fixed] == 0.0)
+
+
+def test_newton_step_matches_oracle_small_rectangle():
+    t = mesh.small_rectangle()
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    x_ref, it_ref, norms_ref = O.newton_step_dense(t, t.x, vs, inv, tol=t.newton_tol)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+        s.set_inv_fg(inv)
+        s.set_viscosity_surface(vs)
+        x, rc, st = s.updateStepNR(t.x, t.dt)
+    assert rc == capi.TF_OK
+    assert st["newton_iters"] == it_ref
+    np.testing.assert_allclose(st["du_norm"][0], norms_ref[0], rtol=1e-9)
+    assert np.abs(x - x_ref).max() <= 1e-9 * t.size
+
+
+def test_ten_time_steps_small_rectangle():
+    """Small rectangle, 10 implicit steps of 60 s, Newton tolerance 1e-10 (growth prologue on the
+    device): positions within 1e-9 of the tissue size of the oracle's dense-LU run."""
+    t = mesh.small_rectangle()
+    x_ref, fg_ref, it_ref, _ = O.simulate_dense(t, n_steps=10)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+        x = t.x.copy()
+        its = []
+        for _ in range(10):
+            x, rc, st = s.runOneStep(x, t.dt)
+            assert rc == capi.TF_OK
+            its.append(st["newton_iters"])
+        fg, _ = s.get_growth()
+    assert its == it_ref
+    np.testing.assert_allclose(fg, fg_ref, rtol=1e-13, atol=1e-15)
+    assert np.abs(x - x_ref).max() <= 1e-9 * t.size
+
+
+def test_time_steps_disc_matches_sparse_oracle():
+    t = mesh.small_disc(11, 3000, 2000.0, n_steps=3)
+    x_ref, fg_ref, it_ref, _ = O.simulate_sparse(t, n_steps=3)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+        x = t.x.copy()
+        for _ in range(3):
+            x, rc, st = s.runOneStep(x, t.dt)
+            assert rc == capi.TF_OK
+    assert np.abs(x - x_ref).max() <= 1e-9 * t.size
+
+
+def test_status_newton_cap():
+    t = mesh.small_rectangle(nx=5, ny=4)
+    with NewtonRaphsonSolver.from_tissue(t, max_newton_iters=0) as s:
+        x, rc, st = s.runOneStep(t.x, t.dt)
+    assert rc == capi.TF_NEWTON_NOT_CONVERGED and st["newton_iters"] == 1
+
+
+def test_status_krylov_cap():
+    t = mesh.small_rectangle(nx=5, ny=4)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_max_iters=1, max_newton_iters=1) as s:
+        x, rc, st = s.runOneStep(t.x, t.dt)
+    assert rc in (capi.TF_KRYLOV_MAX_ITERS, capi.TF_NEWTON_NOT_CONVERGED)
+    assert st["krylov_iters_max"] <= 1
+
+
+def test_status_nonfinite_input():
+    t = mesh.small_rectangle(nx=5, ny=4)
+    x = t.x.copy()
+    x[3, 0] = np.nan
+    with NewtonRaphsonSolver.from_tissue(t) as s:
+        x2, rc, st = s.updateStepNR(x, t.dt)
+    assert rc == capi.TF_NONFINITE
+
+
+def test_status_inverted_element():
+    t = mesh.small_rectangle(nx=5, ny=4)
+    x = t.x.copy()
+    apical = np.nonzero(t.node_placement == mesh.APICAL)[0]
+    x[apical, 2] = -5.0  # push the apical surface below the basal one
+    with NewtonRaphsonSolver.from_tissue(t, max_newton_iters=1) as s:
+        g = np.zeros(3)
+        g, vals, rp, ci, rc = s.assemble(x, t.x, t.dt)
+    assert rc == capi.TF_ELEMENT_INVERTED
+
+
+def test_schedule_and_autotune():
+    t = mesh.wing_disc(n_surface_points=800)
+    with NewtonRaphsonSolver.from_tissue(t) as s:
+        sch = s.schedule()
+        assert sch["n_colours"] > 0
+        tuned = s.autotune(t.x, t.dt)
+        assert tuned["scatter"] in (capi.TF_SCATTER_ATOMIC, capi.TF_SCATTER_COLOURED)
+        assert tuned["elems_per_block"] in (8, 16, 32)
+        me, ms = s.time_kernels(5)
+        assert me > 0 and ms > 0

@@ -1,0 +1,985 @@
+// tf_capi.cu -- host runtime and C ABI of the B200 Newton step (see include/tf_b200.h).
+//
+// The host side owns what the reference keeps in NewtonRaphsonSolver and the element objects:
+// it builds, once per mesh, the BSR3 pattern of the Jacobian, the element-to-block slot map,
+// a greedy element colouring and the slave-master routing, packs each prism into a 416-byte
+// record, and drives the Newton loop of Simulation::updateStepNR
+// (TissueFolding/SourceCode/Simulation.cpp:6605-6747) with one host synchronisation per
+// Newton iteration. The linear solve runs as graph-replayed chunks of BiCGStab iterations
+// whose scalars never leave the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "../../include/tf_b200.h"
+#include "tf_internal.cuh"
+
+using namespace tfb;
+
+namespace {
+
+constexpr int kChunk = 32;  // BiCGStab iterations per graph replay / status poll
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+template <class T>
+T* dptr(DevBuf& b) {
+    return static_cast<T*>(b.p);
+}
+
+}  // namespace
+
+struct tf_ctx {
+    tf_params params{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int32_t N = 0, E = 0;
+    int64_t nnzb = 0;
+
+    // host mirrors
+    std::vector<int32_t> conn;  // [E*6]
+    std::vector<double> xref;   // [E*18]
+    std::vector<int32_t> dofmap;
+    std::vector<int32_t> slave, master;
+    std::vector<int32_t> rowptr, colidx, diag;
+    std::vector<int32_t> colour_offsets;  // colour c: elements colour_list[off[c]..off[c+1])
+    std::vector<int32_t> colour_list;     // colour-sorted element ids, routed ones at the end
+    int32_t n_routed = 0;
+    int n_colours = 0;
+    bool has_visc = false;
+
+    // device buffers
+    DevBuf elems, fixmask, ext_visc, visc_surface, dofmap_d, slaves_d, masters_d;
+    DevBuf rowptr_d, colidx_d, diag_d, vals, colour_list_d;
+    DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
+    DevBuf fg, rates, angles, exposed, peripodial, rotated, xio;
+    KrylovScalars* h_sc = nullptr;  // pinned
+    int32_t* h_flags = nullptr;     // pinned
+
+    int scatter = TF_SCATTER_ATOMIC;
+    int teams = 32;
+    bool tuned = false;
+
+    cudaGraphExec_t krylov_graph = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_call[2] = {nullptr, nullptr};  // brackets a whole public call
+    int64_t launches = 0;                         // kernels launched by the current call
+    char last_error[256] = {0};
+};
+
+namespace {
+
+int set_error(tf_ctx* c, int code, const char* msg) {
+    if (c) std::snprintf(c->last_error, sizeof(c->last_error), "%s", msg);
+    return code;
+}
+
+#define TF_CK(call)                                                                   \
+    do {                                                                              \
+        cudaError_t err__ = (call);                                                   \
+        if (err__ != cudaSuccess) {                                                   \
+            cudaGetLastError();                                                       \
+            return set_error(ctx, err__ == cudaErrorMemoryAllocation ? TF_ERR_OUT_OF_MEMORY : TF_ERR_CUDA, \
+                             cudaGetErrorString(err__));                              \
+        }                                                                             \
+    } while (0)
+
+cudaError_t dalloc(DevBuf& b, size_t bytes) {
+    if (b.p && b.bytes >= bytes) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    if (bytes == 0) bytes = 16;
+    cudaError_t err = cudaMalloc(&b.p, bytes);
+    if (err == cudaSuccess) b.bytes = bytes;
+    return err;
+}
+
+void dfree(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+template <class F>
+void parallel_for(int64_t n, F f) {
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < 200000) nt = 1;
+    if (nt == 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const int64_t chunk = (n + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; ++t) {
+        const int64_t b = t * chunk, e = std::min<int64_t>(n, b + chunk);
+        if (b < e) th.emplace_back([=] { f(b, e); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// Block pattern under slave-master routing: block (r, c) exists when some element holds
+// nodes A, B whose DoFs route to nodes r and c; every node keeps its diagonal block.
+void build_pattern(tf_ctx* c) {
+    const int N = c->N, E = c->E;
+    std::vector<int32_t> ecount(N + 1, 0), eoff(N + 1, 0), elist((size_t)E * 6);
+    for (int e = 0; e < E; ++e)
+        for (int a = 0; a < 6; ++a) ecount[c->conn[(size_t)e * 6 + a]]++;
+    for (int i = 0; i < N; ++i) eoff[i + 1] = eoff[i] + ecount[i];
+    std::vector<int32_t> fill(eoff.begin(), eoff.end() - 1);
+    for (int e = 0; e < E; ++e)
+        for (int a = 0; a < 6; ++a) elist[fill[c->conn[(size_t)e * 6 + a]]++] = e;
+
+    // routed rows of each node and, inversely, the source nodes of each routed row
+    auto routes = [&](int A, int32_t out[3]) {
+        int n = 0;
+        for (int i = 0; i < 3; ++i) {
+            const int r = c->dofmap[(size_t)A * 3 + i] / 3;
+            bool dup = false;
+            for (int k = 0; k < n; ++k) dup |= out[k] == r;
+            if (!dup) out[n++] = r;
+        }
+        return n;
+    };
+    std::vector<std::vector<int32_t>> extra_src;  // only for rows that receive routed DoFs
+    std::vector<int32_t> extra_idx(N, -1);
+    if (!c->slave.empty()) {
+        for (int A = 0; A < N; ++A) {
+            int32_t rr[3];
+            const int n = routes(A, rr);
+            for (int k = 0; k < n; ++k)
+                if (rr[k] != A) {
+                    if (extra_idx[rr[k]] < 0) {
+                        extra_idx[rr[k]] = (int32_t)extra_src.size();
+                        extra_src.emplace_back();
+                    }
+                    extra_src[extra_idx[rr[k]]].push_back(A);
+                }
+        }
+    }
+    std::vector<std::vector<int32_t>> rows(N);
+    parallel_for(N, [&](int64_t b0, int64_t b1) {
+        std::vector<int32_t> mark(N, -1);
+        std::vector<int32_t> tmp;
+        for (int64_t r = b0; r < b1; ++r) {
+            tmp.clear();
+            auto add_src = [&](int A) {
+                for (int k = eoff[A]; k < eoff[A + 1]; ++k) {
+                    const int e = elist[k];
+                    for (int bn = 0; bn < 6; ++bn) {
+                        int32_t cc[3];
+                        const int nc = c->slave.empty() ? (cc[0] = c->conn[(size_t)e * 6 + bn], 1)
+                                                        : routes(c->conn[(size_t)e * 6 + bn], cc);
+                        for (int q = 0; q < nc; ++q)
+                            if (mark[cc[q]] != r) {
+                                mark[cc[q]] = (int32_t)r;
+                                tmp.push_back(cc[q]);
+                            }
+                    }
+                }
+            };
+            if (mark[r] != r) {
+                mark[r] = (int32_t)r;
+                tmp.push_back((int32_t)r);
+            }
+            // node r itself contributes to row r unless all its DoFs are routed elsewhere
+            bool self = true;
+            if (!c->slave.empty()) {
+                self = false;
+                for (int i = 0; i < 3; ++i) self |= c->dofmap[r * 3 + i] / 3 == r;
+            }
+            if (self) add_src((int)r);
+            if (!c->slave.empty() && extra_idx[r] >= 0)
+                for (int A : extra_src[extra_idx[r]]) add_src(A);
+            std::sort(tmp.begin(), tmp.end());
+            rows[r] = tmp;
+        }
+    });
+    c->rowptr.assign(N + 1, 0);
+    for (int i = 0; i < N; ++i) c->rowptr[i + 1] = c->rowptr[i] + (int32_t)rows[i].size();
+    c->nnzb = c->rowptr[N];
+    c->colidx.resize(c->nnzb);
+    c->diag.resize(N);
+    for (int i = 0; i < N; ++i) {
+        std::copy(rows[i].begin(), rows[i].end(), c->colidx.begin() + c->rowptr[i]);
+        c->diag[i] = c->rowptr[i] + (int32_t)(std::lower_bound(rows[i].begin(), rows[i].end(), i) - rows[i].begin());
+    }
+}
+
+// Greedy colouring over elements in mesh order: no two prisms of one colour share a node.
+// Elements that touch a slave DoF are kept out of the colours and listed last.
+void build_colouring(tf_ctx* c, const std::vector<int32_t>& routed) {
+    const int E = c->E;
+    std::vector<uint64_t> used(c->N, 0);
+    std::vector<int8_t> col(E, -1);
+    int ncol = 0;
+    bool ok = true;
+    for (int e = 0; e < E && ok; ++e) {
+        if (routed[e]) continue;
+        uint64_t forb = 0;
+        for (int a = 0; a < 6; ++a) forb |= used[c->conn[(size_t)e * 6 + a]];
+        if (~forb == 0) {
+            ok = false;
+            break;
+        }
+        const int k = __builtin_ctzll(~forb);
+        col[e] = (int8_t)k;
+        ncol = std::max(ncol, k + 1);
+        for (int a = 0; a < 6; ++a) used[c->conn[(size_t)e * 6 + a]] |= (1ull << k);
+    }
+    c->colour_list.clear();
+    c->colour_offsets.clear();
+    c->n_routed = 0;
+    if (!ok) {
+        c->n_colours = 0;
+        return;
+    }
+    std::vector<int32_t> cnt(ncol + 1, 0);
+    for (int e = 0; e < E; ++e)
+        if (col[e] >= 0) cnt[col[e] + 1]++;
+    for (int k = 0; k < ncol; ++k) cnt[k + 1] += cnt[k];
+    c->colour_offsets = cnt;
+    c->colour_list.resize(E);
+    std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+    int32_t tail = cnt[ncol];
+    for (int e = 0; e < E; ++e) {
+        if (col[e] >= 0)
+            c->colour_list[pos[col[e]]++] = e;
+        else
+            c->colour_list[tail++] = e;
+    }
+    c->n_routed = E - cnt[ncol];
+    c->n_colours = ncol;
+}
+
+int upload_structure(tf_ctx* ctx) {
+    const int N = ctx->N, E = ctx->E;
+    build_pattern(ctx);
+    // element flags and slot map
+    std::vector<int32_t> routed(E, 0);
+    std::vector<uint8_t> node_bound(N, 0);
+    for (int A = 0; A < N; ++A)
+        for (int i = 0; i < 3; ++i)
+            if (ctx->dofmap[(size_t)A * 3 + i] != A * 3 + i) node_bound[A] = 1;
+    std::vector<ElemRecord> rec(E);
+    // keep the previous material / growth values if the records already exist on the device
+    const bool keep = ctx->elems.p != nullptr && ctx->elems.bytes >= sizeof(ElemRecord) * (size_t)E;
+    if (keep) TF_CK(cudaMemcpy(rec.data(), ctx->elems.p, sizeof(ElemRecord) * (size_t)E, cudaMemcpyDeviceToHost));
+    parallel_for(E, [&](int64_t b0, int64_t b1) {
+        for (int64_t e = b0; e < b1; ++e) {
+            ElemRecord& R = rec[e];
+            if (!keep) {
+                std::memset(&R, 0, sizeof(R));
+                for (int k = 0; k < 9; ++k) R.inv_fg[k] = (k % 4 == 0) ? 1.0 : 0.0;
+            }
+            const int32_t* cn = &ctx->conn[(size_t)e * 6];
+            bool rt = false;
+            for (int a = 0; a < 6; ++a) {
+                R.conn[a] = cn[a];
+                rt |= node_bound[cn[a]] != 0;
+            }
+            for (int k = 0; k < 18; ++k) R.xref[k] = ctx->xref[(size_t)e * 18 + k];
+            routed[e] = rt;
+            R.flags = rt ? 1 : 0;
+            for (int a = 0; a < 6; ++a)
+                for (int b = 0; b < 6; ++b) {
+                    int32_t slot = -1;
+                    if (!rt) {
+                        const int32_t* r0 = ctx->colidx.data() + ctx->rowptr[cn[a]];
+                        const int32_t* r1 = ctx->colidx.data() + ctx->rowptr[cn[a] + 1];
+                        slot = (int32_t)(std::lower_bound(r0, r1, cn[b]) - ctx->colidx.data());
+                    }
+                    R.slots[a * 6 + b] = slot;
+                }
+        }
+    });
+    build_colouring(ctx, routed);
+    TF_CK(dalloc(ctx->elems, sizeof(ElemRecord) * (size_t)E));
+    TF_CK(cudaMemcpy(ctx->elems.p, rec.data(), sizeof(ElemRecord) * (size_t)E, cudaMemcpyHostToDevice));
+    TF_CK(dalloc(ctx->rowptr_d, sizeof(int32_t) * (N + 1)));
+    TF_CK(dalloc(ctx->colidx_d, sizeof(int32_t) * (size_t)ctx->nnzb));
+    TF_CK(dalloc(ctx->diag_d, sizeof(int32_t) * N));
+    TF_CK(dalloc(ctx->vals, sizeof(double) * 9 * (size_t)ctx->nnzb));
+    TF_CK(cudaMemcpy(ctx->rowptr_d.p, ctx->rowptr.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice));
+    TF_CK(cudaMemcpy(ctx->colidx_d.p, ctx->colidx.data(), sizeof(int32_t) * (size_t)ctx->nnzb, cudaMemcpyHostToDevice));
+    TF_CK(cudaMemcpy(ctx->diag_d.p, ctx->diag.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+    TF_CK(dalloc(ctx->colour_list_d, sizeof(int32_t) * std::max<size_t>(1, ctx->colour_list.size())));
+    if (!ctx->colour_list.empty())
+        TF_CK(cudaMemcpy(ctx->colour_list_d.p, ctx->colour_list.data(), sizeof(int32_t) * ctx->colour_list.size(),
+                         cudaMemcpyHostToDevice));
+    TF_CK(dalloc(ctx->dofmap_d, sizeof(int32_t) * 3 * (size_t)N));
+    TF_CK(cudaMemcpy(ctx->dofmap_d.p, ctx->dofmap.data(), sizeof(int32_t) * 3 * (size_t)N, cudaMemcpyHostToDevice));
+    const size_t np = std::max<size_t>(1, ctx->slave.size());
+    TF_CK(dalloc(ctx->slaves_d, sizeof(int32_t) * np));
+    TF_CK(dalloc(ctx->masters_d, sizeof(int32_t) * np));
+    if (!ctx->slave.empty()) {
+        TF_CK(cudaMemcpy(ctx->slaves_d.p, ctx->slave.data(), sizeof(int32_t) * ctx->slave.size(), cudaMemcpyHostToDevice));
+        TF_CK(cudaMemcpy(ctx->masters_d.p, ctx->master.data(), sizeof(int32_t) * ctx->master.size(), cudaMemcpyHostToDevice));
+    }
+    const size_t np2 = (size_t)std::max(spmv_grid(N), vec_grid(N)) * 2 + 64;
+    TF_CK(dalloc(ctx->partials, sizeof(double) * np2));
+    if (ctx->krylov_graph) {
+        cudaGraphExecDestroy(ctx->krylov_graph);
+        ctx->krylov_graph = nullptr;
+    }
+    return TF_OK;
+}
+
+KrylovWork make_work(tf_ctx* c) {
+    KrylovWork w;
+    w.n_nodes = c->N;
+    w.rowptr = dptr<int32_t>(c->rowptr_d);
+    w.colidx = dptr<int32_t>(c->colidx_d);
+    w.diag = dptr<int32_t>(c->diag_d);
+    w.vals = dptr<double>(c->vals);
+    w.x = dptr<double>(c->du);
+    w.b = dptr<double>(c->g);
+    w.r = dptr<double>(c->r);
+    w.rhat = dptr<double>(c->rhat);
+    w.p = dptr<double>(c->p);
+    w.v = dptr<double>(c->v);
+    w.s = dptr<double>(c->s);
+    w.t = dptr<double>(c->t);
+    w.phat = dptr<double>(c->phat);
+    w.shat = dptr<double>(c->shat);
+    w.dinv = dptr<double>(c->dinv);
+    w.partials = dptr<double>(c->partials);
+    w.n_partials = (int32_t)(c->partials.bytes / sizeof(double));
+    w.sc = dptr<KrylovScalars>(c->sc);
+    w.dflags = dptr<int32_t>(c->dflags);
+    return w;
+}
+
+AssembleArgs make_assemble(tf_ctx* c, double dt) {
+    AssembleArgs a;
+    a.elems = dptr<ElemRecord>(c->elems);
+    a.elem_list = nullptr;
+    a.e_begin = 0;
+    a.e_count = c->E;
+    a.uk = dptr<double>(c->uk);
+    a.un = dptr<double>(c->un);
+    a.inv_dt = 1.0 / dt;
+    a.fixmask = dptr<uint8_t>(c->fixmask);
+    a.dofmap = dptr<int32_t>(c->dofmap_d);
+    a.rowptr = dptr<int32_t>(c->rowptr_d);
+    a.colidx = dptr<int32_t>(c->colidx_d);
+    a.vals = dptr<double>(c->vals);
+    a.g = dptr<double>(c->g);
+    a.dflags = dptr<int32_t>(c->dflags);
+    return a;
+}
+
+// Element kernels for the current schedule (no memset, no node terms).
+cudaError_t launch_elements(tf_ctx* c, double dt, int scatter, int teams) {
+    AssembleArgs a = make_assemble(c, dt);
+    if (scatter == TF_SCATTER_COLOURED && c->n_colours > 0) {
+        c->launches += c->n_colours + (c->n_routed > 0 ? 1 : 0);
+        a.elem_list = dptr<int32_t>(c->colour_list_d);
+        for (int k = 0; k < c->n_colours; ++k) {
+            a.e_begin = c->colour_offsets[k];
+            a.e_count = c->colour_offsets[k + 1] - c->colour_offsets[k];
+            cudaError_t err = launch_element_assemble(a, teams, c->has_visc, 1, c->stream);
+            if (err != cudaSuccess) return err;
+        }
+        if (c->n_routed > 0) {
+            a.e_begin = c->E - c->n_routed;
+            a.e_count = c->n_routed;
+            return launch_element_assemble(a, teams, c->has_visc, 0, c->stream);
+        }
+        return cudaSuccess;
+    }
+    c->launches += 1;
+    return launch_element_assemble(a, teams, c->has_visc, 0, c->stream);
+}
+
+// One Newton iteration's system: J (BSR3) and g in the context's buffers.
+int assemble_system(tf_ctx* ctx, double dt) {
+    TF_CK(cudaMemsetAsync(ctx->vals.p, 0, sizeof(double) * 9 * (size_t)ctx->nnzb, ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->g.p, 0, sizeof(double) * 3 * (size_t)ctx->N, ctx->stream));
+    TF_CK(launch_elements(ctx, dt, ctx->scatter, ctx->teams));
+    NodeArgs na;
+    na.n_nodes = ctx->N;
+    na.uk = dptr<double>(ctx->uk);
+    na.un = dptr<double>(ctx->un);
+    na.dt = dt;
+    na.fixmask = dptr<uint8_t>(ctx->fixmask);
+    na.ext_visc = dptr<double>(ctx->ext_visc);
+    na.visc_surface = dptr<double>(ctx->visc_surface);
+    na.dofmap = dptr<int32_t>(ctx->dofmap_d);
+    na.diag = dptr<int32_t>(ctx->diag_d);
+    na.rowptr = dptr<int32_t>(ctx->rowptr_d);
+    na.colidx = dptr<int32_t>(ctx->colidx_d);
+    na.vals = dptr<double>(ctx->vals);
+    na.g = dptr<double>(ctx->g);
+    na.dflags = dptr<int32_t>(ctx->dflags);
+    TF_CK(launch_node_terms(na, ctx->stream));
+    ctx->launches += 1;
+    return TF_OK;
+}
+
+int krylov_status_to_tf(int ks) {
+    switch (ks) {
+        case KS_CONVERGED: return TF_OK;
+        case KS_MAXIT: return TF_KRYLOV_MAX_ITERS;
+        case KS_BREAKDOWN: return TF_KRYLOV_BREAKDOWN;
+        case KS_NONFINITE: return TF_NONFINITE;
+        default: return TF_KRYLOV_MAX_ITERS;
+    }
+}
+
+// Solve J du = g (buffers in the context). Leaves the scalars in ctx->h_sc.
+int krylov_solve(tf_ctx* ctx) {
+    KrylovWork w = make_work(ctx);
+    TF_CK(launch_block_jacobi_setup(w, ctx->stream));
+    TF_CK(launch_krylov_init(w, ctx->params.krylov_rtol, ctx->params.krylov_max_iters, ctx->stream));
+    ctx->launches += 2;
+    if (ctx->params.use_graphs && !ctx->krylov_graph) {
+        cudaGraph_t graph;
+        TF_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < kChunk; ++i) launch_bicgstab_iteration(w, ctx->stream);
+        cudaError_t cerr = cudaStreamEndCapture(ctx->stream, &graph);
+        TF_CK(cerr);
+        cerr = cudaGraphInstantiate(&ctx->krylov_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        TF_CK(cerr);
+    }
+    const int max_chunks = ctx->params.krylov_max_iters / kChunk + 2;
+    for (int ch = 0; ch < max_chunks; ++ch) {
+        if (ctx->params.use_graphs) {
+            TF_CK(cudaGraphLaunch(ctx->krylov_graph, ctx->stream));
+        } else {
+            for (int i = 0; i < kChunk; ++i) TF_CK(launch_bicgstab_iteration(w, ctx->stream));
+        }
+        ctx->launches += 5 * kChunk;
+        TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        TF_CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_sc->status != KS_RUNNING) break;
+    }
+    return TF_OK;
+}
+
+int read_flags(tf_ctx* ctx) {
+    TF_CK(cudaMemcpyAsync(ctx->h_flags, ctx->dflags.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    return TF_OK;
+}
+
+int worse(int a, int b) {
+    if (a < 0 || b < 0) return std::min(a, b);
+    return std::max(a, b);
+}
+
+// Newton loop on device buffers: un holds x_n; result left in uk.
+int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
+    TF_CK(cudaMemcpyAsync(ctx->uk.p, ctx->un.p, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyDeviceToDevice, ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+    int status = TF_OK;
+    int iteratorK = 0;
+    bool converged = false;
+    float ms;
+    while (!converged) {
+        TF_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        int rc = assemble_system(ctx, dt);
+        if (rc != TF_OK) return rc;
+        TF_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+        rc = krylov_solve(ctx);
+        if (rc != TF_OK) return rc;
+        const KrylovScalars sc = *ctx->h_sc;
+        KrylovWork w = make_work(ctx);
+        TF_CK(launch_newton_update(w, dptr<double>(ctx->uk), dptr<int32_t>(ctx->slaves_d), dptr<int32_t>(ctx->masters_d),
+                                   (int32_t)ctx->slave.size(), ctx->stream));
+        ctx->launches += ctx->slave.empty() ? 1 : 2;
+        TF_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        rc = read_flags(ctx);
+        if (rc != TF_OK) return rc;
+        TF_CK(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
+        st->ms_assemble += ms;
+        TF_CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+        st->ms_solve += ms;
+        const int ks = krylov_status_to_tf(sc.status);
+        if (ks != TF_OK) status = worse(status, ks);
+        if (*ctx->h_flags & DF_INVERTED) status = worse(status, TF_ELEMENT_INVERTED);
+        if (*ctx->h_flags & DF_PATTERN_MISS) return set_error(ctx, TF_ERR_STATE, "routed entry outside the pattern");
+        const double d = std::sqrt(ctx->h_sc->du2);
+        if (iteratorK < 32) {
+            st->du_norm[iteratorK] = d;
+            st->krylov_rel_res[iteratorK] = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+        }
+        st->krylov_iters_total += sc.iter;
+        st->krylov_iters_max = std::max(st->krylov_iters_max, sc.iter);
+        if (!std::isfinite(d)) {
+            status = worse(status, TF_NONFINITE);
+            iteratorK++;
+            break;
+        }
+        // checkConvergenceViaDeltaU (NewtonRaphsonSolver.cpp:807-825), then the cap of
+        // Simulation.cpp:6724-6727 (the update above is applied either way).
+        converged = !(d > ctx->params.newton_tol);
+        iteratorK++;
+        if (!converged && iteratorK > ctx->params.max_newton_iters) {
+            status = worse(status, TF_NEWTON_NOT_CONVERGED);
+            converged = true;
+        }
+    }
+    st->newton_iters = iteratorK;
+    st->status = status;
+    return status;
+}
+
+// Bracket a public call: reset the stats and the launch counter, record the start event.
+int call_begin(tf_ctx* ctx, tf_step_stats* st) {
+    std::memset(st, 0, sizeof(*st));
+    ctx->launches = 0;
+    TF_CK(cudaEventRecord(ctx->ev_call[0], ctx->stream));
+    return TF_OK;
+}
+
+int call_end(tf_ctx* ctx, tf_step_stats* st) {
+    TF_CK(cudaEventRecord(ctx->ev_call[1], ctx->stream));
+    TF_CK(cudaEventSynchronize(ctx->ev_call[1]));
+    float ms = 0.0f;
+    TF_CK(cudaEventElapsedTime(&ms, ctx->ev_call[0], ctx->ev_call[1]));
+    st->ms_total = ms;
+    st->gpu_launches = ctx->launches;
+    return TF_OK;
+}
+
+int prologue(tf_ctx* ctx, double dt) {
+    TF_CK(launch_grow(dptr<ElemRecord>(ctx->elems), ctx->E, dptr<double>(ctx->un), dptr<double>(ctx->fg),
+                      dptr<double>(ctx->rates), dptr<double>(ctx->angles), dt, dptr<int32_t>(ctx->rotated), ctx->stream));
+    TF_CK(launch_viscosity_surface(dptr<ElemRecord>(ctx->elems), ctx->E, ctx->N, dptr<double>(ctx->un),
+                                   dptr<uint8_t>(ctx->exposed), dptr<uint8_t>(ctx->peripodial),
+                                   dptr<double>(ctx->visc_surface), ctx->stream));
+    ctx->launches += 2;
+    return TF_OK;
+}
+
+int check_ctx(tf_ctx* ctx) {
+    if (!ctx) return TF_ERR_ARGUMENT;
+    cudaError_t err = cudaSetDevice(ctx->device);
+    if (err != cudaSuccess) return set_error(ctx, TF_ERR_CUDA, cudaGetErrorString(err));
+    return TF_OK;
+}
+
+// Per-element field setter: writes `ncomp` doubles at byte offset `off` of every record.
+int set_record_field(tf_ctx* ctx, size_t off, int ncomp, const double* src) {
+    std::vector<ElemRecord> rec(ctx->E);
+    TF_CK(cudaMemcpy(rec.data(), ctx->elems.p, sizeof(ElemRecord) * (size_t)ctx->E, cudaMemcpyDeviceToHost));
+    for (int e = 0; e < ctx->E; ++e)
+        std::memcpy(reinterpret_cast<char*>(&rec[e]) + off, src + (size_t)e * ncomp, sizeof(double) * ncomp);
+    TF_CK(cudaMemcpy(ctx->elems.p, rec.data(), sizeof(ElemRecord) * (size_t)ctx->E, cudaMemcpyHostToDevice));
+    return TF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tf_default_params(tf_params* p) {
+    if (!p) return;
+    p->max_newton_iters = 20;
+    p->newton_tol = 1e-8;
+    p->krylov_max_iters = 20000;
+    p->krylov_rtol = 1e-12;
+    p->precond = TF_PRECOND_BLOCK_JACOBI;
+    p->scatter = TF_SCATTER_AUTO;
+    p->elems_per_block = 0;
+    p->device = 0;
+    p->use_graphs = 1;
+}
+
+const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
+
+int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
+    if (!out) return TF_ERR_ARGUMENT;
+    *out = nullptr;
+    if (!mesh || mesh->n_nodes <= 0 || mesh->n_elems <= 0 || !mesh->conn || !mesh->xref) return TF_ERR_ARGUMENT;
+    for (int64_t k = 0; k < (int64_t)mesh->n_elems * 6; ++k)
+        if (mesh->conn[k] < 0 || mesh->conn[k] >= mesh->n_nodes) return TF_ERR_ARGUMENT;
+    std::unique_ptr<tf_ctx> holder(new (std::nothrow) tf_ctx());
+    tf_ctx* ctx = holder.get();
+    if (!ctx) return TF_ERR_OUT_OF_MEMORY;
+    if (params)
+        ctx->params = *params;
+    else
+        tf_default_params(&ctx->params);
+    if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI) return TF_ERR_UNSUPPORTED;
+    if (ctx->params.krylov_max_iters <= 0 || ctx->params.max_newton_iters < 0) return TF_ERR_ARGUMENT;
+    ctx->device = ctx->params.device;
+    TF_CK(cudaSetDevice(ctx->device));
+    TF_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for (auto& e : ctx->ev) TF_CK(cudaEventCreate(&e));
+    for (auto& e : ctx->ev_call) TF_CK(cudaEventCreate(&e));
+    ctx->N = mesh->n_nodes;
+    ctx->E = mesh->n_elems;
+    ctx->conn.assign(mesh->conn, mesh->conn + (size_t)ctx->E * 6);
+    ctx->xref.assign(mesh->xref, mesh->xref + (size_t)ctx->E * 18);
+    ctx->dofmap.resize((size_t)ctx->N * 3);
+    for (size_t i = 0; i < ctx->dofmap.size(); ++i) ctx->dofmap[i] = (int32_t)i;
+    const size_t n3 = (size_t)ctx->N * 3, N = ctx->N, E = ctx->E;
+    DevBuf* vecs[] = {&ctx->uk, &ctx->un, &ctx->g, &ctx->du, &ctx->r, &ctx->rhat, &ctx->p, &ctx->v,
+                      &ctx->s, &ctx->t, &ctx->phat, &ctx->shat, &ctx->xio};
+    for (DevBuf* b : vecs) TF_CK(dalloc(*b, sizeof(double) * n3));
+    TF_CK(dalloc(ctx->dinv, sizeof(double) * 9 * N));
+    TF_CK(dalloc(ctx->fixmask, N));
+    TF_CK(dalloc(ctx->ext_visc, sizeof(double) * n3));
+    TF_CK(dalloc(ctx->visc_surface, sizeof(double) * N));
+    TF_CK(dalloc(ctx->sc, sizeof(KrylovScalars)));
+    TF_CK(dalloc(ctx->dflags, sizeof(int32_t)));
+    TF_CK(dalloc(ctx->fg, sizeof(double) * 9 * E));
+    TF_CK(dalloc(ctx->rates, sizeof(double) * 3 * E));
+    TF_CK(dalloc(ctx->angles, sizeof(double) * E));
+    TF_CK(dalloc(ctx->exposed, E));
+    TF_CK(dalloc(ctx->peripodial, E));
+    TF_CK(dalloc(ctx->rotated, sizeof(int32_t) * E));
+    TF_CK(cudaMemset(ctx->sc.p, 0, sizeof(KrylovScalars)));
+    TF_CK(cudaMemset(ctx->fixmask.p, 0, N));
+    TF_CK(cudaMemset(ctx->ext_visc.p, 0, sizeof(double) * n3));
+    TF_CK(cudaMemset(ctx->visc_surface.p, 0, sizeof(double) * N));
+    TF_CK(cudaMemset(ctx->rates.p, 0, sizeof(double) * 3 * E));
+    TF_CK(cudaMemset(ctx->angles.p, 0, sizeof(double) * E));
+    TF_CK(cudaMemset(ctx->exposed.p, 0, E));
+    TF_CK(cudaMemset(ctx->peripodial.p, 0, E));
+    {
+        std::vector<double> eye((size_t)9 * E);
+        for (size_t e = 0; e < E; ++e)
+            for (int k = 0; k < 9; ++k) eye[e * 9 + k] = (k % 4 == 0) ? 1.0 : 0.0;
+        TF_CK(cudaMemcpy(ctx->fg.p, eye.data(), sizeof(double) * 9 * E, cudaMemcpyHostToDevice));
+    }
+    TF_CK(cudaMallocHost(&ctx->h_sc, sizeof(KrylovScalars)));
+    TF_CK(cudaMallocHost(&ctx->h_flags, sizeof(int32_t)));
+    int rc = upload_structure(ctx);
+    if (rc != TF_OK) return rc;
+    if (ctx->params.scatter == TF_SCATTER_COLOURED && ctx->n_colours == 0) return TF_ERR_UNSUPPORTED;
+    ctx->scatter = ctx->params.scatter == TF_SCATTER_AUTO ? TF_SCATTER_ATOMIC : ctx->params.scatter;
+    ctx->teams = ctx->params.elems_per_block > 0 ? ctx->params.elems_per_block : 16;
+    if (ctx->teams != 8 && ctx->teams != 16 && ctx->teams != 32) return TF_ERR_ARGUMENT;
+    *out = holder.release();
+    return TF_OK;
+}
+
+void tf_destroy(tf_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->krylov_graph) cudaGraphExecDestroy(ctx->krylov_graph);
+    DevBuf* all[] = {&ctx->elems, &ctx->fixmask, &ctx->ext_visc, &ctx->visc_surface, &ctx->dofmap_d,
+                     &ctx->slaves_d, &ctx->masters_d, &ctx->rowptr_d, &ctx->colidx_d, &ctx->diag_d,
+                     &ctx->vals, &ctx->colour_list_d, &ctx->uk, &ctx->un, &ctx->g, &ctx->du, &ctx->r,
+                     &ctx->rhat, &ctx->p, &ctx->v, &ctx->s, &ctx->t, &ctx->phat, &ctx->shat, &ctx->dinv,
+                     &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
+                     &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio};
+    for (DevBuf* b : all) dfree(*b);
+    if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
+    if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->ev_call)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int tf_set_material(tf_ctx* ctx, const double* lambda, const double* mu, const double* eta) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!lambda || !mu) return TF_ERR_ARGUMENT;
+    std::vector<double> lme((size_t)ctx->E * 3);
+    bool visc = false;
+    for (int e = 0; e < ctx->E; ++e) {
+        lme[(size_t)e * 3 + 0] = lambda[e];
+        lme[(size_t)e * 3 + 1] = mu[e];
+        lme[(size_t)e * 3 + 2] = eta ? eta[e] : 0.0;
+        visc |= eta && eta[e] != 0.0;
+    }
+    ctx->has_visc = visc;
+    return set_record_field(ctx, offsetof(ElemRecord, lam), 3, lme.data());
+}
+
+int tf_set_inv_fg(tf_ctx* ctx, const double* inv_fg) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!inv_fg) return TF_ERR_ARGUMENT;
+    return set_record_field(ctx, offsetof(ElemRecord, inv_fg), 9, inv_fg);
+}
+
+int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
+                    const int32_t* slave_master, int32_t n_pairs) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    const int N = ctx->N;
+    if (n_pairs < 0 || (n_pairs > 0 && !slave_master)) return TF_ERR_ARGUMENT;
+    std::vector<uint8_t> fm(N, 0);
+    if (fixed)
+        for (int i = 0; i < N; ++i)
+            fm[i] = (uint8_t)((fixed[i * 3] ? 1 : 0) | (fixed[i * 3 + 1] ? 2 : 0) | (fixed[i * 3 + 2] ? 4 : 0));
+    TF_CK(cudaMemcpy(ctx->fixmask.p, fm.data(), N, cudaMemcpyHostToDevice));
+    if (ext_visc) TF_CK(cudaMemcpy(ctx->ext_visc.p, ext_visc, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+    std::vector<int32_t> dm((size_t)N * 3);
+    for (size_t i = 0; i < dm.size(); ++i) dm[i] = (int32_t)i;
+    std::vector<int32_t> sl, ms;
+    for (int p = 0; p < n_pairs; ++p) {
+        const int32_t s = slave_master[2 * p], m = slave_master[2 * p + 1];
+        if (s < 0 || m < 0 || s >= 3 * N || m >= 3 * N || s == m) return TF_ERR_ARGUMENT;
+        dm[s] = m;
+        sl.push_back(s);
+        ms.push_back(m);
+    }
+    for (int32_t m : ms)
+        if (dm[m] != m) return set_error(ctx, TF_ERR_ARGUMENT, "a master DoF is itself a slave");
+    const bool changed = dm != ctx->dofmap;
+    ctx->dofmap = dm;
+    ctx->slave = sl;
+    ctx->master = ms;
+    if (changed) return upload_structure(ctx);
+    TF_CK(cudaMemcpy(ctx->dofmap_d.p, dm.data(), sizeof(int32_t) * dm.size(), cudaMemcpyHostToDevice));
+    return TF_OK;
+}
+
+int tf_set_viscosity_surface(tf_ctx* ctx, const double* visc_surface) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!visc_surface) return TF_ERR_ARGUMENT;
+    TF_CK(cudaMemcpy(ctx->visc_surface.p, visc_surface, sizeof(double) * ctx->N, cudaMemcpyHostToDevice));
+    return TF_OK;
+}
+
+// Shared body of the four step entry points. `host` selects host (H2D/D2H) or device
+// pointers; `grow` adds the per-step prologue.
+static int step_entry(tf_ctx* ctx, const double* x_n, double dt, double* x_out, tf_step_stats* stats,
+                      bool host, bool grow) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!x_n || !x_out || !(dt > 0)) return TF_ERR_ARGUMENT;
+    tf_step_stats local;
+    tf_step_stats* st = stats ? stats : &local;
+    rc = call_begin(ctx, st);
+    if (rc != TF_OK) return rc;
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(cudaMemcpyAsync(ctx->un.p, x_n, bytes, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+    if (grow) {
+        rc = prologue(ctx, dt);
+        if (rc != TF_OK) return rc;
+    }
+    rc = newton_core(ctx, dt, st);
+    if (rc < 0) return rc;
+    TF_CK(cudaMemcpyAsync(x_out, ctx->uk.p, bytes, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+    const int rc2 = call_end(ctx, st);
+    return rc2 != TF_OK ? rc2 : rc;
+}
+
+int tf_newton_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x_out, tf_step_stats* stats) {
+    return step_entry(ctx, d_x_n, dt, d_x_out, stats, false, false);
+}
+
+int tf_newton_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out, tf_step_stats* stats) {
+    return step_entry(ctx, x_n, dt, x_out, stats, true, false);
+}
+
+int tf_get_pattern(tf_ctx* ctx, int32_t* nnzb, int32_t* rowptr, int32_t* colidx) {
+    if (!ctx) return TF_ERR_ARGUMENT;
+    if (nnzb) *nnzb = (int32_t)ctx->nnzb;
+    if (rowptr) std::memcpy(rowptr, ctx->rowptr.data(), sizeof(int32_t) * (ctx->N + 1));
+    if (colidx) std::memcpy(colidx, ctx->colidx.data(), sizeof(int32_t) * (size_t)ctx->nnzb);
+    return TF_OK;
+}
+
+int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, double* g_out, double* bsr_vals_out) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!uk || !un || !g_out || !(dt > 0)) return TF_ERR_ARGUMENT;
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(cudaMemcpyAsync(ctx->uk.p, uk, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->un.p, un, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+    rc = assemble_system(ctx, dt);
+    if (rc != TF_OK) return rc;
+    TF_CK(cudaMemcpyAsync(g_out, ctx->g.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    if (bsr_vals_out)
+        TF_CK(cudaMemcpyAsync(bsr_vals_out, ctx->vals.p, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    rc = read_flags(ctx);
+    if (rc != TF_OK) return rc;
+    if (*ctx->h_flags & DF_PATTERN_MISS) return set_error(ctx, TF_ERR_STATE, "routed entry outside the pattern");
+    return (*ctx->h_flags & DF_INVERTED) ? TF_ELEMENT_INVERTED : TF_OK;
+}
+
+int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, int32_t* iters, double* rel_res) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!bsr_vals || !g || !du) return TF_ERR_ARGUMENT;
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(cudaMemcpyAsync(ctx->vals.p, bsr_vals, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->g.p, g, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+    rc = krylov_solve(ctx);
+    if (rc != TF_OK) return rc;
+    const KrylovScalars sc = *ctx->h_sc;
+    if (!ctx->slave.empty()) {
+        KrylovWork w = make_work(ctx);
+        // equate slaves only (no position update): reuse the update kernel on a scratch vector
+        TF_CK(cudaMemsetAsync(ctx->xio.p, 0, bytes, ctx->stream));
+        TF_CK(launch_newton_update(w, dptr<double>(ctx->xio), dptr<int32_t>(ctx->slaves_d), dptr<int32_t>(ctx->masters_d),
+                                   (int32_t)ctx->slave.size(), ctx->stream));
+    }
+    TF_CK(cudaMemcpyAsync(du, ctx->du.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    if (iters) *iters = sc.iter;
+    if (rel_res) *rel_res = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+    return krylov_status_to_tf(sc.status);
+}
+
+int tf_set_growth(tf_ctx* ctx, const double* fg, const double* rates, const double* angles,
+                  const uint8_t* exposed, const uint8_t* peripodial) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    const size_t E = ctx->E;
+    if (fg) {
+        TF_CK(cudaMemcpy(ctx->fg.p, fg, sizeof(double) * 9 * E, cudaMemcpyHostToDevice));
+        // keep InvFg consistent with Fg (growShapeByFg leaves both in step)
+        std::vector<double> inv(9 * E);
+        for (size_t e = 0; e < E; ++e) {
+            const double* m = fg + e * 9;
+            const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                               m[2] * (m[3] * m[7] - m[4] * m[6]);
+            if (det == 0.0 || !std::isfinite(det)) return TF_ERR_ARGUMENT;
+            const double id = 1.0 / det;
+            double* o = &inv[e * 9];
+            o[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+            o[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+            o[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+            o[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+            o[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+            o[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+            o[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+            o[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+            o[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+        }
+        rc = set_record_field(ctx, offsetof(ElemRecord, inv_fg), 9, inv.data());
+        if (rc != TF_OK) return rc;
+    }
+    if (rates) TF_CK(cudaMemcpy(ctx->rates.p, rates, sizeof(double) * 3 * E, cudaMemcpyHostToDevice));
+    if (angles) TF_CK(cudaMemcpy(ctx->angles.p, angles, sizeof(double) * E, cudaMemcpyHostToDevice));
+    if (exposed) TF_CK(cudaMemcpy(ctx->exposed.p, exposed, E, cudaMemcpyHostToDevice));
+    if (peripodial) TF_CK(cudaMemcpy(ctx->peripodial.p, peripodial, E, cudaMemcpyHostToDevice));
+    return TF_OK;
+}
+
+int tf_get_growth(tf_ctx* ctx, double* fg, double* inv_fg) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    if (fg) TF_CK(cudaMemcpy(fg, ctx->fg.p, sizeof(double) * 9 * (size_t)ctx->E, cudaMemcpyDeviceToHost));
+    if (inv_fg) {
+        std::vector<ElemRecord> rec(ctx->E);
+        TF_CK(cudaMemcpy(rec.data(), ctx->elems.p, sizeof(ElemRecord) * (size_t)ctx->E, cudaMemcpyDeviceToHost));
+        for (int e = 0; e < ctx->E; ++e) std::memcpy(inv_fg + (size_t)e * 9, rec[e].inv_fg, sizeof(double) * 9);
+    }
+    return TF_OK;
+}
+
+int tf_time_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x_out, tf_step_stats* stats) {
+    return step_entry(ctx, d_x_n, dt, d_x_out, stats, false, true);
+}
+
+int tf_time_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out, tf_step_stats* stats) {
+    return step_entry(ctx, x_n, dt, x_out, stats, true, true);
+}
+
+int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* elems_per_block) {
+    if (!ctx) return TF_ERR_ARGUMENT;
+    if (n_colours) *n_colours = ctx->n_colours;
+    if (scatter) *scatter = ctx->scatter;
+    if (elems_per_block) *elems_per_block = ctx->teams;
+    return TF_OK;
+}
+
+int tf_autotune(tf_ctx* ctx, const double* x_n, double dt) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!x_n || !(dt > 0)) return TF_ERR_ARGUMENT;
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(cudaMemcpyAsync(ctx->uk.p, x_n, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->un.p, x_n, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    const int teams_opts[3] = {8, 16, 32};
+    float best = 1e30f;
+    int best_sc = TF_SCATTER_ATOMIC, best_t = 32;
+    for (int sc = TF_SCATTER_ATOMIC; sc <= TF_SCATTER_COLOURED; ++sc) {
+        if (sc == TF_SCATTER_COLOURED && ctx->n_colours == 0) continue;
+        if (ctx->params.scatter != TF_SCATTER_AUTO && sc != ctx->params.scatter) continue;
+        for (int t : teams_opts) {
+            if (ctx->params.elems_per_block > 0 && t != ctx->params.elems_per_block) continue;
+            std::vector<float> times;
+            for (int rep = 0; rep < 6; ++rep) {
+                TF_CK(cudaMemsetAsync(ctx->vals.p, 0, sizeof(double) * 9 * (size_t)ctx->nnzb, ctx->stream));
+                TF_CK(cudaMemsetAsync(ctx->g.p, 0, bytes, ctx->stream));
+                TF_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+                TF_CK(launch_elements(ctx, dt, sc, t));
+                TF_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+                TF_CK(cudaEventSynchronize(ctx->ev[1]));
+                float ms;
+                TF_CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+                if (rep > 0) times.push_back(ms);
+            }
+            std::sort(times.begin(), times.end());
+            const float med = times[times.size() / 2];
+            if (med < best) {
+                best = med;
+                best_sc = sc;
+                best_t = t;
+            }
+        }
+    }
+    ctx->scatter = best_sc;
+    ctx->teams = best_t;
+    ctx->tuned = true;
+    return TF_OK;
+}
+
+int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_spmv) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (reps <= 0) return TF_ERR_ARGUMENT;
+    const double dt = 60.0;
+    float ms = 0.0f;
+    double tot = 0.0;
+    for (int rep = 0; rep < reps; ++rep) {
+        TF_CK(cudaMemsetAsync(ctx->vals.p, 0, sizeof(double) * 9 * (size_t)ctx->nnzb, ctx->stream));
+        TF_CK(cudaMemsetAsync(ctx->g.p, 0, sizeof(double) * 3 * (size_t)ctx->N, ctx->stream));
+        TF_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+        TF_CK(launch_elements(ctx, dt, ctx->scatter, ctx->teams));
+        TF_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        TF_CK(cudaEventSynchronize(ctx->ev[1]));
+        TF_CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        tot += ms;
+    }
+    if (ms_element) *ms_element = tot / reps;
+    KrylovWork w = make_work(ctx);
+    tot = 0.0;
+    for (int rep = 0; rep < reps; ++rep) {
+        TF_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+        TF_CK(launch_spmv(w, dptr<double>(ctx->uk), dptr<double>(ctx->xio), ctx->stream));
+        TF_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        TF_CK(cudaEventSynchronize(ctx->ev[1]));
+        TF_CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        tot += ms;
+    }
+    if (ms_spmv) *ms_spmv = tot / reps;
+    return TF_OK;
+}
+
+const char* tf_last_error(tf_ctx* ctx) { return ctx ? ctx->last_error : "null context"; }
+
+}  // extern "C"

@@ -1,0 +1,133 @@
+// tf_internal.cuh -- device data model and kernel entry points of the B200 Newton step.
+//
+// Layout in HBM (one tissue):
+//   nodes     : positions uk / un / x_out as [N][3] doubles (DoF 3*node+dim, gathered by
+//               elements), fixed mask [N] (bit d = FixedPos[d]), drag coefficient inputs.
+//   elements  : one 416-byte record per prism (ElemRecord) in the mesh's own order, so a team
+//               of threads reads a whole record with a few coalesced loads whether it is
+//               reached directly (atomic scatter) or through the colour permutation.
+//   Jacobian  : BSR3 - rowptr [N+1], colidx [nnzb], vals [nnzb][3][3] row-major blocks.
+//   Krylov    : eight [N][3] work vectors + the 3x3 inverse diagonal [N][9].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tfb {
+
+// One prism, 416 bytes (13 x 32-byte sectors). slots[a*6+b] is the BSR block index of
+// block (conn[a], conn[b]) in block row conn[a]; -1 for elements that touch a slave DoF
+// (those take the routed slow path).
+struct __align__(16) ElemRecord {
+    int32_t conn[6];
+    int32_t slots[36];
+    int32_t flags;  // bit0: element touches a slave DoF (slave-master routing needed)
+    int32_t pad0;
+    double xref[18];
+    double inv_fg[9];
+    double lam, mu, eta;
+};
+static_assert(sizeof(ElemRecord) == 416, "element record must stay 416 bytes");
+
+constexpr int kElemWords = sizeof(ElemRecord) / 8;  // 52 doubles
+
+// Device scalars of one BiCGStab solve. All updates happen on the device; the host only
+// polls `status` between chunks of iterations.
+struct KrylovScalars {
+    double rho_prev, rho, alpha, omega;
+    double bb, rr, tol2, du2;
+    int32_t iter, max_iter, status, finish;
+    uint32_t ticket[6];
+    int32_t pad[2];
+};
+
+enum KrylovStatus : int32_t {
+    KS_RUNNING = 0,
+    KS_CONVERGED = 1,
+    KS_MAXIT = 2,
+    KS_BREAKDOWN = 3,
+    KS_NONFINITE = 4,
+};
+
+// Device-side error / outcome bits written by kernels.
+enum DeviceFlags : int32_t {
+    DF_INVERTED = 1,      // det(Fe) <= 0 somewhere
+    DF_NONFINITE = 2,     // non-finite value produced
+    DF_PATTERN_MISS = 4,  // routed entry had no block in the pattern (never expected)
+    DF_SINGULAR_DIAG = 8  // a diagonal 3x3 block was singular
+};
+
+struct AssembleArgs {
+    const ElemRecord* elems;
+    const int32_t* elem_list;  // NULL: element i of the launch is elems[e_begin+i]
+    int32_t e_begin, e_count;
+    const double* uk;          // [N][3]
+    const double* un;          // [N][3]
+    double inv_dt;
+    const uint8_t* fixmask;    // [N]
+    const int32_t* dofmap;     // [3N] routed DoF (identity when no binding)
+    const int32_t* rowptr;
+    const int32_t* colidx;
+    double* vals;              // [nnzb][9]
+    double* g;                 // [3N]
+    int32_t* dflags;
+};
+
+struct NodeArgs {
+    int32_t n_nodes;
+    const double* uk;
+    const double* un;
+    double dt;
+    const uint8_t* fixmask;
+    const double* ext_visc;      // [3N]
+    const double* visc_surface;  // [N]
+    const int32_t* dofmap;
+    const int32_t* diag;         // [N] slot of the diagonal block
+    const int32_t* rowptr;
+    const int32_t* colidx;
+    double* vals;
+    double* g;
+    int32_t* dflags;
+};
+
+// --- element assembly (tf_element.cu) ---------------------------------------------------
+// mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class)
+cudaError_t launch_element_assemble(const AssembleArgs& a, int teams, bool visc, int mode,
+                                    cudaStream_t s);
+cudaError_t launch_node_terms(const NodeArgs& a, cudaStream_t s);
+
+// --- growth prologue (tf_element.cu) ------------------------------------------------------
+cudaError_t launch_grow(ElemRecord* elems, int32_t n_elems, const double* x, double* fg,
+                        const double* rates, const double* angles, double dt, int32_t* rotated,
+                        cudaStream_t s);
+cudaError_t launch_viscosity_surface(const ElemRecord* elems, int32_t n_elems, int32_t n_nodes,
+                                     const double* x, const uint8_t* exposed,
+                                     const uint8_t* peripodial, double* visc_surface,
+                                     cudaStream_t s);
+
+// --- Krylov (tf_krylov.cu) ----------------------------------------------------------------
+struct KrylovWork {
+    int32_t n_nodes;
+    const int32_t* rowptr;
+    const int32_t* colidx;
+    const int32_t* diag;
+    const double* vals;
+    double *x, *b;                      // solution du, right-hand side g
+    double *r, *rhat, *p, *v, *s, *t, *phat, *shat;
+    double* dinv;                       // [N][9]
+    double* partials;                   // reduction scratch
+    int32_t n_partials;                 // capacity in doubles
+    KrylovScalars* sc;
+    int32_t* dflags;
+};
+
+cudaError_t launch_block_jacobi_setup(const KrylovWork& w, cudaStream_t s);
+cudaError_t launch_krylov_init(const KrylovWork& w, double rtol, int max_iter, cudaStream_t s);
+cudaError_t launch_bicgstab_iteration(const KrylovWork& w, cudaStream_t s);
+cudaError_t launch_spmv(const KrylovWork& w, const double* xin, double* yout, cudaStream_t s);
+cudaError_t launch_newton_update(const KrylovWork& w, double* uk, const int32_t* slaves,
+                                 const int32_t* masters, int32_t n_pairs, cudaStream_t s);
+int spmv_grid(int n_nodes);
+int vec_grid(int n_nodes);
+
+}  // namespace tfb

@@ -1,0 +1,183 @@
+"""Host-side mirror of TissueOrigami's NewtonRaphsonSolver over the B200 C ABI.
+
+``NewtonRaphsonSolver`` keeps the reference's vocabulary (TissueFolding/SourceCode/
+NewtonRaphsonSolver.h:51-91, Simulation.cpp:6605-6747): one object per tissue that owns the
+device state, is fed the node and element data the reference keeps in ``Node`` / ``ShapeBase``
+and performs ``updateStepNR`` or a whole ``runOneStep`` prologue + Newton step. All work runs
+in the CUDA library; a missing library or GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import capi
+from .mesh import Tissue
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class NewtonRaphsonSolver:
+    """One tissue on one GPU (``NewtonRaphsonSolver`` + the element and node state it reads)."""
+
+    def __init__(self, conn, xref, n_nodes: int, params: Optional[capi.Params] = None, **overrides):
+        L = capi.load()
+        self._L = L
+        self.n_nodes = int(n_nodes)
+        self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, 6)
+        self.xref = _f64(xref).reshape(-1, 18)
+        self.n_elems = self.conn.shape[0]
+        p = params if params is not None else capi.default_params()
+        for k, v in overrides.items():
+            setattr(p, k, v)
+        self.params = p
+        desc = capi.MeshDesc(self.n_nodes, self.n_elems, capi.iptr(self.conn), capi.dptr(self.xref))
+        h = ctypes.c_void_p()
+        capi.check(L.tf_create(ctypes.byref(desc), ctypes.byref(p), ctypes.byref(h)), "tf_create")
+        self._h = h
+        self.last_stats = None
+
+    # -- construction from a synthetic / loaded tissue ---------------------------------------
+    @classmethod
+    def from_tissue(cls, t: Tissue, params: Optional[capi.Params] = None, **overrides):
+        overrides.setdefault("newton_tol", t.newton_tol)
+        s = cls(t.conn, t.xref, t.n_nodes, params, **overrides)
+        s.set_material(t.lam, t.mu, t.eta)
+        s.set_boundary(t.fixed, t.ext_visc, t.slave_master)
+        s.set_growth(t.fg, t.rates, t.angles, t.exposed, t.peripodial)
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.tf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state setters (Node / ShapeBase fields) ----------------------------------------------
+    def set_material(self, lam, mu, eta=None):
+        eta_a = _f64(eta) if eta is not None else None
+        capi.check(self._L.tf_set_material(self._h, capi.dptr(_f64(lam)), capi.dptr(_f64(mu)), capi.dptr(eta_a)),
+                   "tf_set_material", self._h)
+
+    def set_inv_fg(self, inv_fg):
+        capi.check(self._L.tf_set_inv_fg(self._h, capi.dptr(_f64(inv_fg).reshape(-1))), "tf_set_inv_fg", self._h)
+
+    def set_boundary(self, fixed, ext_visc, slave_master=None):
+        sm = np.ascontiguousarray(slave_master if slave_master is not None else np.zeros((0, 2)), dtype=np.int32).reshape(-1)
+        fx = np.ascontiguousarray(fixed, dtype=np.uint8).reshape(-1)
+        capi.check(self._L.tf_set_boundary(self._h, capi.uptr(fx), capi.dptr(_f64(ext_visc).reshape(-1)),
+                                           capi.iptr(sm) if sm.size else None, sm.size // 2),
+                   "tf_set_boundary", self._h)
+
+    def set_viscosity_surface(self, visc_surface):
+        capi.check(self._L.tf_set_viscosity_surface(self._h, capi.dptr(_f64(visc_surface))),
+                   "tf_set_viscosity_surface", self._h)
+
+    def set_growth(self, fg=None, rates=None, angles=None, exposed=None, peripodial=None):
+        capi.check(self._L.tf_set_growth(
+            self._h,
+            capi.dptr(_f64(fg).reshape(-1)) if fg is not None else None,
+            capi.dptr(_f64(rates).reshape(-1)) if rates is not None else None,
+            capi.dptr(_f64(angles)) if angles is not None else None,
+            capi.uptr(np.ascontiguousarray(exposed, dtype=np.uint8)) if exposed is not None else None,
+            capi.uptr(np.ascontiguousarray(peripodial, dtype=np.uint8)) if peripodial is not None else None),
+            "tf_set_growth", self._h)
+
+    def get_growth(self):
+        fg = np.zeros((self.n_elems, 9))
+        inv = np.zeros((self.n_elems, 9))
+        capi.check(self._L.tf_get_growth(self._h, capi.dptr(fg), capi.dptr(inv)), "tf_get_growth", self._h)
+        return fg, inv
+
+    # -- the path -------------------------------------------------------------------------------
+    def updateStepNR(self, x_n, dt: float):
+        """Simulation::updateStepNR: returns (positions, status, stats dict)."""
+        x = _f64(x_n).reshape(self.n_nodes, 3).copy()
+        out = np.empty_like(x)
+        st = capi.StepStats()
+        rc = capi.check(self._L.tf_newton_step(self._h, capi.dptr(x), float(dt), capi.dptr(out), ctypes.byref(st)),
+                        "tf_newton_step", self._h)
+        self.last_stats = st.as_dict()
+        return out, rc, self.last_stats
+
+    def runOneStep(self, x_n, dt: float):
+        """Growth prologue + viscosity surfaces + updateStepNR (Simulation::runOneStep subset)."""
+        x = _f64(x_n).reshape(self.n_nodes, 3).copy()
+        out = np.empty_like(x)
+        st = capi.StepStats()
+        rc = capi.check(self._L.tf_time_step(self._h, capi.dptr(x), float(dt), capi.dptr(out), ctypes.byref(st)),
+                        "tf_time_step", self._h)
+        self.last_stats = st.as_dict()
+        return out, rc, self.last_stats
+
+    def pattern(self):
+        nnzb = ctypes.c_int32()
+        self._L.tf_get_pattern(self._h, ctypes.byref(nnzb), None, None)
+        rowptr = np.zeros(self.n_nodes + 1, np.int32)
+        colidx = np.zeros(nnzb.value, np.int32)
+        self._L.tf_get_pattern(self._h, None, capi.iptr(rowptr), capi.iptr(colidx))
+        return rowptr, colidx
+
+    def assemble(self, uk, un, dt: float, want_matrix: bool = True):
+        """One Newton iteration's residual gSum and Jacobian J = K^T (BSR3 values)."""
+        rowptr, colidx = self.pattern()
+        g = np.zeros(3 * self.n_nodes)
+        vals = np.zeros((colidx.shape[0], 3, 3)) if want_matrix else None
+        rc = capi.check(self._L.tf_assemble(self._h, capi.dptr(_f64(uk).reshape(-1)), capi.dptr(_f64(un).reshape(-1)),
+                                            float(dt), capi.dptr(g), capi.dptr(vals)), "tf_assemble", self._h)
+        return g, vals, rowptr, colidx, rc
+
+    def solveForDeltaU(self, vals, g):
+        """Solve J du = g on the context's pattern (NewtonRaphsonSolver::solveForDeltaU)."""
+        du = np.zeros(3 * self.n_nodes)
+        it = ctypes.c_int32()
+        rr = ctypes.c_double()
+        rc = capi.check(self._L.tf_solve(self._h, capi.dptr(_f64(vals).reshape(-1)), capi.dptr(_f64(g)), capi.dptr(du),
+                                         ctypes.byref(it), ctypes.byref(rr)), "tf_solve", self._h)
+        return du, rc, it.value, rr.value
+
+    def schedule(self):
+        nc, sc, t = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._L.tf_get_schedule(self._h, ctypes.byref(nc), ctypes.byref(sc), ctypes.byref(t))
+        return {"n_colours": nc.value, "scatter": sc.value, "elems_per_block": t.value}
+
+    def autotune(self, x_n, dt: float):
+        capi.check(self._L.tf_autotune(self._h, capi.dptr(_f64(x_n).reshape(-1)), float(dt)), "tf_autotune", self._h)
+        return self.schedule()
+
+    def time_kernels(self, reps: int = 20):
+        me, ms = ctypes.c_double(), ctypes.c_double()
+        capi.check(self._L.tf_time_kernels(self._h, int(reps), ctypes.byref(me), ctypes.byref(ms)), "tf_time_kernels", self._h)
+        return me.value, ms.value
+
+
+def simulate(t: Tissue, n_steps: Optional[int] = None, solver: Optional[NewtonRaphsonSolver] = None, **overrides):
+    """Run n time steps of the path on the GPU; returns (positions, per-step stats)."""
+    own = solver is None
+    s = solver or NewtonRaphsonSolver.from_tissue(t, **overrides)
+    try:
+        x = np.array(t.x, dtype=np.float64, copy=True)
+        stats = []
+        for _ in range(n_steps if n_steps is not None else t.n_steps):
+            x, rc, st = s.runOneStep(x, t.dt)
+            st["rc"] = rc
+            stats.append(st)
+        return x, stats
+    finally:
+        if own:
+            s.close()
