@@ -18,7 +18,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -126,11 +125,17 @@ class ClockSampler:
     def start(self):
         try:
             cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
-            if self.bus_id:
-                cmd += ["-i", self.bus_id]
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+
+    def _mine(self, bus: str) -> bool:
+        """nvidia-smi lists every GPU of the host; keep the rows of the GPU this rank uses."""
+        if not self.bus_id:
+            return True
+        a = bus.lower().split(":")
+        b = self.bus_id.lower().split(":")
+        return a[-2:] == b[-2:]
 
     def stop(self):
         if not self.proc:
@@ -146,7 +151,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in out.splitlines():
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 10:
+            if len(f) < 10 or not self._mine(f[1]):
                 continue
             try:
                 sm.append(float(f[2]))
@@ -209,7 +214,8 @@ def run_b200(args) -> None:
 
     bus = None
     try:
-        bus = torch.cuda.get_device_properties(local).pci_bus_id
+        p = torch.cuda.get_device_properties(local)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
     except Exception:
         bus = None
     clocks = ClockSampler(bus)
@@ -217,6 +223,8 @@ def run_b200(args) -> None:
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.cudart().cudaProfilerStart()
     ms, iters, kry, launches, worst = 0.0, 0, 0, 0, 0
     for _ in range(args.steps):
         flush.zero_()  # L2 flush between timed steps (outside the step's event window)
@@ -228,6 +236,8 @@ def run_b200(args) -> None:
         launches += st.gpu_launches
         worst = max(worst, rc)
     torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.cudart().cudaProfilerStop()
     if dist:
         dist.barrier()
     clk = clocks.stop()
@@ -345,6 +355,8 @@ def main():
     ap.add_argument("--workload", default="wing_disc")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

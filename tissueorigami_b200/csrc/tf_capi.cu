@@ -475,8 +475,10 @@ int read_flags(tf_ctx* ctx) {
     return TF_OK;
 }
 
+// Most severe of two outcomes: errors first, then non-finite values, then the rest by code.
 int worse(int a, int b) {
     if (a < 0 || b < 0) return std::min(a, b);
+    if (a == TF_NONFINITE || b == TF_NONFINITE) return TF_NONFINITE;
     return std::max(a, b);
 }
 
@@ -510,7 +512,10 @@ int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
         st->ms_solve += ms;
         const int ks = krylov_status_to_tf(sc.status);
         if (ks != TF_OK) status = worse(status, ks);
-        if (*ctx->h_flags & DF_INVERTED) status = worse(status, TF_ELEMENT_INVERTED);
+        if (*ctx->h_flags & DF_NONFINITE)
+            status = worse(status, TF_NONFINITE);
+        else if (*ctx->h_flags & DF_INVERTED)
+            status = worse(status, TF_ELEMENT_INVERTED);
         if (*ctx->h_flags & DF_PATTERN_MISS) return set_error(ctx, TF_ERR_STATE, "routed entry outside the pattern");
         const double d = std::sqrt(ctx->h_sc->du2);
         if (iteratorK < 32) {
@@ -813,6 +818,7 @@ int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, doub
     rc = read_flags(ctx);
     if (rc != TF_OK) return rc;
     if (*ctx->h_flags & DF_PATTERN_MISS) return set_error(ctx, TF_ERR_STATE, "routed entry outside the pattern");
+    if (*ctx->h_flags & DF_NONFINITE) return TF_NONFINITE;
     return (*ctx->h_flags & DF_INVERTED) ? TF_ELEMENT_INVERTED : TF_OK;
 }
 

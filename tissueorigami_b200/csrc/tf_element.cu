@@ -164,7 +164,10 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
         mm3(F, Fg, Fe);
         const double detF = det3(F);
         const double Je = det3(Fe);
-        if (!(Je > 0.0)) atomicOr(A.dflags, DF_INVERTED);
+        if (isnan(Je))
+            atomicOr(A.dflags, DF_NONFINITE);
+        else if (!(Je > 0.0))
+            atomicOr(A.dflags, DF_INVERTED);
         const double lnJ = log(Je);
         const double dv = detF * detdX * kGaussWeight;
         const double iJe = 1.0 / Je;
