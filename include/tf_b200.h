@@ -41,6 +41,10 @@ extern "C" {
 #define TF_ERR_OUT_OF_MEMORY (-3)
 #define TF_ERR_STATE (-4)
 #define TF_ERR_UNSUPPORTED (-5)
+#define TF_ERR_TOO_LARGE (-6) /* system larger than tf_solve_bsr_noalloc's fixed scratch   */
+
+/* Largest system (block rows) tf_solve_bsr_noalloc accepts. */
+#define TF_NOALLOC_MAX_NODES 16384
 
 /* ---- options ------------------------------------------------------------------------- */
 #define TF_PRECOND_BLOCK_JACOBI 0 /* 3x3 node-block inverse of the diagonal               */
@@ -192,6 +196,25 @@ int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_sp
 
 /* Text of the last error recorded on the context (no reference counterpart). */
 const char* tf_last_error(tf_ctx* ctx);
+
+/* No counterpart in the reference. The linear solve of tf_solve (block-Jacobi BiCGStab on
+ * J du = g) for callers that cannot allocate GPU memory: hosts that give all device memory to
+ * their own allocator or to a pool fixed at start-up, and therefore cannot let a library call
+ * cudaMalloc / cudaFree. Every pointer is a DEVICE pointer the caller owns: the BSR3 pattern
+ * (rowptr [n_nodes+1], colidx [nnzb], every row holding its diagonal block), the values
+ * vals [nnzb*9], the right-hand side g and the solution du [n_nodes*3]. The work vectors live
+ * in one fixed __device__ array inside the library (about 4.5 MB, held by every GPU that
+ * loads the library until the process exits), so n_nodes may not exceed
+ * TF_NOALLOC_MAX_NODES; larger systems return TF_ERR_TOO_LARGE before any GPU work. The first
+ * call on a device looks up that array's address with cudaGetSymbolAddress (that device must
+ * be current) and should come before any stream capture on it. Calls share the array: ones
+ * that overlap on the GPU race, so serialise them. stream is a cudaStream_t passed as a
+ * pointer (NULL: the legacy default stream); the call returns after the solve has finished.
+ * The call makes no cudaMalloc, cudaFree or other allocating call. Returns the status codes
+ * of tf_solve; iters / rel_res may be NULL. */
+int tf_solve_bsr_noalloc(int32_t n_nodes, const int32_t* d_rowptr, const int32_t* d_colidx,
+                         const double* d_vals, const double* d_g, double* d_du, double rtol,
+                         int32_t max_iters, void* stream, int32_t* iters, double* rel_res);
 
 #ifdef __cplusplus
 }

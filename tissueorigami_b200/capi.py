@@ -24,6 +24,8 @@ TF_ERR_CUDA = -2
 TF_ERR_OUT_OF_MEMORY = -3
 TF_ERR_STATE = -4
 TF_ERR_UNSUPPORTED = -5
+TF_ERR_TOO_LARGE = -6
+TF_NOALLOC_MAX_NODES = 16384
 
 TF_PRECOND_BLOCK_JACOBI = 0
 TF_PRECOND_ILU0 = 1
@@ -34,7 +36,7 @@ TF_SCATTER_COLOURED = 2
 STATUS_NAMES = {
     0: "ok", 1: "newton_not_converged", 2: "krylov_max_iters", 3: "krylov_breakdown",
     4: "nonfinite", 5: "element_inverted", -1: "argument", -2: "cuda", -3: "out_of_memory",
-    -4: "state", -5: "unsupported",
+    -4: "state", -5: "unsupported", -6: "too_large",
 }
 
 # Every entry point include/tf_b200.h declares (checked by the CPU test suite).
@@ -43,7 +45,7 @@ EXPORTS = [
     "tf_set_inv_fg", "tf_set_boundary", "tf_set_viscosity_surface", "tf_newton_step",
     "tf_newton_step_device", "tf_get_pattern", "tf_assemble", "tf_solve", "tf_set_growth",
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
-    "tf_time_kernels", "tf_last_error",
+    "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc",
 ]
 
 
@@ -122,6 +124,7 @@ def load(build_if_missing: bool = True):
     L.tf_get_schedule.argtypes = [_P, _I, _I, _I]
     L.tf_autotune.argtypes = [_P, _D, c_double]
     L.tf_time_kernels.argtypes = [_P, c_int, _D, _D]
+    L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:

@@ -121,6 +121,8 @@ struct KrylovWork {
     int32_t* dflags;
 };
 
+cudaError_t launch_find_diag(const int32_t* rowptr, const int32_t* colidx, int32_t n, int32_t* diag,
+                             int32_t* dflags, cudaStream_t s);
 cudaError_t launch_block_jacobi_setup(const KrylovWork& w, cudaStream_t s);
 cudaError_t launch_krylov_init(const KrylovWork& w, double rtol, int max_iter, cudaStream_t s);
 cudaError_t launch_bicgstab_iteration(const KrylovWork& w, cudaStream_t s);

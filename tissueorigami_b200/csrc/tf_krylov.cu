@@ -273,6 +273,31 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv(KrylovWork w, const doubl
     }
 }
 
+// Slot of the diagonal block of every block row (binary search of the sorted column list).
+__global__ void k_find_diag(const int32_t* rowptr, const int32_t* colidx, int32_t n, int32_t* diag,
+                            int32_t* dflags) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int lo = rowptr[r], hi = rowptr[r + 1] - 1, found = -1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int c = colidx[mid];
+        if (c == r) {
+            found = mid;
+            break;
+        }
+        if (c < r)
+            lo = mid + 1;
+        else
+            hi = mid - 1;
+    }
+    if (found < 0) {
+        atomicOr(dflags, DF_PATTERN_MISS);
+        found = rowptr[r];  // keep the index in range; the flag reports the missing diagonal
+    }
+    diag[r] = found;
+}
+
 // du[slave] = du[master] (equateSlaveDisplacementsToMasters), then uk += du and ||du||^2.
 __global__ void k_equate_slaves(double* du, const int32_t* slaves, const int32_t* masters, int32_t n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -301,6 +326,12 @@ int spmv_grid(int n_nodes) {
     const int rows_per_cta = kSpmvThreads / kGroup;
     const int g = (n_nodes + rows_per_cta - 1) / rows_per_cta;
     return g < 1 ? 1 : g;
+}
+
+cudaError_t launch_find_diag(const int32_t* rowptr, const int32_t* colidx, int32_t n, int32_t* diag,
+                             int32_t* dflags, cudaStream_t s) {
+    k_find_diag<<<(n + 255) / 256, 256, 0, s>>>(rowptr, colidx, n, diag, dflags);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_block_jacobi_setup(const KrylovWork& w, cudaStream_t s) {
