@@ -75,6 +75,8 @@ typedef struct tf_params {
     int32_t elems_per_block;  /* element-kernel teams per CTA: 0 = autotuned                */
     int32_t device;           /* CUDA device ordinal                                        */
     int32_t use_graphs;       /* capture the Krylov iteration in a CUDA graph (1) or not    */
+    int32_t persistent;       /* whole solve in one cooperative persistent kernel (1) or    */
+                              /* graph-replayed chunks of iteration kernels (0)             */
 } tf_params;
 
 typedef struct tf_step_stats {
@@ -91,7 +93,8 @@ typedef struct tf_step_stats {
 } tf_step_stats;
 
 /* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), BiCGStab
- * rtol 1e-12 with cap 20000, block-Jacobi, autotuned scatter, device 0, graphs on. */
+ * rtol 1e-12 with cap 20000, block-Jacobi, autotuned scatter, device 0, graphs on,
+ * persistent solve on. */
 void tf_default_params(tf_params* p);
 
 /* Library version string. */

@@ -59,7 +59,7 @@ class Params(ctypes.Structure):
                 ("krylov_max_iters", ctypes.c_int32), ("krylov_rtol", ctypes.c_double),
                 ("precond", ctypes.c_int32), ("scatter", ctypes.c_int32),
                 ("elems_per_block", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("use_graphs", ctypes.c_int32)]
+                ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):

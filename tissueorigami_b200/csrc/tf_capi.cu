@@ -63,7 +63,8 @@ struct tf_ctx {
     DevBuf elems, fixmask, ext_visc, visc_surface, dofmap_d, slaves_d, masters_d;
     DevBuf rowptr_d, colidx_d, diag_d, vals, colour_list_d;
     DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
-    DevBuf fg, rates, angles, exposed, peripodial, rotated, xio;
+    DevBuf fg, rates, angles, exposed, peripodial, rotated, xio, barrier;
+    int persistent_grid_max = 0;  // 0: cooperative launch unavailable
     KrylovScalars* h_sc = nullptr;  // pinned
     int32_t* h_flags = nullptr;     // pinned
 
@@ -327,7 +328,8 @@ int upload_structure(tf_ctx* ctx) {
         TF_CK(cudaMemcpy(ctx->slaves_d.p, ctx->slave.data(), sizeof(int32_t) * ctx->slave.size(), cudaMemcpyHostToDevice));
         TF_CK(cudaMemcpy(ctx->masters_d.p, ctx->master.data(), sizeof(int32_t) * ctx->master.size(), cudaMemcpyHostToDevice));
     }
-    const size_t np2 = (size_t)std::max(spmv_grid(N), vec_grid(N)) * 2 + 64;
+    const size_t np2 = std::max((size_t)std::max(spmv_grid(N), vec_grid(N)) * 2,
+                                (size_t)ctx->persistent_grid_max * 4) + 64;
     TF_CK(dalloc(ctx->partials, sizeof(double) * np2));
     if (ctx->krylov_graph) {
         cudaGraphExecDestroy(ctx->krylov_graph);
@@ -441,6 +443,21 @@ int krylov_status_to_tf(int ks) {
 // Solve J du = g (buffers in the context). Leaves the scalars in ctx->h_sc.
 int krylov_solve(tf_ctx* ctx) {
     KrylovWork w = make_work(ctx);
+    if (ctx->params.persistent && ctx->persistent_grid_max > 0) {
+        const int grid = persistent_grid(ctx->N, ctx->persistent_grid_max);
+        TF_CK(launch_bicgstab_persistent(w, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
+                                         dptr<GridBarrier>(ctx->barrier), grid, ctx->stream));
+        ctx->launches += 1;
+        TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->h_flags, ctx->dflags.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        TF_CK(cudaStreamSynchronize(ctx->stream));
+        if (*ctx->h_flags & DF_BARRIER_TIMEOUT) {
+            TF_CK(cudaMemsetAsync(ctx->barrier.p, 0, sizeof(GridBarrier), ctx->stream));
+            TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+            return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
+        }
+        return TF_OK;
+    }
     TF_CK(launch_block_jacobi_setup(w, ctx->stream));
     TF_CK(launch_krylov_init(w, ctx->params.krylov_rtol, ctx->params.krylov_max_iters, ctx->stream));
     ctx->launches += 2;
@@ -603,6 +620,7 @@ void tf_default_params(tf_params* p) {
     p->elems_per_block = 0;
     p->device = 0;
     p->use_graphs = 1;
+    p->persistent = 1;
 }
 
 const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
@@ -649,6 +667,13 @@ int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
     TF_CK(dalloc(ctx->exposed, E));
     TF_CK(dalloc(ctx->peripodial, E));
     TF_CK(dalloc(ctx->rotated, sizeof(int32_t) * E));
+    TF_CK(dalloc(ctx->barrier, sizeof(GridBarrier)));
+    TF_CK(cudaMemset(ctx->barrier.p, 0, sizeof(GridBarrier)));
+    {
+        int coop = 0;
+        TF_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+        ctx->persistent_grid_max = coop ? persistent_max_grid(ctx->device) : 0;
+    }
     TF_CK(cudaMemset(ctx->sc.p, 0, sizeof(KrylovScalars)));
     TF_CK(cudaMemset(ctx->fixmask.p, 0, N));
     TF_CK(cudaMemset(ctx->ext_visc.p, 0, sizeof(double) * n3));
@@ -685,7 +710,7 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->vals, &ctx->colour_list_d, &ctx->uk, &ctx->un, &ctx->g, &ctx->du, &ctx->r,
                      &ctx->rhat, &ctx->p, &ctx->v, &ctx->s, &ctx->t, &ctx->phat, &ctx->shat, &ctx->dinv,
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
-                     &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio};
+                     &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier};
     for (DevBuf* b : all) dfree(*b);
     if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);

@@ -54,7 +54,14 @@ enum DeviceFlags : int32_t {
     DF_INVERTED = 1,      // det(Fe) <= 0 somewhere
     DF_NONFINITE = 2,     // non-finite value produced
     DF_PATTERN_MISS = 4,  // routed entry had no block in the pattern (never expected)
-    DF_SINGULAR_DIAG = 8  // a diagonal 3x3 block was singular
+    DF_SINGULAR_DIAG = 8,   // a diagonal 3x3 block was singular
+    DF_BARRIER_TIMEOUT = 16 // a persistent kernel's grid barrier gave up waiting
+};
+
+// Generation-counting grid barrier state of a cooperative launch (zero-initialised).
+struct GridBarrier {
+    uint32_t count;
+    uint32_t gen;
 };
 
 struct AssembleArgs {
@@ -130,6 +137,11 @@ cudaError_t launch_spmv(const KrylovWork& w, const double* xin, double* yout, cu
 cudaError_t launch_newton_update(const KrylovWork& w, double* uk, const int32_t* slaves,
                                  const int32_t* masters, int32_t n_pairs, cudaStream_t s);
 int spmv_grid(int n_nodes);
+// Persistent cooperative BiCGStab: partials must hold 4 * grid doubles.
+int persistent_max_grid(int device);
+int persistent_grid(int n_nodes, int max_grid);
+cudaError_t launch_bicgstab_persistent(const KrylovWork& w, double rtol, int max_iter, GridBarrier* bar, int grid,
+                                       cudaStream_t s);
 int vec_grid(int n_nodes);
 
 }  // namespace tfb

@@ -24,6 +24,7 @@ namespace {
 constexpr int kVecThreads = 256;
 constexpr int kSpmvThreads = 256;
 constexpr int kGroup = 8;  // lanes per block row in the SpMV
+constexpr int kPersistThreads = 256;
 
 __device__ __forceinline__ bool running(const KrylovScalars* sc) {
     return *reinterpret_cast<const volatile int32_t*>(&sc->status) == KS_RUNNING;
@@ -92,6 +93,21 @@ __device__ __forceinline__ void apply_dinv(const double* dinv, int n, const doub
     out[n * 3 + 0] = D[0] * a + D[1] * b + D[2] * c;
     out[n * 3 + 1] = D[3] * a + D[4] * b + D[5] * c;
     out[n * 3 + 2] = D[6] * a + D[7] * b + D[8] * c;
+}
+
+// Partial row product of one lane: blocks k0, k0+G, ... of the row. x is read through L2
+// (ld.cg): inside a persistent kernel it was written by other CTAs.
+template <int G>
+__device__ __forceinline__ void row_dot(const KrylovWork& w, int k0, int k1, const double* __restrict__ xin,
+                                        double& y0, double& y1, double& y2) {
+    for (int k = k0; k < k1; k += G) {
+        const int c = __ldg(w.colidx + k);
+        const double* B = w.vals + (size_t)k * 9;
+        const double x0 = __ldcg(xin + c * 3), x1 = __ldcg(xin + c * 3 + 1), x2 = __ldcg(xin + c * 3 + 2);
+        y0 += __ldg(B + 0) * x0 + __ldg(B + 1) * x1 + __ldg(B + 2) * x2;
+        y1 += __ldg(B + 3) * x0 + __ldg(B + 4) * x1 + __ldg(B + 5) * x2;
+        y2 += __ldg(B + 6) * x0 + __ldg(B + 7) * x1 + __ldg(B + 8) * x2;
+    }
 }
 
 __global__ void k_block_jacobi(KrylovWork w) {
@@ -221,17 +237,7 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv(KrylovWork w, const doubl
     const int gl = threadIdx.x & (kGroup - 1);
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    if (row < w.n_nodes) {
-        const int k1 = __ldg(w.rowptr + row + 1);
-        for (int k = __ldg(w.rowptr + row) + gl; k < k1; k += kGroup) {
-            const int c = __ldg(w.colidx + k);
-            const double* B = w.vals + (size_t)k * 9;
-            const double x0 = __ldg(xin + c * 3), x1 = __ldg(xin + c * 3 + 1), x2 = __ldg(xin + c * 3 + 2);
-            y0 += __ldg(B + 0) * x0 + __ldg(B + 1) * x1 + __ldg(B + 2) * x2;
-            y1 += __ldg(B + 3) * x0 + __ldg(B + 4) * x1 + __ldg(B + 5) * x2;
-            y2 += __ldg(B + 6) * x0 + __ldg(B + 7) * x1 + __ldg(B + 8) * x2;
-        }
-    }
+    if (row < w.n_nodes) row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
 #pragma unroll
     for (int off = kGroup / 2; off > 0; off >>= 1) {
         y0 += __shfl_xor_sync(0xffffffffu, y0, off);
@@ -315,7 +321,288 @@ __global__ void k_newton_update(KrylovWork w, double* uk) {
     if (grid_sum<1>(v, w.partials, &w.sc->ticket[5], tot) && threadIdx.x == 0) w.sc->du2 = tot[0];
 }
 
+// ---- persistent cooperative solve -------------------------------------------------------
+//
+// k_bicgstab_persistent runs a whole block-Jacobi BiCGStab solve in one cooperative launch:
+// every CTA owns a contiguous range of block rows, the five phases of an iteration are
+// separated by a grid barrier, and each of the three reductions is summed by every CTA from
+// the same per-CTA partials in the same order, so all CTAs hold bit-identical scalars and take
+// the same convergence decision. The partials alternate between two buffers so a CTA can start
+// writing the next reduction while a slower one still reads the previous. The barrier is
+// bounded: a CTA that waits longer than kBarrierTimeoutCycles sets DF_BARRIER_TIMEOUT and the
+// kernel returns; co-residency is guaranteed by the cooperative launch, so this never fires
+// in a correct launch.
+// Barrier wait bound in SM clock cycles (~2 s at the B200 boost clock).
+constexpr long long kBarrierTimeoutCycles = 4000000000ll;
+
+__device__ bool grid_barrier(GridBarrier* bar, int32_t* dflags) {
+    __shared__ int ok;
+    if (gridDim.x == 1) {
+        __syncthreads();
+        return true;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile uint32_t* vgen = &bar->gen;
+        const uint32_t g = *vgen;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&bar->count, 1u);
+        if (arrived == gridDim.x - 1) {
+            bar->count = 0u;
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            unsigned polls = 0;
+            while (*vgen == g) {
+                if ((++polls & 255u) == 0u && clock64() - t0 > kBarrierTimeoutCycles) {
+                    atomicOr(dflags, DF_BARRIER_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        if (*reinterpret_cast<volatile int32_t*>(dflags) & DF_BARRIER_TIMEOUT) ok = 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Sum NDOT per-CTA partials of every CTA (same order in every CTA); all threads get the totals.
+template <int NDOT>
+__device__ void sum_partials(const double* buf, double (&tot)[NDOT], double* smem, double* sbcast) {
+    double acc[NDOT];
+#pragma unroll
+    for (int k = 0; k < NDOT; ++k) acc[k] = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NDOT; ++k) acc[k] += __ldcg(buf + i * NDOT + k);
+    block_sum<NDOT>(acc, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NDOT; ++k) sbcast[k] = acc[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NDOT; ++k) tot[k] = sbcast[k];
+    __syncthreads();
+}
+
+template <int NDOT>
+__device__ void write_partials(double (&v)[NDOT], double* buf, double* smem) {
+    block_sum<NDOT>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NDOT; ++k) buf[blockIdx.x * NDOT + k] = v[k];
+}
+
+// y = J x for rows [r0, r1) with kGroup lanes per row; returns this thread's share of the
+// dots (rhat,y) [KIND 1] or (s,y), (y,y) [KIND 2].
+template <int KIND>
+__device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, const double* __restrict__ xin,
+                                          double* __restrict__ yout, double& d0, double& d1) {
+    const int gl = threadIdx.x & (kGroup - 1);
+    const int groups = blockDim.x / kGroup;
+    for (int rb = r0; rb < r1; rb += groups) {
+        const int row = rb + threadIdx.x / kGroup;
+        double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+        if (row < r1) row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+#pragma unroll
+        for (int off = kGroup / 2; off > 0; off >>= 1) {
+            y0 += __shfl_xor_sync(0xffffffffu, y0, off);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, off);
+            y2 += __shfl_xor_sync(0xffffffffu, y2, off);
+        }
+        if (row < r1 && gl == 0) {
+            yout[row * 3 + 0] = y0;
+            yout[row * 3 + 1] = y1;
+            yout[row * 3 + 2] = y2;
+            if (KIND == 1) {
+                d0 += w.rhat[row * 3] * y0 + w.rhat[row * 3 + 1] * y1 + w.rhat[row * 3 + 2] * y2;
+            } else {
+                d0 += w.s[row * 3] * y0 + w.s[row * 3 + 1] * y1 + w.s[row * 3 + 2] * y2;
+                d1 += y0 * y0 + y1 * y1 + y2 * y2;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
+    const double* B = w.vals + (size_t)w.diag[n] * 9;
+    double m[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m[k] = B[k];
+    const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
+    double* D = w.dinv + (size_t)n * 9;
+    if (det == 0.0 || !isfinite(det)) {
+        atomicOr(w.dflags, DF_SINGULAR_DIAG);
+        for (int k = 0; k < 9; ++k) D[k] = (k % 4 == 0) ? 1.0 : 0.0;
+        return;
+    }
+    const double id = 1.0 / det;
+    D[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+    D[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    D[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    D[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    D[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    D[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    D[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    D[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+__global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovWork w, double rtol, int max_iter,
+                                                                         GridBarrier* bar) {
+    __shared__ double smem[32 * 2];
+    __shared__ double sb[2];
+    const int nb = gridDim.x;
+    const int r0 = (int)((long long)w.n_nodes * blockIdx.x / nb);
+    const int r1 = (int)((long long)w.n_nodes * (blockIdx.x + 1) / nb);
+    double* part[2] = {w.partials, w.partials + 2 * nb};
+    int pb = 0;
+    // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2
+    double v1[1] = {0.0};
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        block_jacobi_row(w, n);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            const double b = w.b[d];
+            w.x[d] = 0.0;
+            w.r[d] = b;
+            w.rhat[d] = b;
+            w.p[d] = 0.0;
+            w.v[d] = 0.0;
+            v1[0] += b * b;
+        }
+    }
+    write_partials<1>(v1, part[pb], smem);
+    if (!grid_barrier(bar, w.dflags)) return;
+    double t1[1], t2[2];
+    sum_partials<1>(part[pb], t1, smem, sb);
+    pb ^= 1;
+    const double bb = t1[0];
+    double rho = bb, rho_prev = 1.0, alpha = 1.0, omega = 1.0, rr = bb;
+    const double tol2 = rtol * rtol * bb;
+    int it = 0;
+    int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
+    while (status == KS_RUNNING) {
+        // A: p = r + beta (p - omega v); phat = D^-1 p
+        const double beta = (rho / rho_prev) * (alpha / omega);
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
+            }
+            apply_dinv(w.dinv, n, w.p, w.phat);
+        }
+        if (!grid_barrier(bar, w.dflags)) return;
+        // B: v = J phat; (rhat, v)
+        double d0 = 0.0, d1 = 0.0;
+        spmv_rows<1>(w, r0, r1, w.phat, w.v, d0, d1);
+        v1[0] = d0;
+        write_partials<1>(v1, part[pb], smem);
+        if (!grid_barrier(bar, w.dflags)) return;
+        sum_partials<1>(part[pb], t1, smem, sb);
+        pb ^= 1;
+        if (!isfinite(t1[0])) { status = KS_NONFINITE; break; }
+        if (t1[0] == 0.0) { status = KS_BREAKDOWN; break; }
+        alpha = rho / t1[0];
+        // C: s = r - alpha v; shat = D^-1 s
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.s[d] = w.r[d] - alpha * w.v[d];
+            }
+            apply_dinv(w.dinv, n, w.s, w.shat);
+        }
+        if (!grid_barrier(bar, w.dflags)) return;
+        // D: t = J shat; (t, s), (t, t)
+        d0 = 0.0;
+        d1 = 0.0;
+        spmv_rows<2>(w, r0, r1, w.shat, w.t, d0, d1);
+        double v2[2] = {d0, d1};
+        write_partials<2>(v2, part[pb], smem);
+        if (!grid_barrier(bar, w.dflags)) return;
+        sum_partials<2>(part[pb], t2, smem, sb);
+        pb ^= 1;
+        if (!isfinite(t2[0]) || !isfinite(t2[1])) { status = KS_NONFINITE; break; }
+        omega = t2[1] == 0.0 ? 0.0 : t2[0] / t2[1];
+        // E: x += alpha phat + omega shat; r = s - omega t; (rhat, r), (r, r)
+        double e0 = 0.0, e1 = 0.0;
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.x[d] += alpha * w.phat[d] + omega * w.shat[d];
+                const double r = w.s[d] - omega * w.t[d];
+                w.r[d] = r;
+                e0 += w.rhat[d] * r;
+                e1 += r * r;
+            }
+        }
+        double v3[2] = {e0, e1};
+        write_partials<2>(v3, part[pb], smem);
+        if (!grid_barrier(bar, w.dflags)) return;
+        sum_partials<2>(part[pb], t2, smem, sb);
+        pb ^= 1;
+        rho_prev = rho;
+        rho = t2[0];
+        rr = t2[1];
+        ++it;
+        if (!isfinite(rho) || !isfinite(rr))
+            status = KS_NONFINITE;
+        else if (rr <= tol2)
+            status = KS_CONVERGED;
+        else if (it >= max_iter)
+            status = KS_MAXIT;
+        else if (rho == 0.0 || omega == 0.0)
+            status = KS_BREAKDOWN;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        KrylovScalars* sc = w.sc;
+        sc->bb = bb;
+        sc->rr = rr;
+        sc->rho = rho;
+        sc->rho_prev = rho_prev;
+        sc->alpha = alpha;
+        sc->omega = omega;
+        sc->tol2 = tol2;
+        sc->iter = it;
+        sc->max_iter = max_iter;
+        sc->status = status;
+    }
+}
+
 }  // namespace
+
+int persistent_max_grid(int device) {
+    int sms = 0, occ = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_persistent, kPersistThreads, 0) != cudaSuccess)
+        return 0;
+    const int per_sm = occ < 2 ? occ : 2;  // two CTAs per SM keeps the all-CTA reductions cheap
+    return sms * per_sm;
+}
+
+int persistent_grid(int n_nodes, int max_grid) {
+    // At least 64 block rows per CTA; a single SM is too slow for the SpMV even on small
+    // systems, so small solves still spread over several CTAs.
+    int g = (n_nodes + 63) / 64;
+    if (g < 1) g = 1;
+    return g < max_grid ? g : max_grid;
+}
+
+cudaError_t launch_bicgstab_persistent(const KrylovWork& w, double rtol, int max_iter, GridBarrier* bar, int grid,
+                                       cudaStream_t s) {
+    KrylovWork wc = w;
+    void* args[] = {&wc, &rtol, &max_iter, &bar};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_persistent), dim3(grid),
+                                       dim3(kPersistThreads), args, 0, s);
+}
 
 int vec_grid(int n_nodes) {
     int g = (n_nodes + kVecThreads - 1) / kVecThreads;
