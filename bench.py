@@ -330,6 +330,74 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
 
 
+def run_batch(args) -> None:
+    """Batched uneven tissues: 256 discs / rectangles (500-20k prisms, log-uniform) in one
+    context, against sequential single-tissue GPU runs of the same tissues."""
+    import ctypes
+
+    import torch
+
+    from tissueorigami_b200 import capi, mesh
+    from tissueorigami_b200.newton import BatchSolver, NewtonRaphsonSolver
+
+    L = capi.load()
+    ts = mesh.batch_tissues(n_tissues=args.n_tissues)
+    E_t = np.array([t.n_elems for t in ts], dtype=np.float64)
+    b = BatchSolver(ts)
+    x = torch.from_numpy(b.join([t.x for t in ts]).reshape(-1).copy()).cuda()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        st = capi.StepStats()
+        rc = L.tf_time_step_device(b._h, ctypes.c_void_p(x.data_ptr()), float(ts[0].dt), ctypes.c_void_p(x.data_ptr()),
+                                   ctypes.byref(st))
+        capi.check(rc, "tf_time_step_device", b._h)
+        return rc, st
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(None)
+    clocks.start()
+    ms, units, launches, worst = 0.0, 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        rc, st = step()
+        ts_stats = b.tissue_stats()
+        units += float((E_t * ts_stats["newton_iters"]).sum())
+        ms += st.ms_total
+        launches += st.gpu_launches
+        worst = max(worst, rc)
+    clk = clocks.stop()
+    b.close()
+    # sequential baseline: the same tissues one after another, one context each, same steps
+    seq_ms, seq_units = 0.0, 0.0
+    for t in ts:
+        with NewtonRaphsonSolver.from_tissue(t) as s:
+            xx = t.x.copy()
+            for _ in range(args.warmup):
+                xx, _, _ = s.runOneStep(xx, t.dt)
+            for _ in range(args.steps):
+                xx, _, st = s.runOneStep(xx, t.dt)
+                seq_ms += st["ms_total"]
+                seq_units += t.n_elems * st["newton_iters"]
+    value = units / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded meshes and growth fields)",
+        "config": {"workload": f"batch: {len(ts)} tissues, {int(E_t.sum())} prisms, prism counts log-uniform 500-20000",
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "tissue_steps_per_s": len(ts) * args.steps / (ms / 1000.0),
+        "sequential": {"value": seq_units / (seq_ms / 1000.0), "ms_per_step": seq_ms / args.steps,
+                       "tissue_steps_per_s": len(ts) * args.steps / (seq_ms / 1000.0)},
+        "batch_speedup_vs_sequential": (seq_ms / args.steps) / (ms / args.steps),
+        "gpu_launches": int(launches), "clocks": clk, "status_worst": worst,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def load_traffic():
     """Per-launch DRAM bytes from committed ncu summaries (profiles/traffic.tsv:
     kernel<TAB>workload<TAB>bytes_per_launch); missing entries read as null."""
@@ -355,11 +423,14 @@ def main():
     ap.add_argument("--workload", default="wing_disc")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_b200(args)
 

@@ -106,6 +106,24 @@ const char* tf_version(void);
  * and allocates every device buffer of the tissue. */
 int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out);
 
+/* Batched mode (no single counterpart in the reference, which runs one tissue per process):
+ * n_tissues independent tissues in one context. Tissue t's nodes and elements follow those of
+ * tissue t-1 in every per-node / per-element array the other calls take (concatenated, node
+ * ids of meshes[t].conn local to tissue t). Each tissue runs the reference's Newton loop on
+ * its own - its own convergence test and cap - inside shared launches: one element-kernel
+ * launch over all prisms, one persistent cooperative solve in which every tissue owns a group
+ * of CTAs, per-tissue convergence flags that drop converged tissues from later iterations. */
+int tf_batch_create(int32_t n_tissues, const tf_mesh_desc* meshes, const tf_params* params,
+                    tf_ctx** out);
+
+/* Per-tissue outcome of the last step of a batched (or single) context: Newton iterations,
+ * status and BiCGStab iterations, each [n_tissues] (any may be NULL). */
+int tf_get_tissue_stats(tf_ctx* ctx, int32_t* newton_iters, int32_t* status,
+                        int32_t* krylov_iters);
+
+/* Number of tissues of the context. */
+int tf_get_n_tissues(tf_ctx* ctx);
+
 /* Replaces NewtonRaphsonSolver::~NewtonRaphsonSolver (NewtonRaphsonSolver.cpp:43-71). */
 void tf_destroy(tf_ctx* ctx);
 

@@ -1,0 +1,73 @@
+"""GPU tests of the batched mode: many independent tissues of uneven size in one context.
+
+Each tissue must follow exactly the single-tissue path (its own Newton convergence and cap):
+positions after the steps within 1e-9 of the tissue size of separate single-tissue runs and of
+the oracle, and the same Newton iteration counts.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tissueorigami_b200 import capi, mesh
+from tissueorigami_b200.newton import BatchSolver, NewtonRaphsonSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _tissues():
+    out = []
+    for k, n in enumerate([400, 1500, 700, 3000, 500, 2200]):
+        E = 600.0 + 400.0 * k
+        out.append(mesh.small_disc(100 + k, n, E, n_steps=3) if k % 2 == 0 else mesh.small_rect_sized(100 + k, n, E, n_steps=3))
+    return out
+
+
+def test_batch_matches_single_tissue_runs():
+    ts = _tissues()
+    n_steps = 3
+    singles, its_single = [], []
+    for t in ts:
+        with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+            x = t.x.copy()
+            its = []
+            for _ in range(n_steps):
+                x, rc, st = s.runOneStep(x, t.dt)
+                assert rc == capi.TF_OK
+                its.append(st["newton_iters"])
+            singles.append(x)
+            its_single.append(its)
+    with BatchSolver(ts, krylov_rtol=1e-14) as b:
+        x = b.join([t.x for t in ts])
+        its_batch = [[] for _ in ts]
+        for _ in range(n_steps):
+            x, rc, st = b.runOneStep(x, ts[0].dt)
+            assert rc == capi.TF_OK
+            stats = b.tissue_stats()
+            assert (stats["status"] == 0).all()
+            for i in range(len(ts)):
+                its_batch[i].append(int(stats["newton_iters"][i]))
+        xs = b.split(x)
+    assert its_batch == its_single
+    for t, xb, xsng in zip(ts, xs, singles):
+        assert np.abs(xb - xsng).max() <= 1e-9 * t.size
+
+
+def test_batch_tissue_matches_oracle():
+    ts = _tissues()[:3]
+    with BatchSolver(ts, krylov_rtol=1e-14) as b:
+        x = b.join([t.x for t in ts])
+        for _ in range(2):
+            x, rc, st = b.runOneStep(x, ts[0].dt)
+            assert rc == capi.TF_OK
+        xs = b.split(x)
+    x_ref, _, _, _ = O.simulate_sparse(ts[1], n_steps=2)
+    assert np.abs(xs[1] - x_ref).max() <= 1e-9 * ts[1].size
+
+
+def test_batch_assembly_is_block_diagonal():
+    ts = _tissues()[:2]
+    with BatchSolver(ts) as b:
+        rowptr, colidx = b.pattern()
+        tissue_of = np.repeat(np.arange(len(ts)), [t.n_nodes for t in ts])
+        rows = np.repeat(np.arange(b.n_nodes), np.diff(rowptr))
+        assert (tissue_of[rows] == tissue_of[colidx]).all()

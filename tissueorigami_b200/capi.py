@@ -45,7 +45,8 @@ EXPORTS = [
     "tf_set_inv_fg", "tf_set_boundary", "tf_set_viscosity_surface", "tf_newton_step",
     "tf_newton_step_device", "tf_get_pattern", "tf_assemble", "tf_solve", "tf_set_growth",
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
-    "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc",
+    "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
+    "tf_get_tissue_stats", "tf_get_n_tissues",
 ]
 
 
@@ -124,6 +125,9 @@ def load(build_if_missing: bool = True):
     L.tf_get_schedule.argtypes = [_P, _I, _I, _I]
     L.tf_autotune.argtypes = [_P, _D, c_double]
     L.tf_time_kernels.argtypes = [_P, c_int, _D, _D]
+    L.tf_batch_create.argtypes = [c_int, ctypes.POINTER(MeshDesc), ctypes.POINTER(Params), ctypes.POINTER(_P)]
+    L.tf_get_tissue_stats.argtypes = [_P, _I, _I, _I]
+    L.tf_get_n_tissues.argtypes = [_P]
     L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p

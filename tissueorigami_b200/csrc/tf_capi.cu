@@ -65,6 +65,18 @@ struct tf_ctx {
     DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
     DevBuf fg, rates, angles, exposed, peripodial, rotated, xio, barrier;
     int persistent_grid_max = 0;  // 0: cooperative launch unavailable
+
+    // batch partition: tissue t owns nodes [tissue_node0[t], tissue_node0[t+1]) and elements
+    // [tissue_elem0[t], tissue_elem0[t+1]); a single tissue is T = 1.
+    int32_t T = 1;
+    std::vector<int32_t> tissue_node0, tissue_elem0;
+    std::vector<int32_t> plan_cta_tissue, plan_cta0, plan_ncta;
+    DevBuf node_tissue_d, plan_cta_tissue_d, plan_cta0_d, plan_ncta_d, plan_row0_d, active_d, tbarriers, tscalars, tdu2;
+    int32_t* h_active = nullptr;     // pinned [T]
+    double* h_du2 = nullptr;         // pinned [T]
+    KrylovScalars* h_tsc = nullptr;  // pinned [T]
+    std::vector<int32_t> t_iters, t_status, t_krylov;
+    std::vector<int32_t> last_krylov;  // first-round BiCGStab iterations of each tissue, last step
     KrylovScalars* h_sc = nullptr;  // pinned
     int32_t* h_flags = nullptr;     // pinned
 
@@ -277,6 +289,9 @@ int upload_structure(tf_ctx* ctx) {
     // keep the previous material / growth values if the records already exist on the device
     const bool keep = ctx->elems.p != nullptr && ctx->elems.bytes >= sizeof(ElemRecord) * (size_t)E;
     if (keep) TF_CK(cudaMemcpy(rec.data(), ctx->elems.p, sizeof(ElemRecord) * (size_t)E, cudaMemcpyDeviceToHost));
+    std::vector<int32_t> elem_tissue(E, 0);
+    for (int t = 0; t < ctx->T; ++t)
+        for (int e = ctx->tissue_elem0[t]; e < ctx->tissue_elem0[t + 1]; ++e) elem_tissue[e] = t;
     parallel_for(E, [&](int64_t b0, int64_t b1) {
         for (int64_t e = b0; e < b1; ++e) {
             ElemRecord& R = rec[e];
@@ -284,6 +299,7 @@ int upload_structure(tf_ctx* ctx) {
                 std::memset(&R, 0, sizeof(R));
                 for (int k = 0; k < 9; ++k) R.inv_fg[k] = (k % 4 == 0) ? 1.0 : 0.0;
             }
+            R.tissue = elem_tissue[e];
             const int32_t* cn = &ctx->conn[(size_t)e * 6];
             bool rt = false;
             for (int a = 0; a < 6; ++a) {
@@ -379,7 +395,98 @@ AssembleArgs make_assemble(tf_ctx* c, double dt) {
     a.vals = dptr<double>(c->vals);
     a.g = dptr<double>(c->g);
     a.dflags = dptr<int32_t>(c->dflags);
+    a.tissue_active = dptr<int32_t>(c->active_d);
     return a;
+}
+
+// CTA plan of the persistent solve. Every active tissue gets at least one CTA; the rest of the
+// cooperative grid is shared in proportion to weight[t] (expected work: rows x BiCGStab
+// iterations), keeping at least 64 rows per CTA. Inactive tissues get none. The plan is rebuilt
+// every Newton round of a batch, so that the tissues still iterating take over the CTAs of the
+// converged ones and the largest solves get the most CTAs.
+int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* active) {
+    const int T = ctx->T;
+    const int cmax = std::max(ctx->persistent_grid_max, 1);
+    std::vector<int64_t> rows(T);
+    double wsum = 0.0;
+    int n_act = 0;
+    for (int t = 0; t < T; ++t) {
+        rows[t] = ctx->tissue_node0[t + 1] - ctx->tissue_node0[t];
+        if (active[t]) {
+            wsum += weight[t];
+            ++n_act;
+        }
+    }
+    std::vector<int32_t> n(T, 0);
+    if (ctx->persistent_grid_max > 0) {
+        if (n_act > cmax) return set_error(ctx, TF_ERR_UNSUPPORTED, "more active tissues than co-resident CTAs");
+        const int spare = cmax - n_act;
+        int used = 0;
+        for (int t = 0; t < T; ++t) {
+            if (!active[t]) continue;
+            const int64_t cap = std::max<int64_t>(1, (rows[t] + 63) / 64);
+            const int64_t want = 1 + (wsum > 0 ? (int64_t)((double)spare * weight[t] / wsum) : 0);
+            n[t] = (int32_t)std::min(want, cap);
+            used += n[t];
+        }
+        (void)used;
+    } else {
+        for (int t = 0; t < T; ++t) n[t] = active[t] ? 1 : 0;
+    }
+    ctx->plan_cta0.assign(T, 0);
+    ctx->plan_ncta = n;
+    ctx->plan_cta_tissue.clear();
+    for (int t = 0; t < T; ++t) {
+        ctx->plan_cta0[t] = (int32_t)ctx->plan_cta_tissue.size();
+        for (int k = 0; k < n[t]; ++k) ctx->plan_cta_tissue.push_back(t);
+    }
+    const size_t C = std::max<size_t>(1, ctx->plan_cta_tissue.size());
+    if (ctx->plan_cta_tissue.empty()) ctx->plan_cta_tissue.push_back(0);  // keeps a valid launch shape
+    TF_CK(dalloc(ctx->plan_cta_tissue_d, sizeof(int32_t) * (size_t)cmax));
+    TF_CK(dalloc(ctx->plan_cta0_d, sizeof(int32_t) * T));
+    TF_CK(dalloc(ctx->plan_ncta_d, sizeof(int32_t) * T));
+    TF_CK(dalloc(ctx->plan_row0_d, sizeof(int32_t) * (T + 1)));
+    TF_CK(cudaMemcpyAsync(ctx->plan_cta_tissue_d.p, ctx->plan_cta_tissue.data(), sizeof(int32_t) * C,
+                          cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->plan_cta0_d.p, ctx->plan_cta0.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->plan_ncta_d.p, ctx->plan_ncta.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->plan_row0_d.p, ctx->tissue_node0.data(), sizeof(int32_t) * (T + 1), cudaMemcpyHostToDevice,
+                          ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));  // the host vectors may change before the next round
+    const size_t need = 4 * (size_t)cmax + 64;
+    if (ctx->partials.bytes < sizeof(double) * need) TF_CK(dalloc(ctx->partials, sizeof(double) * need));
+    return TF_OK;
+}
+
+// Initial work estimate of a tissue: rows x sqrt(rows) (BiCGStab iterations grow with the
+// mesh's linear size).
+std::vector<double> rows_weight(tf_ctx* ctx) {
+    std::vector<double> w(ctx->T);
+    for (int t = 0; t < ctx->T; ++t) {
+        const double r = ctx->tissue_node0[t + 1] - ctx->tissue_node0[t];
+        w[t] = r * std::sqrt(r);
+    }
+    return w;
+}
+
+int build_plan_all(tf_ctx* ctx) {
+    std::vector<int32_t> all(ctx->T, 1);
+    return build_plan(ctx, rows_weight(ctx), all.data());
+}
+
+BatchPlan make_plan(tf_ctx* c) {
+    BatchPlan p;
+    p.n_tissues = c->T;
+    p.n_cta = (int32_t)c->plan_cta_tissue.size();
+    p.cta_tissue = dptr<int32_t>(c->plan_cta_tissue_d);
+    p.cta0 = dptr<int32_t>(c->plan_cta0_d);
+    p.ncta = dptr<int32_t>(c->plan_ncta_d);
+    p.row0 = dptr<int32_t>(c->plan_row0_d);
+    p.active = dptr<int32_t>(c->active_d);
+    p.barriers = dptr<GridBarrier>(c->tbarriers);
+    p.scalars = dptr<KrylovScalars>(c->tscalars);
+    p.du2 = dptr<double>(c->tdu2);
+    return p;
 }
 
 // Element kernels for the current schedule (no memset, no node terms).
@@ -425,6 +532,8 @@ int assemble_system(tf_ctx* ctx, double dt) {
     na.vals = dptr<double>(ctx->vals);
     na.g = dptr<double>(ctx->g);
     na.dflags = dptr<int32_t>(ctx->dflags);
+    na.node_tissue = dptr<int32_t>(ctx->node_tissue_d);
+    na.tissue_active = dptr<int32_t>(ctx->active_d);
     TF_CK(launch_node_terms(na, ctx->stream));
     ctx->launches += 1;
     return TF_OK;
@@ -440,22 +549,26 @@ int krylov_status_to_tf(int ks) {
     }
 }
 
-// Solve J du = g (buffers in the context). Leaves the scalars in ctx->h_sc.
+bool use_persistent(tf_ctx* ctx) { return ctx->persistent_grid_max > 0 && (ctx->params.persistent || ctx->T > 1); }
+
+// Solve J du = g (buffers in the context) for every active tissue. Leaves the scalars in
+// ctx->h_tsc[T] (persistent) or ctx->h_sc (chunked, single tissue).
 int krylov_solve(tf_ctx* ctx) {
     KrylovWork w = make_work(ctx);
-    if (ctx->params.persistent && ctx->persistent_grid_max > 0) {
-        const int grid = persistent_grid(ctx->N, ctx->persistent_grid_max);
-        TF_CK(launch_bicgstab_persistent(w, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
-                                         dptr<GridBarrier>(ctx->barrier), grid, ctx->stream));
+    if (use_persistent(ctx)) {
+        const BatchPlan plan = make_plan(ctx);
+        TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters, ctx->stream));
         ctx->launches += 1;
-        TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->h_tsc, ctx->tscalars.p, sizeof(KrylovScalars) * ctx->T, cudaMemcpyDeviceToHost,
+                              ctx->stream));
         TF_CK(cudaMemcpyAsync(ctx->h_flags, ctx->dflags.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
         TF_CK(cudaStreamSynchronize(ctx->stream));
         if (*ctx->h_flags & DF_BARRIER_TIMEOUT) {
-            TF_CK(cudaMemsetAsync(ctx->barrier.p, 0, sizeof(GridBarrier), ctx->stream));
+            TF_CK(cudaMemsetAsync(ctx->tbarriers.p, 0, sizeof(GridBarrier) * ctx->T, ctx->stream));
             TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
             return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
         }
+        *ctx->h_sc = ctx->h_tsc[0];
         return TF_OK;
     }
     TF_CK(launch_block_jacobi_setup(w, ctx->stream));
@@ -500,62 +613,109 @@ int worse(int a, int b) {
 }
 
 // Newton loop on device buffers: un holds x_n; result left in uk.
+// Newton loop on device buffers: un holds x_n; result left in uk. Every tissue of a batch
+// follows Simulation::updateStepNR on its own: it stops once its ||du||_2 <= tol
+// (checkConvergenceViaDeltaU, NewtonRaphsonSolver.cpp:807-825) or after more than
+// max_newton_iters iterations (Simulation.cpp:6724-6727), the last update applied either way;
+// tissues that stopped are skipped by the assembly, the solve and the update.
 int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
+    const int T = ctx->T;
     TF_CK(cudaMemcpyAsync(ctx->uk.p, ctx->un.p, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyDeviceToDevice, ctx->stream));
     TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
-    int status = TF_OK;
-    int iteratorK = 0;
-    bool converged = false;
+    ctx->t_iters.assign(T, 0);
+    ctx->t_status.assign(T, TF_OK);
+    ctx->t_krylov.assign(T, 0);
+    for (int t = 0; t < T; ++t) ctx->h_active[t] = 1;
+    const bool persistent = use_persistent(ctx);
+    int n_active = T;
+    int round = 0;
     float ms;
-    while (!converged) {
+    std::vector<double> weight = rows_weight(ctx);
+    if (T > 1 && ctx->last_krylov.size() == (size_t)T)
+        for (int t = 0; t < T; ++t)
+            weight[t] = (ctx->tissue_node0[t + 1] - ctx->tissue_node0[t]) * std::max(8.0, (double)ctx->last_krylov[t]);
+    ctx->last_krylov.assign(T, 0);
+    while (n_active > 0) {
+        if (T > 1 && persistent) {
+            int rc = build_plan(ctx, weight, ctx->h_active);
+            if (rc != TF_OK) return rc;
+        }
+        TF_CK(cudaMemcpyAsync(ctx->active_d.p, ctx->h_active, sizeof(int32_t) * T, cudaMemcpyHostToDevice, ctx->stream));
         TF_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
         int rc = assemble_system(ctx, dt);
         if (rc != TF_OK) return rc;
         TF_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         rc = krylov_solve(ctx);
         if (rc != TF_OK) return rc;
-        const KrylovScalars sc = *ctx->h_sc;
         KrylovWork w = make_work(ctx);
-        TF_CK(launch_newton_update(w, dptr<double>(ctx->uk), dptr<int32_t>(ctx->slaves_d), dptr<int32_t>(ctx->masters_d),
-                                   (int32_t)ctx->slave.size(), ctx->stream));
+        if (persistent) {
+            TF_CK(launch_newton_update_batched(w, make_plan(ctx), dptr<double>(ctx->uk), dptr<int32_t>(ctx->slaves_d),
+                                               dptr<int32_t>(ctx->masters_d), (int32_t)ctx->slave.size(), ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->h_du2, ctx->tdu2.p, sizeof(double) * T, cudaMemcpyDeviceToHost, ctx->stream));
+        } else {
+            *ctx->h_tsc = *ctx->h_sc;
+            TF_CK(launch_newton_update(w, dptr<double>(ctx->uk), dptr<int32_t>(ctx->slaves_d), dptr<int32_t>(ctx->masters_d),
+                                       (int32_t)ctx->slave.size(), ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        }
         ctx->launches += ctx->slave.empty() ? 1 : 2;
         TF_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-        TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
         rc = read_flags(ctx);
         if (rc != TF_OK) return rc;
+        if (!persistent) ctx->h_du2[0] = ctx->h_sc->du2;
         TF_CK(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
         st->ms_assemble += ms;
         TF_CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
         st->ms_solve += ms;
-        const int ks = krylov_status_to_tf(sc.status);
-        if (ks != TF_OK) status = worse(status, ks);
-        if (*ctx->h_flags & DF_NONFINITE)
-            status = worse(status, TF_NONFINITE);
-        else if (*ctx->h_flags & DF_INVERTED)
-            status = worse(status, TF_ELEMENT_INVERTED);
         if (*ctx->h_flags & DF_PATTERN_MISS) return set_error(ctx, TF_ERR_STATE, "routed entry outside the pattern");
-        const double d = std::sqrt(ctx->h_sc->du2);
-        if (iteratorK < 32) {
-            st->du_norm[iteratorK] = d;
-            st->krylov_rel_res[iteratorK] = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+        int flag_status = TF_OK;
+        if (*ctx->h_flags & DF_NONFINITE)
+            flag_status = TF_NONFINITE;
+        else if (*ctx->h_flags & DF_INVERTED)
+            flag_status = TF_ELEMENT_INVERTED;
+        double dmax = 0.0, relmax = 0.0;
+        int kit_max = 0;
+        for (int t = 0; t < T; ++t) {
+            if (!ctx->h_active[t]) continue;
+            const KrylovScalars& sc = ctx->h_tsc[t];
+            const int ks = krylov_status_to_tf(sc.status);
+            if (ks != TF_OK) ctx->t_status[t] = worse(ctx->t_status[t], ks);
+            if (flag_status != TF_OK) ctx->t_status[t] = worse(ctx->t_status[t], flag_status);
+            ctx->t_krylov[t] += sc.iter;
+            st->krylov_iters_total += sc.iter;
+            weight[t] = (ctx->tissue_node0[t + 1] - ctx->tissue_node0[t]) * std::max(8.0, (double)sc.iter);
+            if (round == 0) ctx->last_krylov[t] = sc.iter;
+            kit_max = std::max(kit_max, sc.iter);
+            const double d = std::sqrt(ctx->h_du2[t]);
+            dmax = std::max(dmax, std::isfinite(d) ? d : INFINITY);
+            relmax = std::max(relmax, sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0);
+            ctx->t_iters[t]++;
+            bool done;
+            if (!std::isfinite(d)) {
+                ctx->t_status[t] = worse(ctx->t_status[t], TF_NONFINITE);
+                done = true;
+            } else {
+                done = !(d > ctx->params.newton_tol);
+                if (!done && ctx->t_iters[t] > ctx->params.max_newton_iters) {
+                    ctx->t_status[t] = worse(ctx->t_status[t], TF_NEWTON_NOT_CONVERGED);
+                    done = true;
+                }
+            }
+            if (done) {
+                ctx->h_active[t] = 0;
+                --n_active;
+            }
         }
-        st->krylov_iters_total += sc.iter;
-        st->krylov_iters_max = std::max(st->krylov_iters_max, sc.iter);
-        if (!std::isfinite(d)) {
-            status = worse(status, TF_NONFINITE);
-            iteratorK++;
-            break;
+        st->krylov_iters_max = std::max(st->krylov_iters_max, kit_max);
+        if (round < 32) {
+            st->du_norm[round] = dmax;
+            st->krylov_rel_res[round] = relmax;
         }
-        // checkConvergenceViaDeltaU (NewtonRaphsonSolver.cpp:807-825), then the cap of
-        // Simulation.cpp:6724-6727 (the update above is applied either way).
-        converged = !(d > ctx->params.newton_tol);
-        iteratorK++;
-        if (!converged && iteratorK > ctx->params.max_newton_iters) {
-            status = worse(status, TF_NEWTON_NOT_CONVERGED);
-            converged = true;
-        }
+        ++round;
     }
-    st->newton_iters = iteratorK;
+    int status = TF_OK;
+    for (int t = 0; t < T; ++t) status = worse(status, ctx->t_status[t]);
+    st->newton_iters = round;
     st->status = status;
     return status;
 }
@@ -586,6 +746,13 @@ int prologue(tf_ctx* ctx, double dt) {
                                    dptr<double>(ctx->visc_surface), ctx->stream));
     ctx->launches += 2;
     return TF_OK;
+}
+
+// Mark every tissue active on the device (the parity hooks and timers act on all tissues).
+int activate_all(tf_ctx* ctx) {
+    for (int t = 0; t < ctx->T; ++t) ctx->h_active[t] = 1;
+    TF_CK(cudaMemcpyAsync(ctx->active_d.p, ctx->h_active, sizeof(int32_t) * ctx->T, cudaMemcpyHostToDevice, ctx->stream));
+    return ctx->T > 1 ? build_plan_all(ctx) : TF_OK;
 }
 
 int check_ctx(tf_ctx* ctx) {
@@ -625,15 +792,29 @@ void tf_default_params(tf_params* p) {
 
 const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
 
-int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
+struct CtxDeleter {
+    void operator()(tf_ctx* c) const { tf_destroy(c); }
+};
+
+// Create a context over one mesh whose nodes and elements are split into T consecutive
+// tissues (node0 / elem0 hold T+1 offsets); T = 1 is the single-tissue context.
+static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t T, const int32_t* node0,
+                      const int32_t* elem0, tf_ctx** out) {
     if (!out) return TF_ERR_ARGUMENT;
     *out = nullptr;
-    if (!mesh || mesh->n_nodes <= 0 || mesh->n_elems <= 0 || !mesh->conn || !mesh->xref) return TF_ERR_ARGUMENT;
-    for (int64_t k = 0; k < (int64_t)mesh->n_elems * 6; ++k)
-        if (mesh->conn[k] < 0 || mesh->conn[k] >= mesh->n_nodes) return TF_ERR_ARGUMENT;
-    std::unique_ptr<tf_ctx> holder(new (std::nothrow) tf_ctx());
+    if (!mesh || mesh->n_nodes <= 0 || mesh->n_elems <= 0 || !mesh->conn || !mesh->xref || T <= 0) return TF_ERR_ARGUMENT;
+    for (int t = 0; t < T; ++t)
+        for (int e = elem0[t]; e < elem0[t + 1]; ++e)
+            for (int a = 0; a < 6; ++a) {
+                const int32_t v = mesh->conn[(int64_t)e * 6 + a];
+                if (v < node0[t] || v >= node0[t + 1]) return TF_ERR_ARGUMENT;
+            }
+    std::unique_ptr<tf_ctx, CtxDeleter> holder(new (std::nothrow) tf_ctx());
     tf_ctx* ctx = holder.get();
     if (!ctx) return TF_ERR_OUT_OF_MEMORY;
+    ctx->T = T;
+    ctx->tissue_node0.assign(node0, node0 + T + 1);
+    ctx->tissue_elem0.assign(elem0, elem0 + T + 1);
     if (params)
         ctx->params = *params;
     else
@@ -670,6 +851,25 @@ int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
     TF_CK(dalloc(ctx->barrier, sizeof(GridBarrier)));
     TF_CK(cudaMemset(ctx->barrier.p, 0, sizeof(GridBarrier)));
     {
+        const size_t T = ctx->T;
+        TF_CK(dalloc(ctx->active_d, sizeof(int32_t) * T));
+        TF_CK(dalloc(ctx->tbarriers, sizeof(GridBarrier) * T));
+        TF_CK(dalloc(ctx->tscalars, sizeof(KrylovScalars) * T));
+        TF_CK(dalloc(ctx->tdu2, sizeof(double) * T));
+        TF_CK(cudaMemset(ctx->tbarriers.p, 0, sizeof(GridBarrier) * T));
+        TF_CK(cudaMemset(ctx->tscalars.p, 0, sizeof(KrylovScalars) * T));
+        std::vector<int32_t> ones(T, 1);
+        TF_CK(cudaMemcpy(ctx->active_d.p, ones.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice));
+        TF_CK(cudaMallocHost(&ctx->h_active, sizeof(int32_t) * T));
+        TF_CK(cudaMallocHost(&ctx->h_du2, sizeof(double) * T));
+        TF_CK(cudaMallocHost(&ctx->h_tsc, sizeof(KrylovScalars) * T));
+        std::vector<int32_t> nt(ctx->N);
+        for (int t = 0; t < ctx->T; ++t)
+            for (int i = ctx->tissue_node0[t]; i < ctx->tissue_node0[t + 1]; ++i) nt[i] = t;
+        TF_CK(dalloc(ctx->node_tissue_d, sizeof(int32_t) * N));
+        TF_CK(cudaMemcpy(ctx->node_tissue_d.p, nt.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+    }
+    {
         int coop = 0;
         TF_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
         ctx->persistent_grid_max = coop ? persistent_max_grid(ctx->device) : 0;
@@ -692,6 +892,9 @@ int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
     TF_CK(cudaMallocHost(&ctx->h_flags, sizeof(int32_t)));
     int rc = upload_structure(ctx);
     if (rc != TF_OK) return rc;
+    rc = build_plan_all(ctx);
+    if (rc != TF_OK) return rc;
+    if (ctx->T > 1 && ctx->persistent_grid_max == 0) return TF_ERR_UNSUPPORTED;
     if (ctx->params.scatter == TF_SCATTER_COLOURED && ctx->n_colours == 0) return TF_ERR_UNSUPPORTED;
     ctx->scatter = ctx->params.scatter == TF_SCATTER_AUTO ? TF_SCATTER_ATOMIC : ctx->params.scatter;
     ctx->teams = ctx->params.elems_per_block > 0 ? ctx->params.elems_per_block : 16;
@@ -699,6 +902,51 @@ int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
     *out = holder.release();
     return TF_OK;
 }
+
+int tf_create(const tf_mesh_desc* mesh, const tf_params* params, tf_ctx** out) {
+    if (!mesh) return TF_ERR_ARGUMENT;
+    const int32_t node0[2] = {0, mesh->n_nodes}, elem0[2] = {0, mesh->n_elems};
+    return create_ctx(mesh, params, 1, node0, elem0, out);
+}
+
+int tf_batch_create(int32_t n_tissues, const tf_mesh_desc* meshes, const tf_params* params, tf_ctx** out) {
+    if (!out) return TF_ERR_ARGUMENT;
+    *out = nullptr;
+    if (n_tissues <= 0 || !meshes) return TF_ERR_ARGUMENT;
+    std::vector<int32_t> node0(n_tissues + 1, 0), elem0(n_tissues + 1, 0);
+    for (int t = 0; t < n_tissues; ++t) {
+        const tf_mesh_desc& m = meshes[t];
+        if (m.n_nodes <= 0 || m.n_elems <= 0 || !m.conn || !m.xref) return TF_ERR_ARGUMENT;
+        if ((int64_t)node0[t] + m.n_nodes > INT32_MAX || (int64_t)elem0[t] + m.n_elems > INT32_MAX) return TF_ERR_ARGUMENT;
+        node0[t + 1] = node0[t] + m.n_nodes;
+        elem0[t + 1] = elem0[t] + m.n_elems;
+    }
+    std::vector<int32_t> conn((size_t)elem0[n_tissues] * 6);
+    std::vector<double> xref((size_t)elem0[n_tissues] * 18);
+    for (int t = 0; t < n_tissues; ++t) {
+        const tf_mesh_desc& m = meshes[t];
+        for (int64_t k = 0; k < (int64_t)m.n_elems * 6; ++k) {
+            if (m.conn[k] < 0 || m.conn[k] >= m.n_nodes) return TF_ERR_ARGUMENT;
+            conn[(size_t)elem0[t] * 6 + k] = m.conn[k] + node0[t];
+        }
+        std::memcpy(&xref[(size_t)elem0[t] * 18], m.xref, sizeof(double) * 18 * m.n_elems);
+    }
+    const tf_mesh_desc all{node0[n_tissues], elem0[n_tissues], conn.data(), xref.data()};
+    return create_ctx(&all, params, n_tissues, node0.data(), elem0.data(), out);
+}
+
+int tf_get_tissue_stats(tf_ctx* ctx, int32_t* newton_iters, int32_t* status, int32_t* krylov_iters) {
+    if (!ctx) return TF_ERR_ARGUMENT;
+    for (int t = 0; t < ctx->T; ++t) {
+        const bool have = (size_t)t < ctx->t_iters.size();
+        if (newton_iters) newton_iters[t] = have ? ctx->t_iters[t] : 0;
+        if (status) status[t] = have ? ctx->t_status[t] : TF_OK;
+        if (krylov_iters) krylov_iters[t] = have ? ctx->t_krylov[t] : 0;
+    }
+    return TF_OK;
+}
+
+int tf_get_n_tissues(tf_ctx* ctx) { return ctx ? ctx->T : TF_ERR_ARGUMENT; }
 
 void tf_destroy(tf_ctx* ctx) {
     if (!ctx) return;
@@ -712,6 +960,12 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
                      &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier};
     for (DevBuf* b : all) dfree(*b);
+    DevBuf* batch[] = {&ctx->node_tissue_d, &ctx->plan_cta_tissue_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d,
+                       &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
+    for (DevBuf* b : batch) dfree(*b);
+    if (ctx->h_active) cudaFreeHost(ctx->h_active);
+    if (ctx->h_du2) cudaFreeHost(ctx->h_du2);
+    if (ctx->h_tsc) cudaFreeHost(ctx->h_tsc);
     if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     for (auto& e : ctx->ev)
@@ -829,6 +1083,8 @@ int tf_get_pattern(tf_ctx* ctx, int32_t* nnzb, int32_t* rowptr, int32_t* colidx)
 int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, double* g_out, double* bsr_vals_out) {
     int rc = check_ctx(ctx);
     if (rc != TF_OK) return rc;
+    rc = activate_all(ctx);
+    if (rc != TF_OK) return rc;
     if (!uk || !un || !g_out || !(dt > 0)) return TF_ERR_ARGUMENT;
     const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
     TF_CK(cudaMemcpyAsync(ctx->uk.p, uk, bytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -849,6 +1105,8 @@ int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, doub
 
 int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, int32_t* iters, double* rel_res) {
     int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    rc = activate_all(ctx);
     if (rc != TF_OK) return rc;
     if (!bsr_vals || !g || !du) return TF_ERR_ARGUMENT;
     const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
@@ -940,6 +1198,8 @@ int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* 
 int tf_autotune(tf_ctx* ctx, const double* x_n, double dt) {
     int rc = check_ctx(ctx);
     if (rc != TF_OK) return rc;
+    rc = activate_all(ctx);
+    if (rc != TF_OK) return rc;
     if (!x_n || !(dt > 0)) return TF_ERR_ARGUMENT;
     const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
     TF_CK(cudaMemcpyAsync(ctx->uk.p, x_n, bytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -981,6 +1241,8 @@ int tf_autotune(tf_ctx* ctx, const double* x_n, double dt) {
 
 int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_spmv) {
     int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    rc = activate_all(ctx);
     if (rc != TF_OK) return rc;
     if (reps <= 0) return TF_ERR_ARGUMENT;
     const double dt = 60.0;

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
     const int team = threadIdx.x / 6;
     const int lane = threadIdx.x - team * 6;
     const int idx = blockIdx.x * TEAMS + team;
-    const bool active = idx < A.e_count;
+    bool active = idx < A.e_count;
     int e = 0;
     if (active) e = A.elem_list ? A.elem_list[A.e_begin + idx] : A.e_begin + idx;
 
@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
     }
     __syncthreads();
     const ElemRecord& R = *reinterpret_cast<const ElemRecord*>(&s_rec[team][0]);
+    if (active && A.tissue_active && !A.tissue_active[R.tissue]) active = false;  // converged tissue
     if (active) {
         const int nd = R.conn[lane];
         s_fix[team][lane] = A.fixmask[nd];
@@ -335,6 +336,7 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
 __global__ void k_node_terms(NodeArgs a) {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= a.n_nodes) return;
+    if (a.tissue_active && !a.tissue_active[a.node_tissue[A]]) return;  // converged tissue
     const int fm = a.fixmask[A];
     const double vs = a.visc_surface[A];
     const double inv_dt = 1.0 / a.dt;

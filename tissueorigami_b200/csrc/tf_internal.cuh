@@ -21,8 +21,8 @@ namespace tfb {
 struct __align__(16) ElemRecord {
     int32_t conn[6];
     int32_t slots[36];
-    int32_t flags;  // bit0: element touches a slave DoF (slave-master routing needed)
-    int32_t pad0;
+    int32_t flags;   // bit0: element touches a slave DoF (slave-master routing needed)
+    int32_t tissue;  // tissue of a batched context (0 for a single tissue)
     double xref[18];
     double inv_fg[9];
     double lam, mu, eta;
@@ -78,6 +78,7 @@ struct AssembleArgs {
     double* vals;              // [nnzb][9]
     double* g;                 // [3N]
     int32_t* dflags;
+    const int32_t* tissue_active;  // [T] 0 = converged tissue, skip (NULL: all active)
 };
 
 struct NodeArgs {
@@ -95,6 +96,24 @@ struct NodeArgs {
     double* vals;
     double* g;
     int32_t* dflags;
+    const int32_t* node_tissue;    // [N] tissue of each node
+    const int32_t* tissue_active;  // [T] (NULL: all active)
+};
+
+// CTA plan of the batched persistent solve: tissue t owns CTAs [cta0[t], cta0[t]+ncta[t]) and
+// node rows [row0[t], row0[t+1]); each tissue has its own barrier, scalars and partials
+// (4 doubles per CTA of the tissue, starting at 4*cta0[t]).
+struct BatchPlan {
+    int32_t n_tissues;
+    int32_t n_cta;
+    const int32_t* cta_tissue;   // [n_cta]
+    const int32_t* cta0;         // [T]
+    const int32_t* ncta;         // [T]
+    const int32_t* row0;         // [T+1]
+    const int32_t* active;       // [T]
+    GridBarrier* barriers;       // [T]
+    KrylovScalars* scalars;      // [T]
+    double* du2;                 // [T] ||du||^2 of the last Newton update
 };
 
 // --- element assembly (tf_element.cu) ---------------------------------------------------
@@ -137,11 +156,15 @@ cudaError_t launch_spmv(const KrylovWork& w, const double* xin, double* yout, cu
 cudaError_t launch_newton_update(const KrylovWork& w, double* uk, const int32_t* slaves,
                                  const int32_t* masters, int32_t n_pairs, cudaStream_t s);
 int spmv_grid(int n_nodes);
-// Persistent cooperative BiCGStab: partials must hold 4 * grid doubles.
+// Persistent cooperative BiCGStab over a batch of tissues (one tissue: a plan with T = 1).
+// w.partials must hold 4 * plan.n_cta doubles.
 int persistent_max_grid(int device);
-int persistent_grid(int n_nodes, int max_grid);
-cudaError_t launch_bicgstab_persistent(const KrylovWork& w, double rtol, int max_iter, GridBarrier* bar, int grid,
-                                       cudaStream_t s);
+cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
+                                    cudaStream_t s);
+// uk += du on active tissues, du[slave] = du[master], per-tissue ||du||^2 into plan.du2
+cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
+                                         const int32_t* slaves, const int32_t* masters, int32_t n_pairs,
+                                         cudaStream_t s);
 int vec_grid(int n_nodes);
 
 }  // namespace tfb

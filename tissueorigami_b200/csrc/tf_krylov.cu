@@ -321,23 +321,26 @@ __global__ void k_newton_update(KrylovWork w, double* uk) {
     if (grid_sum<1>(v, w.partials, &w.sc->ticket[5], tot) && threadIdx.x == 0) w.sc->du2 = tot[0];
 }
 
-// ---- persistent cooperative solve -------------------------------------------------------
+// ---- persistent cooperative solve over a batch of tissues -------------------------------
 //
-// k_bicgstab_persistent runs a whole block-Jacobi BiCGStab solve in one cooperative launch:
-// every CTA owns a contiguous range of block rows, the five phases of an iteration are
-// separated by a grid barrier, and each of the three reductions is summed by every CTA from
-// the same per-CTA partials in the same order, so all CTAs hold bit-identical scalars and take
-// the same convergence decision. The partials alternate between two buffers so a CTA can start
-// writing the next reduction while a slower one still reads the previous. The barrier is
-// bounded: a CTA that waits longer than kBarrierTimeoutCycles sets DF_BARRIER_TIMEOUT and the
-// kernel returns; co-residency is guaranteed by the cooperative launch, so this never fires
-// in a correct launch.
+// k_bicgstab_batched runs block-Jacobi BiCGStab for every active tissue of a batch in one
+// cooperative launch. Tissue t owns a group of CTAs (BatchPlan) and each CTA of the group a
+// contiguous range of the tissue's block rows. The five phases of an iteration are separated
+// by the group's barrier; each of the three reductions is summed by every CTA of the group
+// from the same per-CTA partials in the same order, so the group holds bit-identical scalars
+// and takes one convergence decision. Partials alternate between two buffers so a CTA can
+// write the next reduction while a slower one still reads the previous. Groups are
+// independent: a tissue that converges frees its CTAs while the others iterate on. The
+// barrier wait is bounded: a CTA that waits longer than kBarrierTimeoutCycles sets
+// DF_BARRIER_TIMEOUT and returns; the cooperative launch guarantees co-residency, so this
+// never fires in a correct launch.
+
 // Barrier wait bound in SM clock cycles (~2 s at the B200 boost clock).
 constexpr long long kBarrierTimeoutCycles = 4000000000ll;
 
-__device__ bool grid_barrier(GridBarrier* bar, int32_t* dflags) {
+__device__ bool group_barrier(GridBarrier* bar, int n_group, int32_t* dflags) {
     __shared__ int ok;
-    if (gridDim.x == 1) {
+    if (n_group == 1) {
         __syncthreads();
         return true;
     }
@@ -348,7 +351,7 @@ __device__ bool grid_barrier(GridBarrier* bar, int32_t* dflags) {
         const uint32_t g = *vgen;
         __threadfence();
         const uint32_t arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == (uint32_t)n_group - 1) {
             bar->count = 0u;
             __threadfence();
             atomicAdd(&bar->gen, 1u);
@@ -370,13 +373,13 @@ __device__ bool grid_barrier(GridBarrier* bar, int32_t* dflags) {
     return ok != 0;
 }
 
-// Sum NDOT per-CTA partials of every CTA (same order in every CTA); all threads get the totals.
+// Sum NDOT per-CTA partials of the n_group CTAs (same order in every CTA); all threads get the totals.
 template <int NDOT>
-__device__ void sum_partials(const double* buf, double (&tot)[NDOT], double* smem, double* sbcast) {
+__device__ void sum_partials(const double* buf, int n_group, double (&tot)[NDOT], double* smem, double* sbcast) {
     double acc[NDOT];
 #pragma unroll
     for (int k = 0; k < NDOT; ++k) acc[k] = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+    for (int i = threadIdx.x; i < n_group; i += blockDim.x)
 #pragma unroll
         for (int k = 0; k < NDOT; ++k) acc[k] += __ldcg(buf + i * NDOT + k);
     block_sum<NDOT>(acc, smem);
@@ -390,11 +393,11 @@ __device__ void sum_partials(const double* buf, double (&tot)[NDOT], double* sme
 }
 
 template <int NDOT>
-__device__ void write_partials(double (&v)[NDOT], double* buf, double* smem) {
+__device__ void write_partials(double (&v)[NDOT], double* buf, int local, double* smem) {
     block_sum<NDOT>(v, smem);
     if (threadIdx.x == 0)
 #pragma unroll
-        for (int k = 0; k < NDOT; ++k) buf[blockIdx.x * NDOT + k] = v[k];
+        for (int k = 0; k < NDOT; ++k) buf[local * NDOT + k] = v[k];
 }
 
 // y = J x for rows [r0, r1) with kGroup lanes per row; returns this thread's share of the
@@ -452,14 +455,48 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
     D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
-__global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovWork w, double rtol, int max_iter,
-                                                                         GridBarrier* bar) {
+// BiCGStab restart after a breakdown: rhat = r, p = v = 0, rho = (r, r); at most kMaxRestarts
+// per solve. Returns false when the restarts are used up (the caller reports a breakdown).
+constexpr int kMaxRestarts = 8;
+
+__device__ bool restart(const KrylovWork& w, int r0, int r1, double& rho, double& rho_prev, double& alpha,
+                        double& omega, int& restarts, double* buf, int lc, int nct, GridBarrier* bar, double* smem,
+                        double* sb) {
+    if (++restarts > kMaxRestarts) return false;
+    double v[1] = {0.0}, tot[1];
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            const double r = w.r[d];
+            w.rhat[d] = r;
+            w.p[d] = 0.0;
+            w.v[d] = 0.0;
+            v[0] += r * r;
+        }
+    write_partials<1>(v, buf, lc, smem);
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    sum_partials<1>(buf, nct, tot, smem, sb);
+    rho = tot[0];
+    rho_prev = 1.0;
+    alpha = 1.0;
+    omega = 1.0;
+    return rho > 0.0 && isfinite(rho);
+}
+
+__global__ void __launch_bounds__(kPersistThreads, 3) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
+                                                                      int max_iter) {
     __shared__ double smem[32 * 2];
     __shared__ double sb[2];
-    const int nb = gridDim.x;
-    const int r0 = (int)((long long)w.n_nodes * blockIdx.x / nb);
-    const int r1 = (int)((long long)w.n_nodes * (blockIdx.x + 1) / nb);
-    double* part[2] = {w.partials, w.partials + 2 * nb};
+    const int t = plan.cta_tissue[blockIdx.x];
+    if (!plan.active[t]) return;
+    const int c0 = plan.cta0[t], nct = plan.ncta[t];
+    const int lc = blockIdx.x - c0;
+    const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
+    const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
+    const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+    GridBarrier* bar = plan.barriers + t;
+    double* part[2] = {w.partials + 4 * c0, w.partials + 4 * c0 + 2 * nct};
     int pb = 0;
     // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2
     double v1[1] = {0.0};
@@ -477,15 +514,15 @@ __global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovW
             v1[0] += b * b;
         }
     }
-    write_partials<1>(v1, part[pb], smem);
-    if (!grid_barrier(bar, w.dflags)) return;
+    write_partials<1>(v1, part[pb], lc, smem);
+    if (!group_barrier(bar, nct, w.dflags)) return;
     double t1[1], t2[2];
-    sum_partials<1>(part[pb], t1, smem, sb);
+    sum_partials<1>(part[pb], nct, t1, smem, sb);
     pb ^= 1;
     const double bb = t1[0];
     double rho = bb, rho_prev = 1.0, alpha = 1.0, omega = 1.0, rr = bb;
     const double tol2 = rtol * rtol * bb;
-    int it = 0;
+    int it = 0, restarts = 0;
     int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
     while (status == KS_RUNNING) {
         // A: p = r + beta (p - omega v); phat = D^-1 p
@@ -498,17 +535,24 @@ __global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovW
             }
             apply_dinv(w.dinv, n, w.p, w.phat);
         }
-        if (!grid_barrier(bar, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
         spmv_rows<1>(w, r0, r1, w.phat, w.v, d0, d1);
         v1[0] = d0;
-        write_partials<1>(v1, part[pb], smem);
-        if (!grid_barrier(bar, w.dflags)) return;
-        sum_partials<1>(part[pb], t1, smem, sb);
+        write_partials<1>(v1, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return;
+        sum_partials<1>(part[pb], nct, t1, smem, sb);
         pb ^= 1;
         if (!isfinite(t1[0])) { status = KS_NONFINITE; break; }
-        if (t1[0] == 0.0) { status = KS_BREAKDOWN; break; }
+        if (t1[0] == 0.0) {  // (rhat, v) vanished: restart with rhat = r
+            if (!restart(w, r0, r1, rho, rho_prev, alpha, omega, restarts, part[pb], lc, nct, bar, smem, sb)) {
+                status = KS_BREAKDOWN;
+                break;
+            }
+            pb ^= 1;
+            continue;
+        }
         alpha = rho / t1[0];
         // C: s = r - alpha v; shat = D^-1 s
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
@@ -519,15 +563,15 @@ __global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovW
             }
             apply_dinv(w.dinv, n, w.s, w.shat);
         }
-        if (!grid_barrier(bar, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
         d1 = 0.0;
         spmv_rows<2>(w, r0, r1, w.shat, w.t, d0, d1);
         double v2[2] = {d0, d1};
-        write_partials<2>(v2, part[pb], smem);
-        if (!grid_barrier(bar, w.dflags)) return;
-        sum_partials<2>(part[pb], t2, smem, sb);
+        write_partials<2>(v2, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return;
+        sum_partials<2>(part[pb], nct, t2, smem, sb);
         pb ^= 1;
         if (!isfinite(t2[0]) || !isfinite(t2[1])) { status = KS_NONFINITE; break; }
         omega = t2[1] == 0.0 ? 0.0 : t2[0] / t2[1];
@@ -545,9 +589,9 @@ __global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovW
             }
         }
         double v3[2] = {e0, e1};
-        write_partials<2>(v3, part[pb], smem);
-        if (!grid_barrier(bar, w.dflags)) return;
-        sum_partials<2>(part[pb], t2, smem, sb);
+        write_partials<2>(v3, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return;
+        sum_partials<2>(part[pb], nct, t2, smem, sb);
         pb ^= 1;
         rho_prev = rho;
         rho = t2[0];
@@ -559,11 +603,14 @@ __global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovW
             status = KS_CONVERGED;
         else if (it >= max_iter)
             status = KS_MAXIT;
-        else if (rho == 0.0 || omega == 0.0)
-            status = KS_BREAKDOWN;
+        else if (rho == 0.0 || omega == 0.0) {  // breakdown: restart with rhat = r
+            if (!restart(w, r0, r1, rho, rho_prev, alpha, omega, restarts, part[pb], lc, nct, bar, smem, sb))
+                status = KS_BREAKDOWN;
+            pb ^= 1;
+        }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        KrylovScalars* sc = w.sc;
+    if (lc == 0 && threadIdx.x == 0) {
+        KrylovScalars* sc = plan.scalars + t;
         sc->bb = bb;
         sc->rr = rr;
         sc->rho = rho;
@@ -577,31 +624,69 @@ __global__ void __launch_bounds__(kPersistThreads) k_bicgstab_persistent(KrylovW
     }
 }
 
+// Newton update of a batch: du[slave] = du[master] first (separate kernel), then per CTA of
+// the plan uk += du over its rows (active tissues only) and ||du||^2 partials; the last CTA of
+// each tissue (ticket in its barrier counter, which is idle between solves) sums the tissue's
+// partials in order.
+__global__ void k_newton_update_batched(KrylovWork w, BatchPlan plan, double* uk) {
+    __shared__ double smem[32];
+    __shared__ bool last;
+    const int t = plan.cta_tissue[blockIdx.x];
+    if (!plan.active[t]) return;
+    const int c0 = plan.cta0[t], nct = plan.ncta[t];
+    const int lc = blockIdx.x - c0;
+    const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
+    const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
+    const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+    double v[1] = {0.0};
+    for (int d = r0 * 3 + threadIdx.x; d < r1 * 3; d += blockDim.x) {
+        const double du = w.x[d];
+        v[0] += du * du;
+        uk[d] = uk[d] + du;
+    }
+    block_sum<1>(v, smem);
+    double* part = w.partials + 4 * c0;
+    if (threadIdx.x == 0) {
+        part[lc] = v[0];
+        __threadfence();
+        const uint32_t k = atomicAdd(&plan.barriers[t].count, 1u);
+        last = (k == (uint32_t)nct - 1);
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double sum = 0.0;
+    for (int i = 0; i < nct; ++i) sum += __ldcg(part + i);
+    plan.du2[t] = sum;
+    plan.barriers[t].count = 0u;
+}
+
 }  // namespace
 
 int persistent_max_grid(int device) {
     int sms = 0, occ = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_persistent, kPersistThreads, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_batched, kPersistThreads, 0) != cudaSuccess)
         return 0;
-    const int per_sm = occ < 2 ? occ : 2;  // two CTAs per SM keeps the all-CTA reductions cheap
+    const int per_sm = occ < 3 ? occ : 3;  // the kernel is built for three 256-thread CTAs per SM
     return sms * per_sm;
 }
 
-int persistent_grid(int n_nodes, int max_grid) {
-    // At least 64 block rows per CTA; a single SM is too slow for the SpMV even on small
-    // systems, so small solves still spread over several CTAs.
-    int g = (n_nodes + 63) / 64;
-    if (g < 1) g = 1;
-    return g < max_grid ? g : max_grid;
+cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
+                                    cudaStream_t s) {
+    KrylovWork wc = w;
+    BatchPlan pc = plan;
+    void* args[] = {&wc, &pc, &rtol, &max_iter};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_batched), dim3(plan.n_cta),
+                                       dim3(kPersistThreads), args, 0, s);
 }
 
-cudaError_t launch_bicgstab_persistent(const KrylovWork& w, double rtol, int max_iter, GridBarrier* bar, int grid,
-                                       cudaStream_t s) {
-    KrylovWork wc = w;
-    void* args[] = {&wc, &rtol, &max_iter, &bar};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_persistent), dim3(grid),
-                                       dim3(kPersistThreads), args, 0, s);
+cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
+                                         const int32_t* slaves, const int32_t* masters, int32_t n_pairs,
+                                         cudaStream_t s) {
+    if (n_pairs > 0) k_equate_slaves<<<(n_pairs + 255) / 256, 256, 0, s>>>(w.x, slaves, masters, n_pairs);
+    k_newton_update_batched<<<plan.n_cta, 256, 0, s>>>(w, plan, uk);
+    return cudaGetLastError();
 }
 
 int vec_grid(int n_nodes) {

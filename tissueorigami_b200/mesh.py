@@ -371,11 +371,13 @@ def small_disc(seed: int, n_prisms: int, E: float, growth_length: float = 20.0,
 def small_rect_sized(seed: int, n_prisms: int, E: float, growth_length: float = 20.0,
                      peak_growth: float = 2e-4, n_steps: int = 30) -> Tissue:
     """One-layer rectangle with about n_prisms prisms (aspect 2:1) and a smooth random growth
-    field; basal nodes fixed in z."""
+    field; rim clamped like the discs (a rectangle held in-plane by drag alone buckles under
+    non-uniform growth and leaves the Newton step ill-posed)."""
     rng = np.random.default_rng(seed)
     ny = max(2, int(round(math.sqrt(n_prisms / 4.0))) + 1)
     nx = max(2, int(round(n_prisms / (2.0 * (ny - 1)))) + 1)
     t = small_rectangle(seed=seed, nx=nx, ny=ny, E=E, n_steps=n_steps, newton_tol=1e-8)
+    t.fixed[t.at_circumference != 0, :] = 1
     cen = t.xref.reshape(-1, 6, 3).mean(axis=1)
     field = _smooth_field(rng, cen[:, :2], growth_length)
     r = peak_growth * (0.5 + 0.25 * np.tanh(field))

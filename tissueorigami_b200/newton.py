@@ -166,6 +166,62 @@ class NewtonRaphsonSolver:
         return me.value, ms.value
 
 
+class BatchSolver(NewtonRaphsonSolver):
+    """Many independent tissues in one context (tf_batch_create): one element launch over all
+    prisms, one persistent solve with a CTA group per tissue, per-tissue Newton convergence.
+    Per-node / per-element arrays are the tissues' arrays concatenated in order."""
+
+    def __init__(self, tissues, params: Optional[capi.Params] = None, **overrides):
+        L = capi.load()
+        self._L = L
+        self.tissues = list(tissues)
+        self.node0 = np.cumsum([0] + [t.n_nodes for t in self.tissues])
+        self.elem0 = np.cumsum([0] + [t.n_elems for t in self.tissues])
+        self.n_nodes = int(self.node0[-1])
+        self.n_elems = int(self.elem0[-1])
+        self.n_tissues = len(self.tissues)
+        p = params if params is not None else capi.default_params()
+        overrides.setdefault("newton_tol", self.tissues[0].newton_tol)
+        for k, v in overrides.items():
+            setattr(p, k, v)
+        self.params = p
+        self._keep = []
+        descs = (capi.MeshDesc * self.n_tissues)()
+        for i, t in enumerate(self.tissues):
+            conn = np.ascontiguousarray(t.conn, dtype=np.int32)
+            xref = _f64(t.xref)
+            self._keep += [conn, xref]
+            descs[i] = capi.MeshDesc(t.n_nodes, t.n_elems, capi.iptr(conn), capi.dptr(xref))
+        h = ctypes.c_void_p()
+        capi.check(L.tf_batch_create(self.n_tissues, descs, ctypes.byref(p), ctypes.byref(h)), "tf_batch_create")
+        self._h = h
+        self.conn = np.concatenate([t.conn + self.node0[i] for i, t in enumerate(self.tissues)]).astype(np.int32)
+        self.last_stats = None
+        cat = np.concatenate
+        sm = [t.slave_master + 3 * self.node0[i] for i, t in enumerate(self.tissues) if t.slave_master.size]
+        self.set_material(cat([t.lam for t in self.tissues]), cat([t.mu for t in self.tissues]),
+                          cat([t.eta for t in self.tissues]))
+        self.set_boundary(cat([t.fixed for t in self.tissues]), cat([t.ext_visc for t in self.tissues]),
+                          cat(sm) if sm else None)
+        self.set_growth(cat([t.fg for t in self.tissues]), cat([t.rates for t in self.tissues]),
+                        cat([t.angles for t in self.tissues]), cat([t.exposed for t in self.tissues]),
+                        cat([t.peripodial for t in self.tissues]))
+
+    def join(self, xs):
+        return np.concatenate([np.asarray(x, dtype=np.float64).reshape(-1, 3) for x in xs])
+
+    def split(self, x):
+        x = np.asarray(x).reshape(-1, 3)
+        return [x[self.node0[i]:self.node0[i + 1]] for i in range(self.n_tissues)]
+
+    def tissue_stats(self):
+        it = np.zeros(self.n_tissues, np.int32)
+        st = np.zeros(self.n_tissues, np.int32)
+        kr = np.zeros(self.n_tissues, np.int32)
+        self._L.tf_get_tissue_stats(self._h, capi.iptr(it), capi.iptr(st), capi.iptr(kr))
+        return {"newton_iters": it, "status": st, "krylov_iters": kr}
+
+
 def simulate(t: Tissue, n_steps: Optional[int] = None, solver: Optional[NewtonRaphsonSolver] = None, **overrides):
     """Run n time steps of the path on the GPU; returns (positions, per-step stats)."""
     own = solver is None
