@@ -215,6 +215,22 @@ int tf_autotune(tf_ctx* ctx, const double* x_n, double dt);
  * context's Jacobian buffers. */
 int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_spmv);
 
+/* Discrete adjoint of the time loop (no reference counterpart; the reference has no gradients).
+ * tf_adjoint_forward runs n_steps full time steps (tf_time_step) from host positions x0 and the
+ * context's growth state, stores the positions and Fg every checkpoint_every steps on the device
+ * and writes the final positions to x_final [n_nodes*3]. tf_adjoint_backward then takes
+ * dL/dx_final [n_nodes*3] of a loss of the final positions and returns dL/d(growth rates)
+ * [n_elems*3] (the rates of tf_set_growth, constant over the steps) and, if dL_dx0 is not
+ * NULL, dL/dx0 [n_nodes*3] of the free degrees of freedom. Each segment between checkpoints
+ * is recomputed forward; each step then costs one assembly at its converged state, one solve
+ * with J^T (= J here) and hand-written element / node VJP kernels. Single tissue, no internal
+ * viscosity, no slave-master pairs; the growth rotation is held at its forward value. The
+ * growth state after tf_adjoint_backward is unspecified: set it again before the next run. */
+int tf_adjoint_forward(tf_ctx* ctx, const double* x0, int32_t n_steps, double dt,
+                       int32_t checkpoint_every, double* x_final, tf_step_stats* stats);
+int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drates, double* dL_dx0,
+                        tf_step_stats* stats);
+
 /* Text of the last error recorded on the context (no reference counterpart). */
 const char* tf_last_error(tf_ctx* ctx);
 

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtf_b200.so")
-SOURCES = ["csrc/tf_capi.cu", "csrc/tf_element.cu", "csrc/tf_krylov.cu", "csrc/tf_noalloc.cu"]
+SOURCES = ["csrc/tf_capi.cu", "csrc/tf_element.cu", "csrc/tf_krylov.cu", "csrc/tf_noalloc.cu",
+           "csrc/tf_adjoint.cu"]
 HEADERS = ["csrc/tf_internal.cuh", "../include/tf_b200.h"]
 
 NVCC_FLAGS = [

@@ -46,7 +46,7 @@ EXPORTS = [
     "tf_newton_step_device", "tf_get_pattern", "tf_assemble", "tf_solve", "tf_set_growth",
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
-    "tf_get_tissue_stats", "tf_get_n_tissues",
+    "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
 ]
 
 
@@ -128,6 +128,8 @@ def load(build_if_missing: bool = True):
     L.tf_batch_create.argtypes = [c_int, ctypes.POINTER(MeshDesc), ctypes.POINTER(Params), ctypes.POINTER(_P)]
     L.tf_get_tissue_stats.argtypes = [_P, _I, _I, _I]
     L.tf_get_n_tissues.argtypes = [_P]
+    L.tf_adjoint_forward.argtypes = [_P, _D, c_int, c_double, c_int, _D, ctypes.POINTER(StepStats)]
+    L.tf_adjoint_backward.argtypes = [_P, _D, _D, _D, ctypes.POINTER(StepStats)]
     L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p

@@ -77,6 +77,12 @@ struct tf_ctx {
     KrylovScalars* h_tsc = nullptr;  // pinned [T]
     std::vector<int32_t> t_iters, t_status, t_krylov;
     std::vector<int32_t> last_krylov;  // first-round BiCGStab iterations of each tissue, last step
+
+    // adjoint: forward checkpoints every adj_k steps, segment recompute buffers, adjoint state
+    int32_t adj_steps = 0, adj_k = 0;
+    double adj_dt = 0.0;
+    std::vector<DevBuf> cp_x, cp_fg, seg_x, seg_fg;
+    DevBuf abar, abar2, mubar, dLdr, qbuf;
     KrylovScalars* h_sc = nullptr;  // pinned
     int32_t* h_flags = nullptr;     // pinned
 
@@ -963,6 +969,10 @@ void tf_destroy(tf_ctx* ctx) {
     DevBuf* batch[] = {&ctx->node_tissue_d, &ctx->plan_cta_tissue_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d,
                        &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
     for (DevBuf* b : batch) dfree(*b);
+    for (auto* v : {&ctx->cp_x, &ctx->cp_fg, &ctx->seg_x, &ctx->seg_fg})
+        for (DevBuf& b : *v) dfree(b);
+    DevBuf* adj[] = {&ctx->abar, &ctx->abar2, &ctx->mubar, &ctx->dLdr, &ctx->qbuf};
+    for (DevBuf* b : adj) dfree(*b);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);
     if (ctx->h_du2) cudaFreeHost(ctx->h_du2);
     if (ctx->h_tsc) cudaFreeHost(ctx->h_tsc);
@@ -1271,6 +1281,144 @@ int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_sp
     }
     if (ms_spmv) *ms_spmv = tot / reps;
     return TF_OK;
+}
+
+// One implicit time step on the device: un holds x_n and ctx->fg holds Fg_n on entry; after the
+// call uk holds x_{n+1} and ctx->fg holds Fg_{n+1}.
+static int device_time_step(tf_ctx* ctx, double dt, tf_step_stats* st) {
+    int rc = prologue(ctx, dt);
+    if (rc != TF_OK) return rc;
+    tf_step_stats local;
+    std::memset(&local, 0, sizeof(local));
+    rc = newton_core(ctx, dt, &local);
+    if (st) {
+        st->newton_iters += local.newton_iters;
+        st->krylov_iters_total += local.krylov_iters_total;
+        st->krylov_iters_max = std::max(st->krylov_iters_max, local.krylov_iters_max);
+        st->ms_assemble += local.ms_assemble;
+        st->ms_solve += local.ms_solve;
+        st->status = worse(st->status, local.status);
+    }
+    return rc;
+}
+
+int tf_adjoint_forward(tf_ctx* ctx, const double* x0, int32_t n_steps, double dt, int32_t checkpoint_every,
+                       double* x_final, tf_step_stats* stats) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!x0 || !x_final || n_steps <= 0 || checkpoint_every <= 0 || !(dt > 0)) return TF_ERR_ARGUMENT;
+    if (ctx->has_visc || !ctx->slave.empty() || ctx->T != 1) return set_error(ctx, TF_ERR_UNSUPPORTED,
+        "adjoint: single tissue without internal viscosity or slave-master pairs");
+    tf_step_stats local;
+    tf_step_stats* st = stats ? stats : &local;
+    rc = call_begin(ctx, st);
+    if (rc != TF_OK) return rc;
+    const size_t bx = sizeof(double) * 3 * (size_t)ctx->N, bf = sizeof(double) * 9 * (size_t)ctx->E;
+    const int n_cp = (n_steps + checkpoint_every - 1) / checkpoint_every;
+    ctx->cp_x.resize(n_cp);
+    ctx->cp_fg.resize(n_cp);
+    for (int i = 0; i < n_cp; ++i) {
+        TF_CK(dalloc(ctx->cp_x[i], bx));
+        TF_CK(dalloc(ctx->cp_fg[i], bf));
+    }
+    ctx->adj_steps = n_steps;
+    ctx->adj_k = checkpoint_every;
+    ctx->adj_dt = dt;
+    TF_CK(cudaMemcpyAsync(ctx->un.p, x0, bx, cudaMemcpyHostToDevice, ctx->stream));
+    for (int n = 0; n < n_steps; ++n) {
+        if (n % checkpoint_every == 0) {
+            TF_CK(cudaMemcpyAsync(ctx->cp_x[n / checkpoint_every].p, ctx->un.p, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->cp_fg[n / checkpoint_every].p, ctx->fg.p, bf, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        rc = device_time_step(ctx, dt, st);
+        if (rc < 0) return rc;
+        TF_CK(cudaMemcpyAsync(ctx->un.p, ctx->uk.p, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    TF_CK(cudaMemcpyAsync(x_final, ctx->un.p, bx, cudaMemcpyDeviceToHost, ctx->stream));
+    const int rc2 = call_end(ctx, st);
+    return rc2 != TF_OK ? rc2 : st->status;
+}
+
+int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drates, double* dL_dx0,
+                        tf_step_stats* stats) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!dL_dx_final || !dL_drates) return TF_ERR_ARGUMENT;
+    if (ctx->adj_steps <= 0) return set_error(ctx, TF_ERR_STATE, "tf_adjoint_forward has not run");
+    tf_step_stats local;
+    tf_step_stats* st = stats ? stats : &local;
+    rc = call_begin(ctx, st);
+    if (rc != TF_OK) return rc;
+    const int N = ctx->N, E = ctx->E, K = ctx->adj_k, S = ctx->adj_steps;
+    const double dt = ctx->adj_dt;
+    const size_t bx = sizeof(double) * 3 * (size_t)N, bf = sizeof(double) * 9 * (size_t)E;
+    ctx->seg_x.resize(K + 1);
+    ctx->seg_fg.resize(K + 1);
+    for (int i = 0; i <= K; ++i) {
+        TF_CK(dalloc(ctx->seg_x[i], bx));
+        TF_CK(dalloc(ctx->seg_fg[i], bf));
+    }
+    TF_CK(dalloc(ctx->abar, bx));
+    TF_CK(dalloc(ctx->abar2, bx));
+    TF_CK(dalloc(ctx->mubar, bf));
+    TF_CK(dalloc(ctx->dLdr, sizeof(double) * 3 * E));
+    TF_CK(dalloc(ctx->qbuf, sizeof(double) * N));
+    TF_CK(cudaMemcpyAsync(ctx->abar.p, dL_dx_final, bx, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(launch_mask_fixed(N, dptr<uint8_t>(ctx->fixmask), dptr<double>(ctx->abar), ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->mubar.p, 0, bf, ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->dLdr.p, 0, sizeof(double) * 3 * E, ctx->stream));
+    const int n_seg = (S + K - 1) / K;
+    for (int seg = n_seg - 1; seg >= 0; --seg) {
+        const int s0 = seg * K, L = std::min(S, s0 + K) - s0;
+        // recompute the segment's states from its checkpoint
+        TF_CK(cudaMemcpyAsync(ctx->seg_x[0].p, ctx->cp_x[seg].p, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->seg_fg[0].p, ctx->cp_fg[seg].p, bf, cudaMemcpyDeviceToDevice, ctx->stream));
+        for (int j = 0; j < L; ++j) {
+            TF_CK(cudaMemcpyAsync(ctx->un.p, ctx->seg_x[j].p, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->fg.p, ctx->seg_fg[j].p, bf, cudaMemcpyDeviceToDevice, ctx->stream));
+            rc = device_time_step(ctx, dt, st);
+            if (rc < 0) return rc;
+            TF_CK(cudaMemcpyAsync(ctx->seg_x[j + 1].p, ctx->uk.p, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->seg_fg[j + 1].p, ctx->fg.p, bf, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        // adjoint steps, last to first
+        for (int j = L - 1; j >= 0; --j) {
+            const double* x_n = dptr<double>(ctx->seg_x[j]);
+            const double* x_n1 = dptr<double>(ctx->seg_x[j + 1]);
+            TF_CK(launch_set_inv_fg(dptr<ElemRecord>(ctx->elems), E, dptr<double>(ctx->seg_fg[j + 1]), ctx->stream));
+            TF_CK(launch_viscosity_surface(dptr<ElemRecord>(ctx->elems), E, N, x_n, dptr<uint8_t>(ctx->exposed),
+                                           dptr<uint8_t>(ctx->peripodial), dptr<double>(ctx->visc_surface), ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->uk.p, x_n1, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+            TF_CK(cudaMemcpyAsync(ctx->un.p, x_n, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+            rc = activate_all(ctx);
+            if (rc != TF_OK) return rc;
+            rc = assemble_system(ctx, dt);  // J at the converged state of the step
+            if (rc != TF_OK) return rc;
+            // J^T lambda = abar (J is symmetric on this path); the solve reads its RHS from g
+            TF_CK(cudaMemcpyAsync(ctx->g.p, ctx->abar.p, bx, cudaMemcpyDeviceToDevice, ctx->stream));
+            rc = krylov_solve(ctx);
+            if (rc != TF_OK) return rc;
+            const KrylovScalars sc = *ctx->h_sc;
+            st->krylov_iters_total += sc.iter;
+            st->krylov_iters_max = std::max(st->krylov_iters_max, sc.iter);
+            if (krylov_status_to_tf(sc.status) != TF_OK) st->status = worse(st->status, krylov_status_to_tf(sc.status));
+            double* lam = dptr<double>(ctx->du);
+            TF_CK(launch_mask_fixed(N, dptr<uint8_t>(ctx->fixmask), lam, ctx->stream));
+            TF_CK(launch_growth_vjp(dptr<ElemRecord>(ctx->elems), E, lam, dptr<uint8_t>(ctx->fixmask), x_n1,
+                                    dptr<double>(ctx->seg_fg[j]), dptr<double>(ctx->rates), dptr<double>(ctx->angles), dt,
+                                    dptr<double>(ctx->mubar), dptr<double>(ctx->dLdr), ctx->stream));
+            TF_CK(launch_position_vjp(dptr<ElemRecord>(ctx->elems), E, N, lam, dptr<uint8_t>(ctx->fixmask), x_n, x_n1,
+                                      dptr<double>(ctx->visc_surface), dptr<double>(ctx->ext_visc),
+                                      dptr<uint8_t>(ctx->exposed), dptr<uint8_t>(ctx->peripodial), dt,
+                                      dptr<double>(ctx->qbuf), dptr<double>(ctx->abar2), ctx->stream));
+            ctx->launches += 5;
+            std::swap(ctx->abar, ctx->abar2);
+        }
+    }
+    TF_CK(cudaMemcpyAsync(dL_drates, ctx->dLdr.p, sizeof(double) * 3 * E, cudaMemcpyDeviceToHost, ctx->stream));
+    if (dL_dx0) TF_CK(cudaMemcpyAsync(dL_dx0, ctx->abar.p, bx, cudaMemcpyDeviceToHost, ctx->stream));
+    const int rc2 = call_end(ctx, st);
+    return rc2 != TF_OK ? rc2 : st->status;
 }
 
 const char* tf_last_error(tf_ctx* ctx) { return ctx ? ctx->last_error : "null context"; }

@@ -131,6 +131,17 @@ cudaError_t launch_viscosity_surface(const ElemRecord* elems, int32_t n_elems, i
                                      const uint8_t* peripodial, double* visc_surface,
                                      cudaStream_t s);
 
+// --- adjoint (tf_adjoint.cu) ------------------------------------------------------------------
+cudaError_t launch_growth_vjp(const ElemRecord* elems, int32_t n_elems, const double* lam, const uint8_t* fixmask,
+                              const double* x1, const double* fg_n, const double* rates, const double* angles, double dt,
+                              double* mubar, double* dLdr, cudaStream_t s);
+cudaError_t launch_position_vjp(const ElemRecord* elems, int32_t n_elems, int32_t n_nodes, const double* lam,
+                                const uint8_t* fixmask, const double* x0, const double* x1, const double* visc_surface,
+                                const double* ext_visc, const uint8_t* exposed, const uint8_t* peripodial, double dt,
+                                double* q, double* abar, cudaStream_t s);
+cudaError_t launch_set_inv_fg(ElemRecord* elems, int32_t n_elems, const double* fg, cudaStream_t s);
+cudaError_t launch_mask_fixed(int32_t n_nodes, const uint8_t* fixmask, double* v, cudaStream_t s);
+
 // --- Krylov (tf_krylov.cu) ----------------------------------------------------------------
 struct KrylovWork {
     int32_t n_nodes;

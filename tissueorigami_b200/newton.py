@@ -151,6 +151,26 @@ class NewtonRaphsonSolver:
                                          ctypes.byref(it), ctypes.byref(rr)), "tf_solve", self._h)
         return du, rc, it.value, rr.value
 
+    # -- discrete adjoint ------------------------------------------------------------------------
+    def adjoint_forward(self, x0, n_steps: int, dt: float, checkpoint_every: int = 5):
+        """Run n_steps time steps from x0 keeping checkpoints; returns (x_final, status, stats)."""
+        x = _f64(x0).reshape(self.n_nodes, 3).copy()
+        out = np.empty_like(x)
+        st = capi.StepStats()
+        rc = capi.check(self._L.tf_adjoint_forward(self._h, capi.dptr(x), int(n_steps), float(dt), int(checkpoint_every),
+                                                   capi.dptr(out), ctypes.byref(st)), "tf_adjoint_forward", self._h)
+        return out, rc, st.as_dict()
+
+    def adjoint_backward(self, dL_dx_final, want_dx0: bool = False):
+        """dL/d(growth rates) [E,3] (and dL/dx0 [N,3]) for dL/dx_final of the last forward run."""
+        g = _f64(dL_dx_final).reshape(-1).copy()
+        dr = np.zeros((self.n_elems, 3))
+        dx0 = np.zeros((self.n_nodes, 3)) if want_dx0 else None
+        st = capi.StepStats()
+        rc = capi.check(self._L.tf_adjoint_backward(self._h, capi.dptr(g), capi.dptr(dr), capi.dptr(dx0), ctypes.byref(st)),
+                        "tf_adjoint_backward", self._h)
+        return dr, dx0, rc, st.as_dict()
+
     def schedule(self):
         nc, sc, t = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         self._L.tf_get_schedule(self._h, ctypes.byref(nc), ctypes.byref(sc), ctypes.byref(t))
