@@ -398,6 +398,67 @@ def run_batch(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args) -> None:
+    """Adjoint growth-map fit on the wing disc: per-element growth rates from a 32x32 bilinear
+    grid (1024 parameters), loss = squared node-position misfit after 20 steps against the shape
+    a seeded hidden grid produces, checkpoint every 5 steps. Reports the cost of one gradient
+    (forward with checkpoints + adjoint backward) against one plain forward run."""
+    from tissueorigami_b200 import capi, mesh
+    from tissueorigami_b200.newton import NewtonRaphsonSolver
+
+    t = mesh.wing_disc()
+    n_steps, k, grid = 20, 5, 32
+    idx, w = mesh.bilinear_growth_weights(t, grid)
+    rng = np.random.default_rng(1004)
+    gx, gy = np.meshgrid(np.linspace(t.x[:, 0].min(), t.x[:, 0].max(), grid),
+                         np.linspace(t.x[:, 1].min(), t.x[:, 1].max(), grid), indexing="xy")
+    rho2 = (gx ** 2 + gy ** 2).ravel()
+    hidden = 2e-4 * np.exp(-rho2 / (2 * 40.0 ** 2)) * (1 + rng.uniform(-0.1, 0.1, grid * grid))
+    theta = hidden * (1 + rng.uniform(-0.2, 0.2, grid * grid))
+
+    def rates(p):
+        r = (w * p[idx]).sum(axis=1)
+        out = np.zeros((t.n_elems, 3))
+        out[:, 0] = r
+        out[:, 1] = r
+        return out
+
+    s = NewtonRaphsonSolver.from_tissue(t)
+    s.set_growth(t.fg, rates(hidden), t.angles)
+    target, rc, _ = s.adjoint_forward(t.x, n_steps, t.dt, k)
+    fwd_ms, grad_ms, plain_ms, worst = [], [], [], rc
+    for rep in range(args.warmup + args.steps):
+        s.set_growth(t.fg, rates(theta), t.angles)
+        x = t.x.copy()
+        pm = 0.0
+        for _ in range(n_steps):
+            x, rc, st = s.runOneStep(x, t.dt)
+            pm += st["ms_total"]
+            worst = max(worst, rc)
+        s.set_growth(t.fg, rates(theta), t.angles)
+        xf, rc, stf = s.adjoint_forward(t.x, n_steps, t.dt, k)
+        dr, _, rcb, stb = s.adjoint_backward(2 * (xf - target))
+        worst = max(worst, rc, rcb)
+        if rep >= args.warmup:
+            plain_ms.append(pm)
+            fwd_ms.append(stf["ms_total"])
+            grad_ms.append(stf["ms_total"] + stb["ms_total"])
+    s.close()
+    dtheta = np.zeros(grid * grid)
+    np.add.at(dtheta, idx.ravel(), (w * (dr[:, 0] + dr[:, 1])[:, None]).ravel())
+    line = {
+        "metric": "adjoint gradient cost / one forward run", "value": float(np.mean(grad_ms) / np.mean(plain_ms)),
+        "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "dtype": "f64", "data": "synthetic (seeded disc, hidden and current 32x32 growth grids)",
+        "config": {"workload": f"adjoint fit: wing_disc {t.n_elems} prisms, 1024 grid parameters, {n_steps} steps, "
+                               f"checkpoint every {k}"},
+        "ms_plain_forward": float(np.mean(plain_ms)), "ms_forward_with_checkpoints": float(np.mean(fwd_ms)),
+        "ms_gradient": float(np.mean(grad_ms)), "grad_norm": float(np.linalg.norm(dtheta)),
+        "status_worst": int(worst),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def load_traffic():
     """Per-launch DRAM bytes from committed ncu summaries (profiles/traffic.tsv:
     kernel<TAB>workload<TAB>bytes_per_launch); missing entries read as null."""
@@ -431,6 +492,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_b200(args)
 

@@ -29,6 +29,10 @@ import numpy as np
 BASAL, APICAL, MIDLINE, LATERAL = 0, 1, 2, 3
 # element exposure bits used by the viscosity-surface update (Prism.cpp:1650-1709)
 EXPOSED_APICAL, EXPOSED_BASAL = 1, 2
+# External viscosities of the reference's wing-disc runs (DiscProperApicalExternalViscosity 16000,
+# DiscProperBasalExternalViscosity 10 in tests/sim_no_pardiso_reg/run07008/modelinput07008), used
+# for the disc, slab and batch tissues whose drag the workload does not state.
+WING_DISC_APICAL_VISC, WING_DISC_BASAL_VISC = 16000.0, 10.0
 
 
 @dataclasses.dataclass
@@ -260,13 +264,15 @@ def _renumber_points(pts2: np.ndarray, tri: np.ndarray, flags: List[np.ndarray])
 
 def wing_disc(seed: int = 1001, radius: float = 100.0, n_surface_points: int = 20000,
               ecm: float = 2.0, columnar: float = 25.0, E_col: float = 1000.0,
-              E_ecm: float = 4000.0, nu: float = 0.3, ext_visc: float = 10.0,
+              E_ecm: float = 4000.0, nu: float = 0.3, apical_visc: float = WING_DISC_APICAL_VISC,
+              basal_visc: float = WING_DISC_BASAL_VISC,
               peak_growth: float = 2e-4, sigma: float = 40.0, noise: float = 0.1,
               dt: float = 60.0, n_steps: int = 50, newton_tol: float = 1e-8) -> Tissue:
     """Wing-disc-like disc: Delaunay-triangulated disc of radius 100 um from seeded points
     (~40k triangles), extruded into a 2 um ECM layer (E=4000 Pa) under a 25 um columnar layer
     (E=1000 Pa), ~80k prisms, nu=0.3; radial Gaussian in-plane growth, peak 2e-4 /s at the
-    centre, sigma 40 um, times a uniform-random +-10 % per element; rim clamped; dt 60 s."""
+    centre, sigma 40 um, times a uniform-random +-10 % per element; rim clamped; dt 60 s; apical /
+    basal external viscosity of the reference's wing-disc runs (16000 / 10 Pa s)."""
     rng = np.random.default_rng(seed)
     pts2, is_rim = _disc_points(rng, radius, n_surface_points)
     tri = _delaunay(pts2)
@@ -285,7 +291,7 @@ def wing_disc(seed: int = 1001, radius: float = 100.0, n_surface_points: int = 2
     rates[:, 0] = r
     rates[:, 1] = r
     return Tissue("wing_disc", conn, xref, x, lam, mu, np.zeros(conn.shape[0]), fixed,
-                  _ext_visc(place, at_circ, ext_visc, ext_visc), _element_exposure(layer, 2),
+                  _ext_visc(place, at_circ, apical_visc, basal_visc), _element_exposure(layer, 2),
                   np.zeros(conn.shape[0], np.uint8), rates, np.zeros(conn.shape[0]), place,
                   at_circ, dt=dt, n_steps=n_steps, newton_tol=newton_tol, seed=seed)
 
@@ -301,8 +307,9 @@ def _smooth_field(rng: np.random.Generator, xy: np.ndarray, length: float, n_fea
 
 def large_slab(seed: int = 1002, nx: int = 1000, ny: int = 500, spacing: float = 0.5,
                layer_thickness: float = 1.0, n_layers: int = 3, E_median: float = 1000.0,
-               sigma_log: float = 0.3, nu: float = 0.3, ext_visc: float = 10.0,
-               r1: float = 2e-4, r2: float = 5e-5, angle_length: float = 20.0,
+               sigma_log: float = 0.3, nu: float = 0.3, apical_visc: float = WING_DISC_APICAL_VISC,
+               basal_visc: float = WING_DISC_BASAL_VISC, r1: float = 2e-4, r2: float = 5e-5,
+               angle_length: float = 20.0,
                dt: float = 60.0, n_steps: int = 20, newton_tol: float = 1e-8) -> Tissue:
     """Large slab: 1000x500-node rectangle at 0.5 um spacing, triangulated and extruded into
     3 layers (2,991,006 prisms); log-normal stiffness per element (median 1000 Pa,
@@ -334,14 +341,15 @@ def large_slab(seed: int = 1002, nx: int = 1000, ny: int = 500, spacing: float =
     rates[:, 0] = r1
     rates[:, 1] = r2
     return Tissue("large_slab", conn, xref, x, lam, mu, np.zeros(conn.shape[0]), fixed,
-                  _ext_visc(place, at_circ, ext_visc, ext_visc),
+                  _ext_visc(place, at_circ, apical_visc, basal_visc),
                   _element_exposure(layer, n_layers), np.zeros(conn.shape[0], np.uint8), rates,
                   ang, place, at_circ, dt=dt, n_steps=n_steps, newton_tol=newton_tol, seed=seed)
 
 
 def small_disc(seed: int, n_prisms: int, E: float, growth_length: float = 20.0,
                peak_growth: float = 2e-4, thickness: float = 10.0, nu: float = 0.3,
-               ext_visc: float = 10.0, dt: float = 60.0, n_steps: int = 30) -> Tissue:
+               apical_visc: float = WING_DISC_APICAL_VISC, basal_visc: float = WING_DISC_BASAL_VISC,
+               dt: float = 60.0, n_steps: int = 30) -> Tissue:
     """One-layer disc with about n_prisms prisms (radius grows with the count), rim clamped,
     growth from a seeded smooth random field (RBF length scale growth_length)."""
     rng = np.random.default_rng(seed)
@@ -363,7 +371,7 @@ def small_disc(seed: int, n_prisms: int, E: float, growth_length: float = 20.0,
     rates[:, 0] = r
     rates[:, 1] = r
     return Tissue("small_disc", conn, xref, x, lam, mu, np.zeros(conn.shape[0]), fixed,
-                  _ext_visc(place, at_circ, ext_visc, ext_visc), _element_exposure(layer, 1),
+                  _ext_visc(place, at_circ, apical_visc, basal_visc), _element_exposure(layer, 1),
                   np.zeros(conn.shape[0], np.uint8), rates, np.zeros(conn.shape[0]), place,
                   at_circ, dt=dt, n_steps=n_steps, seed=seed)
 
@@ -378,6 +386,7 @@ def small_rect_sized(seed: int, n_prisms: int, E: float, growth_length: float = 
     nx = max(2, int(round(n_prisms / (2.0 * (ny - 1)))) + 1)
     t = small_rectangle(seed=seed, nx=nx, ny=ny, E=E, n_steps=n_steps, newton_tol=1e-8)
     t.fixed[t.at_circumference != 0, :] = 1
+    t.ext_visc = _ext_visc(t.node_placement, t.at_circumference, WING_DISC_APICAL_VISC, WING_DISC_BASAL_VISC)
     cen = t.xref.reshape(-1, 6, 3).mean(axis=1)
     field = _smooth_field(rng, cen[:, :2], growth_length)
     r = peak_growth * (0.5 + 0.25 * np.tanh(field))
