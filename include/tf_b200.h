@@ -90,6 +90,9 @@ typedef struct tf_step_stats {
     double ms_solve;            /* device time in the linear solves                         */
     double ms_total;            /* device time of the whole call, host copies included      */
     int64_t gpu_launches;       /* kernels this call launched (graph nodes counted)         */
+    double ms_solve_kernel;     /* device time inside the persistent BiCGStab launches      */
+    int32_t solve_launches;     /* number of those launches                                 */
+    int32_t reserved;
 } tf_step_stats;
 
 /* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), BiCGStab
@@ -179,6 +182,14 @@ int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, doub
  * g and du [n_nodes*3]. iters / rel_res may be NULL. */
 int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, int32_t* iters,
              double* rel_res);
+
+/* Direct alternative to tf_solve, timed beside it: the same J du = g factorised and solved on
+ * the GPU by cuSOLVER's sparse Cholesky (QR when Cholesky meets a non-positive pivot), the way
+ * the reference refactorises every system with Pardiso (NewtonRaphsonSolver.cpp:498-763).
+ * ms_factor_solve receives the device time of factorisation + solve, method 1 (Cholesky) or 2
+ * (QR); either may be NULL. Returns TF_KRYLOV_BREAKDOWN when the matrix is singular. */
+int tf_solve_direct(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du,
+                    double* ms_factor_solve, int32_t* method);
 
 /* Growth state for the per-step prologue on the device: fg [n_elems*9] (ShapeBase::Fg),
  * rates [n_elems*3] growth rates in 1/s and angles [n_elems] in radians with the uniform

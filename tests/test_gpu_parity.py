@@ -188,3 +188,51 @@ def test_schedule_and_autotune():
         assert tuned["elems_per_block"] in (8, 16, 32)
         me, ms = s.time_kernels(5)
         assert me > 0 and ms > 0
+
+
+def test_direct_solve_matches_scipy_and_krylov():
+    """tf_solve_direct (cuSOLVER sparse Cholesky / QR) against SuperLU and against BiCGStab."""
+    t = mesh.small_disc(7, 1500, 1200.0)
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
+    du_ref = sla.spsolve(O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc(), g)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13) as s:
+        du_d, rc_d, ms, method = s.solve_direct(vals, g)
+        du_k, rc_k, _, _ = s.solveForDeltaU(vals, g)
+    assert rc_d == capi.TF_OK and method in (1, 2) and ms > 0
+    assert np.linalg.norm(du_d - du_ref) / np.linalg.norm(du_ref) < 1e-10
+    assert np.linalg.norm(du_k - du_d) / np.linalg.norm(du_d) < 1e-8
+
+
+def test_ilu0_solve_matches_direct_with_fewer_iterations():
+    """Multicolour block ILU(0)-preconditioned BiCGStab: same solution as SuperLU (1e-8 relative),
+    and no more iterations than the block-Jacobi preconditioner needs."""
+    t = mesh.small_disc(7, 1500, 1200.0)
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
+    du_ref = sla.spsolve(O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc(), g)
+    iters = {}
+    for pc in (capi.TF_PRECOND_BLOCK_JACOBI, capi.TF_PRECOND_ILU0):
+        with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, precond=pc, persistent=0) as s:
+            du, rc, it, rr = s.solveForDeltaU(vals, g)
+        assert rc == capi.TF_OK and rr <= 1e-13
+        assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
+        iters[pc] = it
+    assert iters[capi.TF_PRECOND_ILU0] <= iters[capi.TF_PRECOND_BLOCK_JACOBI]
+
+
+def test_ilu0_time_steps_match_oracle():
+    """Three implicit steps of a small disc with the ILU(0) preconditioner: positions within 1e-9
+    of the tissue size of the oracle's sparse-LU run."""
+    t = mesh.small_disc(11, 3000, 2000.0, n_steps=3)
+    x_ref, fg_ref, it_ref, _ = O.simulate_sparse(t, n_steps=3)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14, precond=capi.TF_PRECOND_ILU0) as s:
+        x = t.x.copy()
+        for _ in range(3):
+            x, rc, st = s.runOneStep(x, t.dt)
+            assert rc == capi.TF_OK
+    assert np.abs(x - x_ref).max() <= 1e-9 * t.size

@@ -14,7 +14,8 @@ ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtf_b200.so")
 SOURCES = ["csrc/tf_capi.cu", "csrc/tf_element.cu", "csrc/tf_krylov.cu", "csrc/tf_noalloc.cu",
-           "csrc/tf_adjoint.cu"]
+           "csrc/tf_adjoint.cu", "csrc/tf_direct.cu"]
+LIBS = ["-lcusolver", "-lcusparse"]
 HEADERS = ["csrc/tf_internal.cuh", "../include/tf_b200.h"]
 
 NVCC_FLAGS = [
@@ -44,7 +45,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB_PATH
     os.makedirs(LIB_DIR, exist_ok=True)
     tmp = LIB_PATH + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, "-o", tmp, *SOURCES]
+    cmd = [_nvcc(), *NVCC_FLAGS, "-o", tmp, *SOURCES, *LIBS]
     res = subprocess.run(cmd, cwd=HERE, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)

@@ -47,6 +47,7 @@ EXPORTS = [
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
+    "tf_solve_direct",
 ]
 
 
@@ -68,7 +69,9 @@ class StepStats(ctypes.Structure):
                 ("krylov_iters_max", ctypes.c_int32), ("status", ctypes.c_int32),
                 ("du_norm", ctypes.c_double * 32), ("krylov_rel_res", ctypes.c_double * 32),
                 ("ms_assemble", ctypes.c_double), ("ms_solve", ctypes.c_double),
-                ("ms_total", ctypes.c_double), ("gpu_launches", ctypes.c_int64)]
+                ("ms_total", ctypes.c_double), ("gpu_launches", ctypes.c_int64),
+                ("ms_solve_kernel", ctypes.c_double), ("solve_launches", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
     def as_dict(self):
         n = min(self.newton_iters, 32)
@@ -76,7 +79,8 @@ class StepStats(ctypes.Structure):
                 "krylov_iters_max": self.krylov_iters_max, "status": self.status,
                 "du_norm": list(self.du_norm[:n]), "krylov_rel_res": list(self.krylov_rel_res[:n]),
                 "ms_assemble": self.ms_assemble, "ms_solve": self.ms_solve, "ms_total": self.ms_total,
-                "gpu_launches": int(self.gpu_launches)}
+                "gpu_launches": int(self.gpu_launches), "ms_solve_kernel": self.ms_solve_kernel,
+                "solve_launches": int(self.solve_launches)}
 
 
 _lib = None
@@ -130,6 +134,7 @@ def load(build_if_missing: bool = True):
     L.tf_get_n_tissues.argtypes = [_P]
     L.tf_adjoint_forward.argtypes = [_P, _D, c_int, c_double, c_int, _D, ctypes.POINTER(StepStats)]
     L.tf_adjoint_backward.argtypes = [_P, _D, _D, _D, ctypes.POINTER(StepStats)]
+    L.tf_solve_direct.argtypes = [_P, _D, _D, _D, _D, _I]
     L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p

@@ -78,6 +78,12 @@ struct tf_ctx {
     std::vector<int32_t> t_iters, t_status, t_krylov;
     std::vector<int32_t> last_krylov;  // first-round BiCGStab iterations of each tissue, last step
 
+    // multicolour block ILU(0) (precond == TF_PRECOND_ILU0)
+    std::vector<int32_t> ilu_colour_ptr;
+    int32_t ilu_colours = 0;
+    DevBuf ilu_cnodes, ilu_lo_ptr, ilu_lo_idx, ilu_up_ptr, ilu_up_idx, ilu_lu, ilu_uinv, ilu_y;
+    cudaGraphExec_t ilu_graph = nullptr;
+
     // adjoint: forward checkpoints every adj_k steps, segment recompute buffers, adjoint state
     int32_t adj_steps = 0, adj_k = 0;
     double adj_dt = 0.0;
@@ -93,6 +99,9 @@ struct tf_ctx {
     cudaGraphExec_t krylov_graph = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_call[2] = {nullptr, nullptr};  // brackets a whole public call
+    cudaEvent_t ev_solve[2] = {nullptr, nullptr}; // brackets one persistent solve launch
+    double solve_kernel_ms = 0.0;                 // accumulated over the current call
+    int32_t solve_kernel_launches = 0;
     int64_t launches = 0;                         // kernels launched by the current call
     char last_error[256] = {0};
 };
@@ -282,6 +291,8 @@ void build_colouring(tf_ctx* c, const std::vector<int32_t>& routed) {
     c->n_colours = ncol;
 }
 
+int build_ilu(tf_ctx* ctx);
+
 int upload_structure(tf_ctx* ctx) {
     const int N = ctx->N, E = ctx->E;
     build_pattern(ctx);
@@ -350,6 +361,10 @@ int upload_structure(tf_ctx* ctx) {
         TF_CK(cudaMemcpy(ctx->slaves_d.p, ctx->slave.data(), sizeof(int32_t) * ctx->slave.size(), cudaMemcpyHostToDevice));
         TF_CK(cudaMemcpy(ctx->masters_d.p, ctx->master.data(), sizeof(int32_t) * ctx->master.size(), cudaMemcpyHostToDevice));
     }
+    if (ctx->params.precond == TF_PRECOND_ILU0) {
+        const int irc = build_ilu(ctx);
+        if (irc != TF_OK) return irc;
+    }
     const size_t np2 = std::max((size_t)std::max(spmv_grid(N), vec_grid(N)) * 2,
                                 (size_t)ctx->persistent_grid_max * 4) + 64;
     TF_CK(dalloc(ctx->partials, sizeof(double) * np2));
@@ -358,6 +373,81 @@ int upload_structure(tf_ctx* ctx) {
         ctx->krylov_graph = nullptr;
     }
     return TF_OK;
+}
+
+// Multicolour structure of ILU(0): greedy colouring of the block-row graph (two rows share a
+// colour only if the pattern has no block between them), nodes sorted by colour, and for every
+// row its lower blocks (earlier colour, sorted by colour) and upper blocks (later colour).
+int build_ilu(tf_ctx* ctx) {
+    const int N = ctx->N;
+    std::vector<int32_t> col(N, -1);
+    int ncol = 0;
+    std::vector<char> used;
+    for (int i = 0; i < N; ++i) {
+        used.assign(ncol + 1, 0);
+        for (int k = ctx->rowptr[i]; k < ctx->rowptr[i + 1]; ++k) {
+            const int c = col[ctx->colidx[k]];
+            if (c >= 0) used[c] = 1;
+        }
+        int c = 0;
+        while (c < ncol && used[c]) ++c;
+        col[i] = c;
+        ncol = std::max(ncol, c + 1);
+    }
+    std::vector<int32_t> cptr(ncol + 1, 0), cnodes(N);
+    for (int i = 0; i < N; ++i) cptr[col[i] + 1]++;
+    for (int c = 0; c < ncol; ++c) cptr[c + 1] += cptr[c];
+    std::vector<int32_t> pos(cptr.begin(), cptr.end() - 1);
+    for (int i = 0; i < N; ++i) cnodes[pos[col[i]]++] = i;
+    std::vector<int32_t> lo_ptr(N + 1, 0), up_ptr(N + 1, 0), lo_idx, up_idx;
+    for (int i = 0; i < N; ++i) {
+        std::vector<std::pair<int, int>> lo;
+        for (int k = ctx->rowptr[i]; k < ctx->rowptr[i + 1]; ++k) {
+            const int c = col[ctx->colidx[k]];
+            if (ctx->colidx[k] == i) continue;
+            if (c < col[i]) lo.emplace_back(c, k);
+            else up_idx.push_back(k);
+        }
+        std::sort(lo.begin(), lo.end());
+        for (auto& q : lo) lo_idx.push_back(q.second);
+        lo_ptr[i + 1] = (int32_t)lo_idx.size();
+        up_ptr[i + 1] = (int32_t)up_idx.size();
+    }
+    ctx->ilu_colour_ptr = cptr;
+    ctx->ilu_colours = ncol;
+    auto up = [&](DevBuf& b, const std::vector<int32_t>& v) -> cudaError_t {
+        cudaError_t e = dalloc(b, sizeof(int32_t) * std::max<size_t>(1, v.size()));
+        if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(b.p, v.data(), sizeof(int32_t) * v.size(), cudaMemcpyHostToDevice);
+        return e;
+    };
+    TF_CK(up(ctx->ilu_cnodes, cnodes));
+    TF_CK(up(ctx->ilu_lo_ptr, lo_ptr));
+    TF_CK(up(ctx->ilu_lo_idx, lo_idx));
+    TF_CK(up(ctx->ilu_up_ptr, up_ptr));
+    TF_CK(up(ctx->ilu_up_idx, up_idx));
+    TF_CK(dalloc(ctx->ilu_lu, sizeof(double) * 9 * (size_t)ctx->nnzb));
+    TF_CK(dalloc(ctx->ilu_uinv, sizeof(double) * 9 * (size_t)N));
+    TF_CK(dalloc(ctx->ilu_y, sizeof(double) * 3 * (size_t)N));
+    if (ctx->ilu_graph) {
+        cudaGraphExecDestroy(ctx->ilu_graph);
+        ctx->ilu_graph = nullptr;
+    }
+    return TF_OK;
+}
+
+IluPlan make_ilu(tf_ctx* c) {
+    IluPlan p;
+    p.n_colours = c->ilu_colours;
+    p.colour_ptr = c->ilu_colour_ptr.data();
+    p.cnodes = dptr<int32_t>(c->ilu_cnodes);
+    p.lo_ptr = dptr<int32_t>(c->ilu_lo_ptr);
+    p.lo_idx = dptr<int32_t>(c->ilu_lo_idx);
+    p.up_ptr = dptr<int32_t>(c->ilu_up_ptr);
+    p.up_idx = dptr<int32_t>(c->ilu_up_idx);
+    p.lu = dptr<double>(c->ilu_lu);
+    p.uinv = dptr<double>(c->ilu_uinv);
+    p.y = dptr<double>(c->ilu_y);
+    return p;
 }
 
 KrylovWork make_work(tf_ctx* c) {
@@ -555,7 +645,10 @@ int krylov_status_to_tf(int ks) {
     }
 }
 
-bool use_persistent(tf_ctx* ctx) { return ctx->persistent_grid_max > 0 && (ctx->params.persistent || ctx->T > 1); }
+bool use_persistent(tf_ctx* ctx) {
+    return ctx->params.precond == TF_PRECOND_BLOCK_JACOBI && ctx->persistent_grid_max > 0 &&
+           (ctx->params.persistent || ctx->T > 1);
+}
 
 // Solve J du = g (buffers in the context) for every active tissue. Leaves the scalars in
 // ctx->h_tsc[T] (persistent) or ctx->h_sc (chunked, single tissue).
@@ -563,12 +656,20 @@ int krylov_solve(tf_ctx* ctx) {
     KrylovWork w = make_work(ctx);
     if (use_persistent(ctx)) {
         const BatchPlan plan = make_plan(ctx);
+        TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
         TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters, ctx->stream));
+        TF_CK(cudaEventRecord(ctx->ev_solve[1], ctx->stream));
         ctx->launches += 1;
         TF_CK(cudaMemcpyAsync(ctx->h_tsc, ctx->tscalars.p, sizeof(KrylovScalars) * ctx->T, cudaMemcpyDeviceToHost,
                               ctx->stream));
         TF_CK(cudaMemcpyAsync(ctx->h_flags, ctx->dflags.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
         TF_CK(cudaStreamSynchronize(ctx->stream));
+        {
+            float kms = 0.0f;
+            TF_CK(cudaEventElapsedTime(&kms, ctx->ev_solve[0], ctx->ev_solve[1]));
+            ctx->solve_kernel_ms += kms;
+            ctx->solve_kernel_launches += 1;
+        }
         if (*ctx->h_flags & DF_BARRIER_TIMEOUT) {
             TF_CK(cudaMemsetAsync(ctx->tbarriers.p, 0, sizeof(GridBarrier) * ctx->T, ctx->stream));
             TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
@@ -577,9 +678,43 @@ int krylov_solve(tf_ctx* ctx) {
         *ctx->h_sc = ctx->h_tsc[0];
         return TF_OK;
     }
-    TF_CK(launch_block_jacobi_setup(w, ctx->stream));
+    const bool ilu = ctx->params.precond == TF_PRECOND_ILU0;
+    if (ilu) {
+        TF_CK(cudaMemcpyAsync(ctx->ilu_lu.p, ctx->vals.p, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+        TF_CK(launch_ilu_factor(w, make_ilu(ctx), ctx->stream));
+        ctx->launches += ctx->ilu_colours;
+    } else {
+        TF_CK(launch_block_jacobi_setup(w, ctx->stream));
+        ctx->launches += 1;
+    }
     TF_CK(launch_krylov_init(w, ctx->params.krylov_rtol, ctx->params.krylov_max_iters, ctx->stream));
-    ctx->launches += 2;
+    ctx->launches += 1;
+    if (ilu) {
+        const IluPlan ip = make_ilu(ctx);
+        if (ctx->params.use_graphs && !ctx->ilu_graph) {
+            cudaGraph_t graph;
+            TF_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            for (int i = 0; i < kChunk; ++i) launch_bicgstab_iteration_ilu(w, ip, ctx->stream);
+            cudaError_t cerr = cudaStreamEndCapture(ctx->stream, &graph);
+            TF_CK(cerr);
+            cerr = cudaGraphInstantiate(&ctx->ilu_graph, graph, 0);
+            cudaGraphDestroy(graph);
+            TF_CK(cerr);
+        }
+        const int max_chunks = ctx->params.krylov_max_iters / kChunk + 2;
+        for (int ch = 0; ch < max_chunks; ++ch) {
+            if (ctx->params.use_graphs)
+                TF_CK(cudaGraphLaunch(ctx->ilu_graph, ctx->stream));
+            else
+                for (int i = 0; i < kChunk; ++i) TF_CK(launch_bicgstab_iteration_ilu(w, ip, ctx->stream));
+            ctx->launches += (int64_t)kChunk * (5 + 4 * ctx->ilu_colours);
+            TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+            TF_CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->h_sc->status != KS_RUNNING) break;
+        }
+        return TF_OK;
+    }
     if (ctx->params.use_graphs && !ctx->krylov_graph) {
         cudaGraph_t graph;
         TF_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -730,6 +865,8 @@ int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
 int call_begin(tf_ctx* ctx, tf_step_stats* st) {
     std::memset(st, 0, sizeof(*st));
     ctx->launches = 0;
+    ctx->solve_kernel_ms = 0.0;
+    ctx->solve_kernel_launches = 0;
     TF_CK(cudaEventRecord(ctx->ev_call[0], ctx->stream));
     return TF_OK;
 }
@@ -741,6 +878,8 @@ int call_end(tf_ctx* ctx, tf_step_stats* st) {
     TF_CK(cudaEventElapsedTime(&ms, ctx->ev_call[0], ctx->ev_call[1]));
     st->ms_total = ms;
     st->gpu_launches = ctx->launches;
+    st->ms_solve_kernel = ctx->solve_kernel_ms;
+    st->solve_launches = ctx->solve_kernel_launches;
     return TF_OK;
 }
 
@@ -825,13 +964,15 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         ctx->params = *params;
     else
         tf_default_params(&ctx->params);
-    if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI) return TF_ERR_UNSUPPORTED;
+    if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI && !(ctx->params.precond == TF_PRECOND_ILU0 && T == 1))
+        return TF_ERR_UNSUPPORTED;
     if (ctx->params.krylov_max_iters <= 0 || ctx->params.max_newton_iters < 0) return TF_ERR_ARGUMENT;
     ctx->device = ctx->params.device;
     TF_CK(cudaSetDevice(ctx->device));
     TF_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     for (auto& e : ctx->ev) TF_CK(cudaEventCreate(&e));
     for (auto& e : ctx->ev_call) TF_CK(cudaEventCreate(&e));
+    for (auto& e : ctx->ev_solve) TF_CK(cudaEventCreate(&e));
     ctx->N = mesh->n_nodes;
     ctx->E = mesh->n_elems;
     ctx->conn.assign(mesh->conn, mesh->conn + (size_t)ctx->E * 6);
@@ -971,8 +1112,10 @@ void tf_destroy(tf_ctx* ctx) {
     for (DevBuf* b : batch) dfree(*b);
     for (auto* v : {&ctx->cp_x, &ctx->cp_fg, &ctx->seg_x, &ctx->seg_fg})
         for (DevBuf& b : *v) dfree(b);
-    DevBuf* adj[] = {&ctx->abar, &ctx->abar2, &ctx->mubar, &ctx->dLdr, &ctx->qbuf};
+    DevBuf* adj[] = {&ctx->abar, &ctx->abar2, &ctx->mubar, &ctx->dLdr, &ctx->qbuf, &ctx->ilu_cnodes, &ctx->ilu_lo_ptr,
+                     &ctx->ilu_lo_idx, &ctx->ilu_up_ptr, &ctx->ilu_up_idx, &ctx->ilu_lu, &ctx->ilu_uinv, &ctx->ilu_y};
     for (DevBuf* b : adj) dfree(*b);
+    if (ctx->ilu_graph) cudaGraphExecDestroy(ctx->ilu_graph);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);
     if (ctx->h_du2) cudaFreeHost(ctx->h_du2);
     if (ctx->h_tsc) cudaFreeHost(ctx->h_tsc);
@@ -981,6 +1124,8 @@ void tf_destroy(tf_ctx* ctx) {
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : ctx->ev_call)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->ev_solve)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1281,6 +1426,29 @@ int tf_time_kernels(tf_ctx* ctx, int32_t reps, double* ms_element, double* ms_sp
     }
     if (ms_spmv) *ms_spmv = tot / reps;
     return TF_OK;
+}
+
+int tf_solve_direct(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, double* ms_factor_solve,
+                    int32_t* method) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!bsr_vals || !g || !du) return TF_ERR_ARGUMENT;
+    if (!ctx->slave.empty()) return set_error(ctx, TF_ERR_UNSUPPORTED, "direct solve: no slave-master pairs");
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(cudaMemcpyAsync(ctx->vals.p, bsr_vals, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->g.p, g, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    float ms = 0.0f;
+    int m = 0;
+    const int drc = direct_solve_bsr3(ctx->N, ctx->nnzb, dptr<int32_t>(ctx->rowptr_d), dptr<int32_t>(ctx->colidx_d),
+                                      dptr<double>(ctx->vals), dptr<double>(ctx->g), dptr<double>(ctx->du), ctx->stream,
+                                      &ms, &m);
+    if (drc == -3) return set_error(ctx, TF_ERR_OUT_OF_MEMORY, "direct solve: CSR buffers");
+    if (drc < 0) return set_error(ctx, TF_ERR_CUDA, "direct solve: cuSOLVER failure");
+    TF_CK(cudaMemcpyAsync(du, ctx->du.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    if (ms_factor_solve) *ms_factor_solve = ms;
+    if (method) *method = m;
+    return drc == 3 ? TF_KRYLOV_BREAKDOWN : TF_OK;
 }
 
 // One implicit time step on the device: un holds x_n and ctx->fg holds Fg_n on entry; after the

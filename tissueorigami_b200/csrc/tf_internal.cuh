@@ -142,6 +142,12 @@ cudaError_t launch_position_vjp(const ElemRecord* elems, int32_t n_elems, int32_
 cudaError_t launch_set_inv_fg(ElemRecord* elems, int32_t n_elems, const double* fg, cudaStream_t s);
 cudaError_t launch_mask_fixed(int32_t n_nodes, const uint8_t* fixmask, double* v, cudaStream_t s);
 
+// --- direct solve (tf_direct.cu) -----------------------------------------------------------
+// 0 ok, 3 singular, < 0 CUDA / cuSOLVER failure; ms = factorise + solve time; method 1 = Cholesky,
+// 2 = QR.
+int direct_solve_bsr3(int32_t n_nodes, int64_t nnzb, const int32_t* rowptr, const int32_t* colidx, const double* vals,
+                      const double* b, double* x, cudaStream_t s, float* ms, int* method);
+
 // --- Krylov (tf_krylov.cu) ----------------------------------------------------------------
 struct KrylovWork {
     int32_t n_nodes;
@@ -160,6 +166,22 @@ struct KrylovWork {
 
 cudaError_t launch_find_diag(const int32_t* rowptr, const int32_t* colidx, int32_t n, int32_t* diag,
                              int32_t* dflags, cudaStream_t s);
+// Multicolour block ILU(0) on the BSR3 pattern. Nodes of one colour never couple, so every
+// colour class is factorised / solved in parallel once the earlier classes are done.
+struct IluPlan {
+    int32_t n_colours;
+    const int32_t* colour_ptr;    // host: offsets into nodes by colour [n_colours+1]
+    const int32_t* cnodes;        // device: nodes sorted by colour
+    const int32_t* lo_ptr;        // device [N+1]: lower blocks of each row, sorted by colour
+    const int32_t* lo_idx;
+    const int32_t* up_ptr;        // device [N+1]: upper blocks of each row
+    const int32_t* up_idx;
+    double* lu;                   // device [nnzb][9]: L (unit diagonal implied) and U blocks
+    double* uinv;                 // device [N][9]: inverse of the U diagonal blocks
+    double* y;                    // device [N][3]: forward-solve scratch
+};
+cudaError_t launch_ilu_factor(const KrylovWork& w, const IluPlan& ilu, cudaStream_t s);
+cudaError_t launch_bicgstab_iteration_ilu(const KrylovWork& w, const IluPlan& ilu, cudaStream_t s);
 cudaError_t launch_block_jacobi_setup(const KrylovWork& w, cudaStream_t s);
 cudaError_t launch_krylov_init(const KrylovWork& w, double rtol, int max_iter, cudaStream_t s);
 cudaError_t launch_bicgstab_iteration(const KrylovWork& w, cudaStream_t s);

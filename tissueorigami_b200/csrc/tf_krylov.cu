@@ -661,7 +661,166 @@ __global__ void k_newton_update_batched(KrylovWork w, BatchPlan plan, double* uk
     plan.barriers[t].count = 0u;
 }
 
+// ---- multicolour block ILU(0) ---------------------------------------------------------------
+
+__device__ __forceinline__ void mat3_mul(const double* a, const double* b, double* c) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) c[i * 3 + j] = a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+}
+
+__device__ __forceinline__ void mat3_inv(const double* m, double* o, int32_t* dflags) {
+    const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
+    if (det == 0.0 || !isfinite(det)) {
+        atomicOr(dflags, DF_SINGULAR_DIAG);
+        for (int k = 0; k < 9; ++k) o[k] = (k % 4 == 0) ? 1.0 : 0.0;
+        return;
+    }
+    const double id = 1.0 / det;
+    o[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+    o[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    o[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    o[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    o[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    o[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    o[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    o[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    o[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+__device__ int find_col(const int32_t* colidx, int k0, int k1, int col) {
+    int lo = k0, hi = k1 - 1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int c = colidx[mid];
+        if (c == col) return mid;
+        if (c < col)
+            lo = mid + 1;
+        else
+            hi = mid - 1;
+    }
+    return -1;
+}
+
+// Factorise the rows of one colour class: for each lower block (i,K) in colour order,
+// L_iK = A_iK U_KK^-1, then A_iJ -= L_iK U_KJ over row K's upper blocks that exist in row i
+// (the ILU(0) rule: no fill outside the pattern); finally invert the U diagonal block of row i.
+__global__ void k_ilu_factor_colour(KrylovWork w, IluPlan ilu, int c0, int c1) {
+    const int q = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= c1) return;
+    const int i = ilu.cnodes[q];
+    const int r0 = w.rowptr[i], r1 = w.rowptr[i + 1];
+    for (int t = ilu.lo_ptr[i]; t < ilu.lo_ptr[i + 1]; ++t) {
+        const int k = ilu.lo_idx[t];
+        const int K = w.colidx[k];
+        double L[9];
+        mat3_mul(ilu.lu + (size_t)k * 9, ilu.uinv + (size_t)K * 9, L);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) ilu.lu[(size_t)k * 9 + m] = L[m];
+        for (int u = ilu.up_ptr[K]; u < ilu.up_ptr[K + 1]; ++u) {
+            const int j = ilu.up_idx[u];
+            const int pos = find_col(w.colidx, r0, r1, w.colidx[j]);
+            if (pos < 0) continue;
+            double P[9];
+            mat3_mul(L, ilu.lu + (size_t)j * 9, P);
+#pragma unroll
+            for (int m = 0; m < 9; ++m) ilu.lu[(size_t)pos * 9 + m] -= P[m];
+        }
+    }
+    mat3_inv(ilu.lu + (size_t)w.diag[i] * 9, ilu.uinv + (size_t)i * 9, w.dflags);
+}
+
+// Forward solve of one colour class: y_i = r_i - sum_{lower k} L_ik y_K.
+__global__ void k_ilu_fwd_colour(KrylovWork w, IluPlan ilu, int c0, int c1, const double* rin) {
+    if (!running(w.sc)) return;
+    const int q = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= c1) return;
+    const int i = ilu.cnodes[q];
+    double y0 = rin[i * 3], y1 = rin[i * 3 + 1], y2 = rin[i * 3 + 2];
+    for (int t = ilu.lo_ptr[i]; t < ilu.lo_ptr[i + 1]; ++t) {
+        const int k = ilu.lo_idx[t];
+        const int K = w.colidx[k];
+        const double* Lb = ilu.lu + (size_t)k * 9;
+        const double a = ilu.y[K * 3], b = ilu.y[K * 3 + 1], c = ilu.y[K * 3 + 2];
+        y0 -= Lb[0] * a + Lb[1] * b + Lb[2] * c;
+        y1 -= Lb[3] * a + Lb[4] * b + Lb[5] * c;
+        y2 -= Lb[6] * a + Lb[7] * b + Lb[8] * c;
+    }
+    ilu.y[i * 3] = y0;
+    ilu.y[i * 3 + 1] = y1;
+    ilu.y[i * 3 + 2] = y2;
+}
+
+// Backward solve of one colour class: z_i = U_ii^-1 (y_i - sum_{upper j} U_ij z_J).
+__global__ void k_ilu_bwd_colour(KrylovWork w, IluPlan ilu, int c0, int c1, double* zout) {
+    if (!running(w.sc)) return;
+    const int q = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= c1) return;
+    const int i = ilu.cnodes[q];
+    double y0 = ilu.y[i * 3], y1 = ilu.y[i * 3 + 1], y2 = ilu.y[i * 3 + 2];
+    for (int u = ilu.up_ptr[i]; u < ilu.up_ptr[i + 1]; ++u) {
+        const int j = ilu.up_idx[u];
+        const int J = w.colidx[j];
+        const double* Ub = ilu.lu + (size_t)j * 9;
+        const double a = zout[J * 3], b = zout[J * 3 + 1], c = zout[J * 3 + 2];
+        y0 -= Ub[0] * a + Ub[1] * b + Ub[2] * c;
+        y1 -= Ub[3] * a + Ub[4] * b + Ub[5] * c;
+        y2 -= Ub[6] * a + Ub[7] * b + Ub[8] * c;
+    }
+    const double* D = ilu.uinv + (size_t)i * 9;
+    zout[i * 3] = D[0] * y0 + D[1] * y1 + D[2] * y2;
+    zout[i * 3 + 1] = D[3] * y0 + D[4] * y1 + D[5] * y2;
+    zout[i * 3 + 2] = D[6] * y0 + D[7] * y1 + D[8] * y2;
+}
+
+__global__ void k_bicg_p_only(KrylovWork w) {
+    if (!running(w.sc)) return;
+    const double beta = (w.sc->rho / w.sc->rho_prev) * (w.sc->alpha / w.sc->omega);
+    const double omega = w.sc->omega;
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < w.n_nodes * 3; d += gridDim.x * blockDim.x)
+        w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
+}
+
+__global__ void k_bicg_s_only(KrylovWork w) {
+    if (!running(w.sc)) return;
+    const double alpha = w.sc->alpha;
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < w.n_nodes * 3; d += gridDim.x * blockDim.x)
+        w.s[d] = w.r[d] - alpha * w.v[d];
+}
+
+void ilu_apply(const KrylovWork& w, const IluPlan& ilu, const double* rin, double* zout, cudaStream_t s) {
+    for (int c = 0; c < ilu.n_colours; ++c) {
+        const int c0 = ilu.colour_ptr[c], c1 = ilu.colour_ptr[c + 1];
+        if (c1 > c0) k_ilu_fwd_colour<<<(c1 - c0 + 127) / 128, 128, 0, s>>>(w, ilu, c0, c1, rin);
+    }
+    for (int c = ilu.n_colours - 1; c >= 0; --c) {
+        const int c0 = ilu.colour_ptr[c], c1 = ilu.colour_ptr[c + 1];
+        if (c1 > c0) k_ilu_bwd_colour<<<(c1 - c0 + 127) / 128, 128, 0, s>>>(w, ilu, c0, c1, zout);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_ilu_factor(const KrylovWork& w, const IluPlan& ilu, cudaStream_t s) {
+    for (int c = 0; c < ilu.n_colours; ++c) {
+        const int c0 = ilu.colour_ptr[c], c1 = ilu.colour_ptr[c + 1];
+        if (c1 > c0) k_ilu_factor_colour<<<(c1 - c0 + 127) / 128, 128, 0, s>>>(w, ilu, c0, c1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bicgstab_iteration_ilu(const KrylovWork& w, const IluPlan& ilu, cudaStream_t s) {
+    const int vg = vec_grid(w.n_nodes), sg = spmv_grid(w.n_nodes);
+    k_bicg_p_only<<<vg, kVecThreads, 0, s>>>(w);
+    ilu_apply(w, ilu, w.p, w.phat, s);
+    k_spmv<1><<<sg, kSpmvThreads, 0, s>>>(w, w.phat, w.v, 1);
+    k_bicg_s_only<<<vg, kVecThreads, 0, s>>>(w);
+    ilu_apply(w, ilu, w.s, w.shat, s);
+    k_spmv<2><<<sg, kSpmvThreads, 0, s>>>(w, w.shat, w.t, 1);
+    k_bicg_xr<<<vg, kVecThreads, 0, s>>>(w);
+    return cudaGetLastError();
+}
 
 int persistent_max_grid(int device) {
     int sms = 0, occ = 0;

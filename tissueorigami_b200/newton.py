@@ -171,6 +171,15 @@ class NewtonRaphsonSolver:
                         "tf_adjoint_backward", self._h)
         return dr, dx0, rc, st.as_dict()
 
+    def solve_direct(self, vals, g):
+        """cuSOLVER sparse Cholesky / QR solve of J du = g (timed beside the Krylov solve)."""
+        du = np.zeros(3 * self.n_nodes)
+        ms = ctypes.c_double()
+        m = ctypes.c_int32()
+        rc = capi.check(self._L.tf_solve_direct(self._h, capi.dptr(_f64(vals).reshape(-1)), capi.dptr(_f64(g)), capi.dptr(du),
+                                                ctypes.byref(ms), ctypes.byref(m)), "tf_solve_direct", self._h)
+        return du, rc, ms.value, m.value
+
     def schedule(self):
         nc, sc, t = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         self._L.tf_get_schedule(self._h, ctypes.byref(nc), ctypes.byref(sc), ctypes.byref(t))
