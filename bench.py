@@ -196,9 +196,10 @@ def run_b200(args) -> None:
     L = capi.load()
     t = make_tissue(args.workload)
     precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0}[args.precond]
-    s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond)
+    s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent)
     sched = s.autotune(t.x, t.dt)
     sched["precond"] = args.precond
+    sched["solve"] = {0: "graph-replayed iteration kernels", 1: "persistent cooperative kernel"}[args.persistent]
     n3 = 3 * t.n_nodes
     x_dev = torch.from_numpy(np.ascontiguousarray(t.x.reshape(-1))).to(f"cuda:{local}")
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
@@ -297,7 +298,7 @@ def run_b200(args) -> None:
 
     r_el = roof("element_assemble", bytes_asm, ms_el)
     r_sp = roof("bsr3_spmv", bytes_spmv, ms_spmv)
-    # the persistent solve: per BiCGStab iteration two SpMVs (each also reads one dot vector)
+    # persistent solve: per BiCGStab iteration two SpMVs (each also reads one dot vector)
     # and three node-wise phases (p/phat: r,p,v,D -> p,phat; s/shat: r,v,D -> s,shat;
     # x/r: x,phat,shat,s,t,rhat -> x,r); plus one setup pass (diagonal inverses, r, rhat, p, v)
     per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 72 + 4 * 24 + 72 + 8 * 24)
@@ -513,6 +514,8 @@ def main():
     ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")
     ap.add_argument("--precond", choices=["block_jacobi", "ilu0"], default="block_jacobi",
                     help="Krylov preconditioner of the single-tissue workloads")
+    ap.add_argument("--persistent", type=int, choices=[0, 1], default=1,
+                    help="solve path of the single-tissue workloads (tf_params.persistent)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()

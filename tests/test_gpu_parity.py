@@ -80,7 +80,10 @@ def test_slave_master_assembly_matches_dense_oracle():
     assert _rel(g, g_ref) < 1e-12
 
 
-def test_solve_matches_direct():
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_solve_matches_direct(persistent):
+    """Both solve paths (graph-replayed iteration kernels, persistent cooperative kernel) against
+    SuperLU: 1e-8 relative in ||du||, fixed DoFs exactly zero."""
     t = mesh.small_disc(7, 1500, 1200.0)
     fg, inv, _, _ = O.grow(t, t.x, t.fg)
     vs = O.viscosity_surfaces(t, t.x)
@@ -88,7 +91,7 @@ def test_solve_matches_direct():
     vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
     J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
     du_ref = sla.spsolve(J, g)
-    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13) as s:
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, persistent=persistent) as s:
         rp, ci = s.pattern()
         np.testing.assert_array_equal(rp, rowptr)
         np.testing.assert_array_equal(ci, colidx)
@@ -132,10 +135,11 @@ def test_ten_time_steps_small_rectangle():
     assert np.abs(x - x_ref).max() <= 1e-9 * t.size
 
 
-def test_time_steps_disc_matches_sparse_oracle():
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_time_steps_disc_matches_sparse_oracle(persistent):
     t = mesh.small_disc(11, 3000, 2000.0, n_steps=3)
     x_ref, fg_ref, it_ref, _ = O.simulate_sparse(t, n_steps=3)
-    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14, persistent=persistent) as s:
         x = t.x.copy()
         for _ in range(3):
             x, rc, st = s.runOneStep(x, t.dt)

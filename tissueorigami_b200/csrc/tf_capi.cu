@@ -65,6 +65,7 @@ struct tf_ctx {
     DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
     DevBuf fg, rates, angles, exposed, peripodial, rotated, xio, barrier;
     int persistent_grid_max = 0;  // 0: cooperative launch unavailable
+    int persist_threads = 256;    // CTA width of the persistent solve
 
     // batch partition: tissue t owns nodes [tissue_node0[t], tissue_node0[t+1]) and elements
     // [tissue_elem0[t], tissue_elem0[t+1]); a single tissue is T = 1.
@@ -657,7 +658,8 @@ int krylov_solve(tf_ctx* ctx) {
     if (use_persistent(ctx)) {
         const BatchPlan plan = make_plan(ctx);
         TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
-        TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters, ctx->stream));
+        TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
+                                      ctx->persist_threads, ctx->stream));
         TF_CK(cudaEventRecord(ctx->ev_solve[1], ctx->stream));
         ctx->launches += 1;
         TF_CK(cudaMemcpyAsync(ctx->h_tsc, ctx->tscalars.p, sizeof(KrylovScalars) * ctx->T, cudaMemcpyDeviceToHost,
@@ -1019,7 +1021,13 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
     {
         int coop = 0;
         TF_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
-        ctx->persistent_grid_max = coop ? persistent_max_grid(ctx->device) : 0;
+        // a large single tissue: one 768-thread CTA per SM (fewest grid-barrier participants);
+        // small tissues and batches: three 256-thread CTAs per SM (more, smaller row ranges, and
+        // in a batch many tissues each with their own CTAs)
+        int sms = 0;
+        TF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        ctx->persist_threads = (T == 1 && (int64_t)ctx->N >= (int64_t)sms * 256) ? 768 : 256;
+        ctx->persistent_grid_max = coop ? persistent_max_grid(ctx->device, ctx->persist_threads) : 0;
     }
     TF_CK(cudaMemset(ctx->sc.p, 0, sizeof(KrylovScalars)));
     TF_CK(cudaMemset(ctx->fixmask.p, 0, N));

@@ -191,9 +191,10 @@ cudaError_t launch_newton_update(const KrylovWork& w, double* uk, const int32_t*
 int spmv_grid(int n_nodes);
 // Persistent cooperative BiCGStab over a batch of tissues (one tissue: a plan with T = 1).
 // w.partials must hold 4 * plan.n_cta doubles.
-int persistent_max_grid(int device);
+// threads: CTA width, 256 (three CTAs per SM, for batches of many tissues) or 768 (one per SM).
+int persistent_max_grid(int device, int threads);
 cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
-                                    cudaStream_t s);
+                                    int threads, cudaStream_t s);
 // uk += du on active tissues, du[slave] = du[master], per-tissue ||du||^2 into plan.du2
 cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
                                          const int32_t* slaves, const int32_t* masters, int32_t n_pairs,

@@ -24,7 +24,7 @@ namespace {
 constexpr int kVecThreads = 256;
 constexpr int kSpmvThreads = 256;
 constexpr int kGroup = 8;  // lanes per block row in the SpMV
-constexpr int kPersistThreads = 256;
+constexpr int kPersistThreadsMax = 768;  // persistent solve: 3 x 256 or 1 x 768 threads per SM
 
 __device__ __forceinline__ bool running(const KrylovScalars* sc) {
     return *reinterpret_cast<const volatile int32_t*>(&sc->status) == KS_RUNNING;
@@ -484,7 +484,7 @@ __device__ bool restart(const KrylovWork& w, int r0, int r1, double& rho, double
     return rho > 0.0 && isfinite(rho);
 }
 
-__global__ void __launch_bounds__(kPersistThreads, 3) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
+__global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
                                                                       int max_iter) {
     __shared__ double smem[32 * 2];
     __shared__ double sb[2];
@@ -822,22 +822,22 @@ cudaError_t launch_bicgstab_iteration_ilu(const KrylovWork& w, const IluPlan& il
     return cudaGetLastError();
 }
 
-int persistent_max_grid(int device) {
+int persistent_max_grid(int device, int threads) {
     int sms = 0, occ = 0;
+    if (threads != 256 && threads != 768) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_batched, kPersistThreads, 0) != cudaSuccess)
-        return 0;
-    const int per_sm = occ < 3 ? occ : 3;  // the kernel is built for three 256-thread CTAs per SM
-    return sms * per_sm;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_batched, threads, 0) != cudaSuccess) return 0;
+    const int want = kPersistThreadsMax / threads;  // the kernel is built for 768 threads per SM
+    return sms * (occ < want ? occ : want);
 }
 
 cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
-                                    cudaStream_t s) {
+                                    int threads, cudaStream_t s) {
     KrylovWork wc = w;
     BatchPlan pc = plan;
     void* args[] = {&wc, &pc, &rtol, &max_iter};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_batched), dim3(plan.n_cta),
-                                       dim3(kPersistThreads), args, 0, s);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_batched), dim3(plan.n_cta), dim3(threads),
+                                       args, 0, s);
 }
 
 cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
