@@ -358,21 +358,39 @@ def run_b200(args) -> None:
 
 
 def run_batch(args) -> None:
-    """Batched uneven tissues: 256 discs / rectangles (500-20k prisms, log-uniform) in one
-    context, against sequential single-tissue GPU runs of the same tissues."""
+    """Batched uneven tissues: 256 discs / rectangles (500-20k prisms, log-uniform). One process
+    per GPU: each rank runs its share of whole tissues (greedy bin packing on prisms x sqrt(nodes))
+    as one batched context; no collective on the data path, time = max over ranks. At N = 1 the
+    line also carries sequential single-tissue GPU runs of the same tissues."""
     import ctypes
+    import datetime
 
     import torch
 
     from tissueorigami_b200 import capi, mesh
     from tissueorigami_b200.newton import BatchSolver, NewtonRaphsonSolver
+    from tissueorigami_b200.sharding import ShardedBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     L = capi.load()
     ts = mesh.batch_tissues(n_tissues=args.n_tissues)
-    E_t = np.array([t.n_elems for t in ts], dtype=np.float64)
-    b = BatchSolver(ts)
-    x = torch.from_numpy(b.join([t.x for t in ts]).reshape(-1).copy()).cuda()
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    E_all = float(sum(t.n_elems for t in ts))
+    sb = ShardedBatch(ts, rank, world, lambda tl: BatchSolver(tl, device=local))
+    b = sb.solver
+    dev = f"cuda:{local}"
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    if b is not None:
+        E_t = np.array([ts[i].n_elems for i in sb.mine], dtype=np.float64)
+        x = torch.from_numpy(sb.initial_positions().reshape(-1).copy()).to(dev)
     torch.cuda.synchronize()
 
     def step():
@@ -382,47 +400,74 @@ def run_batch(args) -> None:
         capi.check(rc, "tf_time_step_device", b._h)
         return rc, st
 
-    for _ in range(args.warmup):
-        step()
+    if b is not None:
+        for _ in range(args.warmup):
+            step()
     clocks = ClockSampler(None)
     clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
     ms, units, launches, worst = 0.0, 0.0, 0, 0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
+        if b is None:
+            continue
         rc, st = step()
         ts_stats = b.tissue_stats()
         units += float((E_t * ts_stats["newton_iters"]).sum())
         ms += st.ms_total
         launches += st.gpu_launches
         worst = max(worst, rc)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     clk = clocks.stop()
-    b.close()
-    # sequential baseline: the same tissues one after another, one context each, same steps
-    seq_ms, seq_units = 0.0, 0.0
-    for t in ts:
-        with NewtonRaphsonSolver.from_tissue(t) as s:
-            xx = t.x.copy()
-            for _ in range(args.warmup):
-                xx, _, _ = s.runOneStep(xx, t.dt)
-            for _ in range(args.steps):
-                xx, _, st = s.runOneStep(xx, t.dt)
-                seq_ms += st["ms_total"]
-                seq_units += t.n_elems * st["newton_iters"]
-    value = units / (ms / 1000.0)
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded meshes and growth fields)",
-        "config": {"workload": f"batch: {len(ts)} tissues, {int(E_t.sum())} prisms, prism counts log-uniform 500-20000",
-                   "l2": "flushed (256 MB write) between timed steps"},
-        "tissue_steps_per_s": len(ts) * args.steps / (ms / 1000.0),
-        "sequential": {"value": seq_units / (seq_ms / 1000.0), "ms_per_step": seq_ms / args.steps,
-                       "tissue_steps_per_s": len(ts) * args.steps / (seq_ms / 1000.0)},
-        "batch_speedup_vs_sequential": (seq_ms / args.steps) / (ms / args.steps),
-        "gpu_launches": int(launches), "clocks": clk, "status_worst": worst,
-    }
-    print(json.dumps(line), flush=True)
+    sb.close()
+    t_dev = ms / 1000.0
+    if dist:
+        tot = torch.tensor([units, float(launches), float(worst)], dtype=torch.float64, device=dev)
+        tm = torch.tensor([t_dev], dtype=torch.float64, device=dev)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        units, launches, worst = tot.tolist()
+        t_dev = tm.item()
+    seq = None
+    if world == 1:
+        # sequential baseline: the same tissues one after another, one context each, same steps
+        seq_ms, seq_units = 0.0, 0.0
+        for t in ts:
+            with NewtonRaphsonSolver.from_tissue(t) as s:
+                xx = t.x.copy()
+                for _ in range(args.warmup):
+                    xx, _, _ = s.runOneStep(xx, t.dt)
+                for _ in range(args.steps):
+                    xx, _, st = s.runOneStep(xx, t.dt)
+                    seq_ms += st["ms_total"]
+                    seq_units += t.n_elems * st["newton_iters"]
+        seq = {"value": seq_units / (seq_ms / 1000.0), "ms_per_step": seq_ms / args.steps,
+               "tissue_steps_per_s": len(ts) * args.steps / (seq_ms / 1000.0)}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": units / t_dev, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded meshes and growth fields)",
+            "config": {"workload": f"batch: {len(ts)} tissues, {int(E_all)} prisms, prism counts log-uniform 500-20000",
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"{world} rank(s), whole tissues per rank (greedy bin packing), "
+                                      "no collective on the data path",
+                       "tissues_per_rank": [len(s_) for s_ in sb.shards]},
+            "tissue_steps_per_s": len(ts) * args.steps / t_dev,
+            "gpu_launches": int(launches), "clocks": clk, "status_worst": int(worst),
+        }
+        if seq is not None:
+            line["sequential"] = seq
+            line["batch_speedup_vs_sequential"] = seq["ms_per_step"] / (1000.0 * t_dev / args.steps)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_adjoint(args) -> None:
