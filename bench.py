@@ -195,7 +195,8 @@ def run_b200(args) -> None:
 
     L = capi.load()
     t = make_tissue(args.workload)
-    precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0}[args.precond]
+    precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0,
+               "two_level": capi.TF_PRECOND_TWO_LEVEL}[args.precond]
     s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent)
     sched = s.autotune(t.x, t.dt)
     sched["precond"] = args.precond
@@ -563,7 +564,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")
-    ap.add_argument("--precond", choices=["block_jacobi", "ilu0"], default="block_jacobi",
+    ap.add_argument("--precond", choices=["block_jacobi", "ilu0", "two_level"], default="block_jacobi",
                     help="Krylov preconditioner of the single-tissue workloads")
     ap.add_argument("--persistent", type=int, choices=[0, 1], default=1,
                     help="solve path of the single-tissue workloads (tf_params.persistent)")

@@ -29,6 +29,7 @@ TF_NOALLOC_MAX_NODES = 16384
 
 TF_PRECOND_BLOCK_JACOBI = 0
 TF_PRECOND_ILU0 = 1
+TF_PRECOND_TWO_LEVEL = 2
 TF_SCATTER_AUTO = 0
 TF_SCATTER_ATOMIC = 1
 TF_SCATTER_COLOURED = 2

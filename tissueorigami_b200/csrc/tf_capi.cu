@@ -8,8 +8,10 @@
 // Newton iteration. The linear solve runs as graph-replayed chunks of BiCGStab iterations
 // whose scalars never leave the device.
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -78,6 +80,16 @@ struct tf_ctx {
     KrylovScalars* h_tsc = nullptr;  // pinned [T]
     std::vector<int32_t> t_iters, t_status, t_krylov;
     std::vector<int32_t> last_krylov;  // first-round BiCGStab iterations of each tissue, last step
+
+    // two-level preconditioner (precond == TF_PRECOND_TWO_LEVEL, single tissue, persistent solve)
+    std::vector<uint8_t> h_fixmask;
+    bool coarse_dirty = true;
+    int coarse_m = 0, n_coarse = 0, n_agg = 0, coarse_lwork = 0, n_coarse_empty = 0;
+    bool coarse_ok = false;  // the last coarse factorisation succeeded
+    DevBuf pmode_d, coarse_a, coarse_inv, coarse_r, coarse_ipiv, coarse_info, coarse_work;
+    DevBuf ca_agg_slot_ptr, ca_slot_agg, ca_slot_ptr, ca_blk, ca_blk_row, ca_empty;
+    cusolverDnHandle_t dn = nullptr;
+    int32_t* h_coarse_info = nullptr;  // pinned
 
     // multicolour block ILU(0) (precond == TF_PRECOND_ILU0)
     std::vector<int32_t> ilu_colour_ptr;
@@ -366,6 +378,7 @@ int upload_structure(tf_ctx* ctx) {
         const int irc = build_ilu(ctx);
         if (irc != TF_OK) return irc;
     }
+    ctx->coarse_dirty = true;
     const size_t np2 = std::max((size_t)std::max(spmv_grid(N), vec_grid(N)) * 2,
                                 (size_t)ctx->persistent_grid_max * 4) + 64;
     TF_CK(dalloc(ctx->partials, sizeof(double) * np2));
@@ -573,6 +586,11 @@ int build_plan_all(tf_ctx* ctx) {
 
 BatchPlan make_plan(tf_ctx* c) {
     BatchPlan p;
+    p.agg_per_cta = (c->coarse_m > 0 && c->coarse_ok) ? c->coarse_m : 0;
+    p.n_coarse = c->n_coarse;
+    p.pmode = dptr<double>(c->pmode_d);
+    p.coarse_inv = dptr<double>(c->coarse_inv);
+    p.coarse_r = dptr<double>(c->coarse_r);
     p.n_tissues = c->T;
     p.n_cta = (int32_t)c->plan_cta_tissue.size();
     p.cta_tissue = dptr<int32_t>(c->plan_cta_tissue_d);
@@ -646,9 +664,192 @@ int krylov_status_to_tf(int ks) {
     }
 }
 
+// ---- two-level preconditioner ----------------------------------------------------------
+//
+// Coarse space of one tissue for the persistent solve: the plan's CTA row ranges, each split
+// into m contiguous aggregates (the kernel's formula), so restriction and prolongation stay
+// inside a CTA. Meshes numbered point-major along a space-filling curve make contiguous node
+// ranges compact patches. Each aggregate gets six modes - three translations and three
+// rotations about its centroid in reference coordinates - with fixed and slave DoFs zeroed
+// (the solve never moves them), orthonormalised by modified Gram-Schmidt; a mode that
+// vanishes there (below 1e-10 of its initial norm) is dropped and its coarse unknown gets a
+// unit diagonal. The coarse operator P^T J P is assembled on the device every solve and
+// inverted explicitly (LU, cuSOLVER), so an application is a dense row-block product.
+int build_coarse(tf_ctx* ctx) {
+    ctx->coarse_dirty = false;
+    ctx->coarse_m = 0;
+    if (ctx->params.precond != TF_PRECOND_TWO_LEVEL || ctx->T != 1 || ctx->plan_ncta.empty()) return TF_OK;
+    const int N = ctx->N, nct = ctx->plan_ncta[0];
+    if (nct <= 0) return TF_OK;
+    int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
+    while (m > 1 && N / (nct * m) < 8) --m;
+    const int nw = ctx->persist_threads / 32;
+    while (m > 1 && nw / m < 1) --m;
+    const int n_agg = nct * m, nc = 6 * n_agg;
+    std::vector<double> X((size_t)N * 3, 0.0);
+    for (int e = 0; e < ctx->E; ++e)
+        for (int a = 0; a < 6; ++a)
+            for (int d = 0; d < 3; ++d) X[(size_t)ctx->conn[(size_t)e * 6 + a] * 3 + d] = ctx->xref[(size_t)e * 18 + a * 3 + d];
+    std::vector<int32_t> agg0(n_agg + 1);
+    for (int lc = 0; lc < nct; ++lc) {
+        const int r0 = (int)((long long)N * lc / nct), r1 = (int)((long long)N * (lc + 1) / nct), L = r1 - r0;
+        for (int k = 0; k < m; ++k) agg0[lc * m + k] = r0 + (int)((long long)L * k / m);
+    }
+    agg0[n_agg] = N;
+    std::vector<double> pm((size_t)N * 18, 0.0);
+    std::vector<int32_t> empty;
+    for (int a = 0; a < n_agg; ++a) {
+        const int s0 = agg0[a], n = agg0[a + 1] - s0;
+        if (n <= 0) {
+            for (int q = 0; q < 6; ++q) empty.push_back(6 * a + q);
+            continue;
+        }
+        double c[3] = {0, 0, 0};
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) c[d] += X[(size_t)(s0 + i) * 3 + d] / n;
+        const size_t len = (size_t)3 * n;
+        std::vector<double> B(6 * len, 0.0);
+        for (int i = 0; i < n; ++i) {
+            const double dx = X[(size_t)(s0 + i) * 3] - c[0], dy = X[(size_t)(s0 + i) * 3 + 1] - c[1],
+                         dz = X[(size_t)(s0 + i) * 3 + 2] - c[2];
+            for (int q = 0; q < 3; ++q) B[q * len + 3 * i + q] = 1.0;
+            B[3 * len + 3 * i + 1] = -dz, B[3 * len + 3 * i + 2] = dy;   // rotation about x
+            B[4 * len + 3 * i + 0] = dz, B[4 * len + 3 * i + 2] = -dx;   // about y
+            B[5 * len + 3 * i + 0] = -dy, B[5 * len + 3 * i + 1] = dx;   // about z
+            for (int d = 0; d < 3; ++d) {
+                const size_t dof = (size_t)(s0 + i) * 3 + d;
+                const bool fixed = (ctx->h_fixmask.size() == (size_t)N) && (ctx->h_fixmask[s0 + i] >> d & 1);
+                if (fixed || ctx->dofmap[dof] != (int32_t)dof)
+                    for (int q = 0; q < 6; ++q) B[q * len + 3 * i + d] = 0.0;
+            }
+        }
+        std::vector<char> kept(6, 0);
+        for (int q = 0; q < 6; ++q) {
+            double* bq = &B[q * len];
+            double n0 = 0.0;
+            for (size_t r = 0; r < len; ++r) n0 += bq[r] * bq[r];
+            n0 = std::sqrt(n0);
+            for (int pass = 0; pass < 2; ++pass)
+                for (int p = 0; p < q; ++p) {
+                    if (!kept[p]) continue;
+                    const double* bp = &B[p * len];
+                    double dot = 0.0;
+                    for (size_t r = 0; r < len; ++r) dot += bp[r] * bq[r];
+                    for (size_t r = 0; r < len; ++r) bq[r] -= dot * bp[r];
+                }
+            double nq = 0.0;
+            for (size_t r = 0; r < len; ++r) nq += bq[r] * bq[r];
+            nq = std::sqrt(nq);
+            if (n0 == 0.0 || nq <= 1e-10 * n0) {
+                for (size_t r = 0; r < len; ++r) bq[r] = 0.0;
+                empty.push_back(6 * a + q);
+                continue;
+            }
+            kept[q] = 1;
+            for (size_t r = 0; r < len; ++r) bq[r] /= nq;
+        }
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d)
+                for (int q = 0; q < 6; ++q) pm[(size_t)(s0 + i) * 18 + d * 6 + q] = B[q * len + 3 * i + d];
+    }
+    // Jacobian blocks grouped by (row aggregate, column aggregate)
+    std::vector<int32_t> aggof(N);
+    for (int a = 0; a < n_agg; ++a)
+        for (int i = agg0[a]; i < agg0[a + 1]; ++i) aggof[i] = a;
+    std::vector<int32_t> agg_slot_ptr(n_agg + 1, 0), slot_agg, slot_ptr(1, 0), blk, blk_row;
+    blk.reserve(ctx->nnzb);
+    blk_row.reserve(ctx->nnzb);
+    std::vector<std::array<int32_t, 3>> items;
+    for (int a = 0; a < n_agg; ++a) {
+        items.clear();
+        for (int i = agg0[a]; i < agg0[a + 1]; ++i)
+            for (int k = ctx->rowptr[i]; k < ctx->rowptr[i + 1]; ++k) items.push_back({aggof[ctx->colidx[k]], k, i});
+        std::sort(items.begin(), items.end());
+        for (size_t q = 0; q < items.size(); ++q) {
+            if (q == 0 || items[q][0] != items[q - 1][0]) {
+                if (q > 0) slot_ptr.push_back((int32_t)blk.size());
+                slot_agg.push_back(items[q][0]);
+            }
+            blk.push_back(items[q][1]);
+            blk_row.push_back(items[q][2]);
+        }
+        if (!items.empty()) slot_ptr.push_back((int32_t)blk.size());
+        agg_slot_ptr[a + 1] = (int32_t)slot_agg.size();
+    }
+    auto up = [&](DevBuf& b, const void* h, size_t bytes) -> cudaError_t {
+        cudaError_t e = dalloc(b, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess && bytes) e = cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice);
+        return e;
+    };
+    TF_CK(up(ctx->pmode_d, pm.data(), sizeof(double) * pm.size()));
+    TF_CK(up(ctx->ca_agg_slot_ptr, agg_slot_ptr.data(), sizeof(int32_t) * agg_slot_ptr.size()));
+    TF_CK(up(ctx->ca_slot_agg, slot_agg.data(), sizeof(int32_t) * slot_agg.size()));
+    TF_CK(up(ctx->ca_slot_ptr, slot_ptr.data(), sizeof(int32_t) * slot_ptr.size()));
+    TF_CK(up(ctx->ca_blk, blk.data(), sizeof(int32_t) * blk.size()));
+    TF_CK(up(ctx->ca_blk_row, blk_row.data(), sizeof(int32_t) * blk_row.size()));
+    TF_CK(up(ctx->ca_empty, empty.data(), sizeof(int32_t) * empty.size()));
+    TF_CK(dalloc(ctx->coarse_a, sizeof(double) * (size_t)nc * nc));
+    TF_CK(dalloc(ctx->coarse_inv, sizeof(double) * (size_t)nc * nc));
+    TF_CK(dalloc(ctx->coarse_r, sizeof(double) * (size_t)nc));
+    TF_CK(dalloc(ctx->coarse_ipiv, sizeof(int32_t) * (size_t)nc));
+    TF_CK(dalloc(ctx->coarse_info, sizeof(int32_t)));
+    if (!ctx->dn) {
+        if (cusolverDnCreate(&ctx->dn) != CUSOLVER_STATUS_SUCCESS) return set_error(ctx, TF_ERR_CUDA, "cusolverDnCreate");
+        if (cusolverDnSetStream(ctx->dn, ctx->stream) != CUSOLVER_STATUS_SUCCESS)
+            return set_error(ctx, TF_ERR_CUDA, "cusolverDnSetStream");
+    }
+    int lwork = 0;
+    if (cusolverDnDgetrf_bufferSize(ctx->dn, nc, nc, dptr<double>(ctx->coarse_a), nc, &lwork) != CUSOLVER_STATUS_SUCCESS)
+        return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrf_bufferSize");
+    TF_CK(dalloc(ctx->coarse_work, sizeof(double) * (size_t)std::max(lwork, 1)));
+    if (!ctx->h_coarse_info) TF_CK(cudaMallocHost(&ctx->h_coarse_info, sizeof(int32_t)));
+    ctx->coarse_lwork = lwork;
+    ctx->n_agg = n_agg;
+    ctx->n_coarse = nc;
+    ctx->n_coarse_empty = (int)empty.size();
+    ctx->coarse_m = m;
+    return TF_OK;
+}
+
+// Assemble P^T J P for the current J and invert it; on a singular coarse operator the solve
+// runs with block-Jacobi alone (coarse_ok = false).
+int coarse_setup(tf_ctx* ctx) {
+    ctx->coarse_ok = false;
+    if (ctx->coarse_m == 0) return TF_OK;
+    const int nc = ctx->n_coarse;
+    CoarseAssembly ca;
+    ca.n_agg = ctx->n_agg;
+    ca.n_coarse = nc;
+    ca.agg_slot_ptr = dptr<int32_t>(ctx->ca_agg_slot_ptr);
+    ca.slot_agg = dptr<int32_t>(ctx->ca_slot_agg);
+    ca.slot_ptr = dptr<int32_t>(ctx->ca_slot_ptr);
+    ca.blk = dptr<int32_t>(ctx->ca_blk);
+    ca.blk_row = dptr<int32_t>(ctx->ca_blk_row);
+    ca.empty = dptr<int32_t>(ctx->ca_empty);
+    ca.n_empty = ctx->n_coarse_empty;
+    double* A = dptr<double>(ctx->coarse_a);
+    double* inv = dptr<double>(ctx->coarse_inv);
+    int32_t* ipiv = dptr<int32_t>(ctx->coarse_ipiv);
+    int32_t* info = dptr<int32_t>(ctx->coarse_info);
+    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), A, ctx->stream));
+    ctx->launches += 2;
+    if (cusolverDnDgetrf(ctx->dn, nc, nc, A, nc, dptr<double>(ctx->coarse_work), ipiv, info) != CUSOLVER_STATUS_SUCCESS)
+        return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrf");
+    TF_CK(cudaMemcpyAsync(ctx->h_coarse_info, info, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->h_coarse_info != 0) return TF_OK;  // singular: block-Jacobi only
+    // X with A^T X = I is A^-1 in row-major order (the layout the solve reads)
+    TF_CK(launch_set_identity(inv, nc, ctx->stream));
+    if (cusolverDnDgetrs(ctx->dn, CUBLAS_OP_T, nc, nc, A, nc, ipiv, inv, nc, info) != CUSOLVER_STATUS_SUCCESS)
+        return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrs");
+    ctx->launches += 1;
+    ctx->coarse_ok = true;
+    return TF_OK;
+}
+
 bool use_persistent(tf_ctx* ctx) {
-    return ctx->params.precond == TF_PRECOND_BLOCK_JACOBI && ctx->persistent_grid_max > 0 &&
-           (ctx->params.persistent || ctx->T > 1);
+    return (ctx->params.precond == TF_PRECOND_BLOCK_JACOBI || ctx->params.precond == TF_PRECOND_TWO_LEVEL) &&
+           ctx->persistent_grid_max > 0 && (ctx->params.persistent || ctx->T > 1);
 }
 
 // Solve J du = g (buffers in the context) for every active tissue. Leaves the scalars in
@@ -656,6 +857,14 @@ bool use_persistent(tf_ctx* ctx) {
 int krylov_solve(tf_ctx* ctx) {
     KrylovWork w = make_work(ctx);
     if (use_persistent(ctx)) {
+        if (ctx->params.precond == TF_PRECOND_TWO_LEVEL) {
+            if (ctx->coarse_dirty) {
+                const int crc = build_coarse(ctx);
+                if (crc != TF_OK) return crc;
+            }
+            const int crc = coarse_setup(ctx);
+            if (crc != TF_OK) return crc;
+        }
         const BatchPlan plan = make_plan(ctx);
         TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
         TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
@@ -966,7 +1175,8 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         ctx->params = *params;
     else
         tf_default_params(&ctx->params);
-    if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI && !(ctx->params.precond == TF_PRECOND_ILU0 && T == 1))
+    if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI && !(ctx->params.precond == TF_PRECOND_ILU0 && T == 1) &&
+        !(ctx->params.precond == TF_PRECOND_TWO_LEVEL && T == 1 && ctx->params.persistent))
         return TF_ERR_UNSUPPORTED;
     if (ctx->params.krylov_max_iters <= 0 || ctx->params.max_newton_iters < 0) return TF_ERR_ARGUMENT;
     ctx->device = ctx->params.device;
@@ -1050,6 +1260,8 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
     rc = build_plan_all(ctx);
     if (rc != TF_OK) return rc;
     if (ctx->T > 1 && ctx->persistent_grid_max == 0) return TF_ERR_UNSUPPORTED;
+    if (ctx->params.precond == TF_PRECOND_TWO_LEVEL && ctx->persistent_grid_max == 0) return TF_ERR_UNSUPPORTED;
+    ctx->h_fixmask.assign(N, 0);
     if (ctx->params.scatter == TF_SCATTER_COLOURED && ctx->n_colours == 0) return TF_ERR_UNSUPPORTED;
     ctx->scatter = ctx->params.scatter == TF_SCATTER_AUTO ? TF_SCATTER_ATOMIC : ctx->params.scatter;
     ctx->teams = ctx->params.elems_per_block > 0 ? ctx->params.elems_per_block : 16;
@@ -1124,6 +1336,12 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->ilu_lo_idx, &ctx->ilu_up_ptr, &ctx->ilu_up_idx, &ctx->ilu_lu, &ctx->ilu_uinv, &ctx->ilu_y};
     for (DevBuf* b : adj) dfree(*b);
     if (ctx->ilu_graph) cudaGraphExecDestroy(ctx->ilu_graph);
+    DevBuf* coarse[] = {&ctx->pmode_d, &ctx->coarse_a, &ctx->coarse_inv, &ctx->coarse_r, &ctx->coarse_ipiv,
+                        &ctx->coarse_info, &ctx->coarse_work, &ctx->ca_agg_slot_ptr, &ctx->ca_slot_agg,
+                        &ctx->ca_slot_ptr, &ctx->ca_blk, &ctx->ca_blk_row, &ctx->ca_empty};
+    for (DevBuf* b : coarse) dfree(*b);
+    if (ctx->dn) cusolverDnDestroy(ctx->dn);
+    if (ctx->h_coarse_info) cudaFreeHost(ctx->h_coarse_info);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);
     if (ctx->h_du2) cudaFreeHost(ctx->h_du2);
     if (ctx->h_tsc) cudaFreeHost(ctx->h_tsc);
@@ -1173,6 +1391,8 @@ int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
         for (int i = 0; i < N; ++i)
             fm[i] = (uint8_t)((fixed[i * 3] ? 1 : 0) | (fixed[i * 3 + 1] ? 2 : 0) | (fixed[i * 3 + 2] ? 4 : 0));
     TF_CK(cudaMemcpy(ctx->fixmask.p, fm.data(), N, cudaMemcpyHostToDevice));
+    ctx->h_fixmask = fm;
+    ctx->coarse_dirty = true;
     if (ext_visc) TF_CK(cudaMemcpy(ctx->ext_visc.p, ext_visc, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
     std::vector<int32_t> dm((size_t)N * 3);
     for (size_t i = 0; i < dm.size(); ++i) dm[i] = (int32_t)i;

@@ -114,7 +114,17 @@ struct BatchPlan {
     GridBarrier* barriers;       // [T]
     KrylovScalars* scalars;      // [T]
     double* du2;                 // [T] ||du||^2 of the last Newton update
+    // two-level preconditioner of a single tissue (agg_per_cta = 0: block-Jacobi only). Each
+    // CTA's rows [r0, r1) split into agg_per_cta aggregates [r0 + L k / m, r0 + L (k+1) / m);
+    // aggregate a (CTA lc, local k: a = lc m + k) owns coarse unknowns 6a .. 6a+5.
+    int32_t agg_per_cta;
+    int32_t n_coarse;            // 6 x aggregates
+    const double* pmode;         // [N][3][6] coarse modes of each node's DoFs
+    const double* coarse_inv;    // [n_coarse][n_coarse] row-major inverse of P^T J P
+    double* coarse_r;            // [n_coarse] restricted vector
 };
+
+constexpr int kMaxAggPerCta = 4;
 
 // --- element assembly (tf_element.cu) ---------------------------------------------------
 // mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class)
@@ -193,6 +203,24 @@ int spmv_grid(int n_nodes);
 // w.partials must hold 4 * plan.n_cta doubles.
 // threads: CTA width, 256 (three CTAs per SM, for batches of many tissues) or 768 (one per SM).
 int persistent_max_grid(int device, int threads);
+// Coarse operator of the two-level preconditioner, column-major dense n_coarse^2: entry
+// (6a+r, 6b+c) = sum over the Jacobian blocks k in rows of aggregate a and columns of
+// aggregate b of P_row(k)[:, r]^T J_k P_col(k)[:, c]. Blocks are listed per (aggregate, slot)
+// with slot_agg[slot] = b, summed in list order (deterministic). Coarse unknowns whose mode is
+// empty get a unit diagonal.
+struct CoarseAssembly {
+    int32_t n_agg, n_coarse;
+    const int32_t* agg_slot_ptr;   // [n_agg+1] slots of each aggregate
+    const int32_t* slot_agg;       // [slots] neighbour aggregate of each slot
+    const int32_t* slot_ptr;       // [slots+1] offsets into blk / blk_row
+    const int32_t* blk;            // Jacobian block ids
+    const int32_t* blk_row;        // their block rows
+    const int32_t* empty;          // [n_empty] coarse unknowns without a mode
+    int32_t n_empty;
+};
+cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
+                                   cudaStream_t s);
+cudaError_t launch_set_identity(double* m, int n, cudaStream_t s);
 cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
                                     int threads, cudaStream_t s);
 // uk += du on active tissues, du[slave] = du[master], per-tissue ||du||^2 into plan.du2

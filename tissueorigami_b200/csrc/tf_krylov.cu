@@ -455,6 +455,81 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
     D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
+// out = M^-1 in on the CTA's rows [r0, r1): block-Jacobi D^-1, plus with a coarse space
+// (plan.agg_per_cta = m > 0) the additive correction P (P^T J P)^-1 P^T in. The restriction
+// of the CTA's m aggregates is summed inside the CTA (fixed order), written to coarse_r, and
+// after a group barrier every CTA multiplies its 6m rows of the dense coarse inverse with the
+// whole restricted vector and prolongs the result onto its own rows. Returns false when the
+// group barrier timed out.
+__device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, const double* in,
+                              double* out, GridBarrier* bar, int nct, double* red, double* ys) {
+    const int m = plan.agg_per_cta;
+    if (m == 0) {
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
+        return true;
+    }
+    const int L = r1 - r0;
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
+    __syncthreads();  // the restriction below reads rows of `in` written by other threads of the CTA
+    // restriction: the CTA's warps split evenly over its m aggregates; lanes stride the rows,
+    // then a warp sum and a fixed-order sum over the aggregate's warps
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int wpa = nw / m;
+    {
+        const int k = warp / wpa, wi = warp - k * wpa;
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (k < m) {
+            const int a0 = r0 + (int)((long long)L * k / m), a1 = r0 + (int)((long long)L * (k + 1) / m);
+            for (int n = a0 + wi * 32 + lane; n < a1; n += wpa * 32) {
+                const double* P = plan.pmode + (size_t)n * 18;
+                const double a = in[n * 3], b = in[n * 3 + 1], c = in[n * 3 + 2];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) acc[q] += P[q] * a + P[6 + q] * b + P[12 + q] * c;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+        if (lane == 0 && k < m)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) red[warp * 6 + q] = acc[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6 * m) {
+        const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
+        double sum = 0.0;
+        for (int wi = 0; wi < wpa; ++wi) sum += red[(k * wpa + wi) * 6 + q];
+        plan.coarse_r[6 * lc * m + threadIdx.x] = sum;
+    }
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    // this CTA's 6m rows of the coarse inverse times the restricted vector, one warp per row
+    const int nc = plan.n_coarse;
+    for (int j = warp; j < 6 * m; j += nw) {
+        const double* row = plan.coarse_inv + (size_t)(6 * lc * m + j) * nc;
+        double sum = 0.0;
+        for (int c = lane; c < nc; c += 32) sum += __ldcg(row + c) * __ldcg(plan.coarse_r + c);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (lane == 0) ys[j] = sum;
+    }
+    __syncthreads();
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        int k = 0;
+        while (k + 1 < m && n >= r0 + (int)((long long)L * (k + 1) / m)) ++k;
+        const double* P = plan.pmode + (size_t)n * 18;
+        const double* y = ys + 6 * k;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double v = 0.0;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v += P[d * 6 + q] * y[q];
+            out[n * 3 + d] += v;
+        }
+    }
+    return true;
+}
+
 // BiCGStab restart after a breakdown: rhat = r, p = v = 0, rho = (r, r); at most kMaxRestarts
 // per solve. Returns false when the restarts are used up (the caller reports a breakdown).
 constexpr int kMaxRestarts = 8;
@@ -488,6 +563,8 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                                                                       int max_iter) {
     __shared__ double smem[32 * 2];
     __shared__ double sb[2];
+    __shared__ double red[32 * 6];
+    __shared__ double ys[kMaxAggPerCta * 6];
     const int t = plan.cta_tissue[blockIdx.x];
     if (!plan.active[t]) return;
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
@@ -525,7 +602,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     int it = 0, restarts = 0;
     int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
     while (status == KS_RUNNING) {
-        // A: p = r + beta (p - omega v); phat = D^-1 p
+        // A: p = r + beta (p - omega v); phat = M^-1 p
         const double beta = (rho / rho_prev) * (alpha / omega);
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -533,8 +610,8 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 const int d = n * 3 + i;
                 w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
             }
-            apply_dinv(w.dinv, n, w.p, w.phat);
         }
+        if (!precond_apply(w, plan, lc, r0, r1, w.p, w.phat, bar, nct, red, ys)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
@@ -554,15 +631,15 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
             continue;
         }
         alpha = rho / t1[0];
-        // C: s = r - alpha v; shat = D^-1 s
+        // C: s = r - alpha v; shat = M^-1 s
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const int d = n * 3 + i;
                 w.s[d] = w.r[d] - alpha * w.v[d];
             }
-            apply_dinv(w.dinv, n, w.s, w.shat);
         }
+        if (!precond_apply(w, plan, lc, r0, r1, w.s, w.shat, bar, nct, red, ys)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
@@ -819,6 +896,61 @@ cudaError_t launch_bicgstab_iteration_ilu(const KrylovWork& w, const IluPlan& il
     ilu_apply(w, ilu, w.s, w.shat, s);
     k_spmv<2><<<sg, kSpmvThreads, 0, s>>>(w, w.shat, w.t, 1);
     k_bicg_xr<<<vg, kVecThreads, 0, s>>>(w);
+    return cudaGetLastError();
+}
+
+namespace {
+
+// One CTA per aggregate a; thread t of a slot s computes entry e = (r, c) of the 6x6 coarse
+// block (a, slot_agg[s]) by summing its Jacobian blocks in list order.
+__global__ void k_coarse_assemble(KrylovWork w, CoarseAssembly ca, const double* __restrict__ pmode,
+                                  double* __restrict__ a_cm) {
+    const int a = blockIdx.x;
+    if (a >= ca.n_agg) return;
+    const int s0 = ca.agg_slot_ptr[a], ns = ca.agg_slot_ptr[a + 1] - s0;
+    for (int t = threadIdx.x; t < ns * 36; t += blockDim.x) {
+        const int s = s0 + t / 36, e = t % 36, r = e / 6, c = e % 6;
+        double sum = 0.0;
+        for (int q = ca.slot_ptr[s]; q < ca.slot_ptr[s + 1]; ++q) {
+            const int k = ca.blk[q];
+            const int i = ca.blk_row[q], j = __ldg(w.colidx + k);
+            const double* J = w.vals + (size_t)k * 9;
+            const double* Pi = pmode + (size_t)i * 18;
+            const double* Pj = pmode + (size_t)j * 18;
+            const double u0 = Pj[c], u1 = Pj[6 + c], u2 = Pj[12 + c];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                sum += Pi[d * 6 + r] * (__ldg(J + d * 3) * u0 + __ldg(J + d * 3 + 1) * u1 + __ldg(J + d * 3 + 2) * u2);
+        }
+        const int R = 6 * a + r, C = 6 * ca.slot_agg[s] + c;
+        a_cm[(size_t)R + (size_t)C * ca.n_coarse] = sum;
+    }
+}
+
+__global__ void k_coarse_empty(double* a_cm, int n, const int32_t* empty, int n_empty) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_empty) a_cm[(size_t)empty[i] * (n + 1)] = 1.0;
+}
+
+__global__ void k_set_identity(double* m, int n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < (size_t)n * n) m[i] = (i % (size_t)(n + 1) == 0) ? 1.0 : 0.0;
+}
+
+}  // namespace
+
+cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
+                                   cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(a_cm, 0, sizeof(double) * (size_t)ca.n_coarse * ca.n_coarse, s);
+    if (e != cudaSuccess) return e;
+    if (ca.n_agg > 0) k_coarse_assemble<<<ca.n_agg, 256, 0, s>>>(w, ca, pmode, a_cm);
+    if (ca.n_empty > 0) k_coarse_empty<<<(ca.n_empty + 255) / 256, 256, 0, s>>>(a_cm, ca.n_coarse, ca.empty, ca.n_empty);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_identity(double* m, int n, cudaStream_t s) {
+    const size_t total = (size_t)n * n;
+    k_set_identity<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(m, n);
     return cudaGetLastError();
 }
 
