@@ -29,6 +29,7 @@ using namespace tfb;
 namespace {
 
 constexpr int kChunk = 32;  // BiCGStab iterations per graph replay / status poll
+constexpr int kCoarseMaxAge = 16;  // solves between refreshes of the two-level coarse operator
 
 struct DevBuf {
     void* p = nullptr;
@@ -87,6 +88,9 @@ struct tf_ctx {
     int coarse_m = 0, n_coarse = 0, n_agg = 0, coarse_lwork = 0, n_coarse_empty = 0;
     bool coarse_ok = false;  // the last coarse factorisation succeeded
     DevBuf pmode_d, coarse_a, coarse_inv, coarse_r, coarse_ipiv, coarse_info, coarse_work;
+    DevBuf node_d, node_mask, agg_m;
+    int coarse_age = 0, coarse_base_iters = 0;  // solves since the last coarse refresh; iterations of the first
+    int last_solve_iters = 0;
     DevBuf ca_agg_slot_ptr, ca_slot_agg, ca_slot_ptr, ca_blk, ca_blk_row, ca_empty;
     cusolverDnHandle_t dn = nullptr;
     int32_t* h_coarse_info = nullptr;  // pinned
@@ -588,7 +592,9 @@ BatchPlan make_plan(tf_ctx* c) {
     BatchPlan p;
     p.agg_per_cta = (c->coarse_m > 0 && c->coarse_ok) ? c->coarse_m : 0;
     p.n_coarse = c->n_coarse;
-    p.pmode = dptr<double>(c->pmode_d);
+    p.node_d = dptr<double>(c->node_d);
+    p.node_mask = dptr<uint8_t>(c->node_mask);
+    p.agg_m = dptr<double>(c->agg_m);
     p.coarse_inv = dptr<double>(c->coarse_inv);
     p.coarse_r = dptr<double>(c->coarse_r);
     p.n_tissues = c->T;
@@ -686,6 +692,7 @@ int build_coarse(tf_ctx* ctx) {
     const int nw = ctx->persist_threads / 32;
     while (m > 1 && nw / m < 1) --m;
     const int n_agg = nct * m, nc = 6 * n_agg;
+    if (nc > kMaxCoarse) return TF_OK;  // plan too large for a staged coarse vector: block-Jacobi only
     std::vector<double> X((size_t)N * 3, 0.0);
     for (int e = 0; e < ctx->E; ++e)
         for (int a = 0; a < 6; ++a)
@@ -696,36 +703,42 @@ int build_coarse(tf_ctx* ctx) {
         for (int k = 0; k < m; ++k) agg0[lc * m + k] = r0 + (int)((long long)L * k / m);
     }
     agg0[n_agg] = N;
-    std::vector<double> pm((size_t)N * 18, 0.0);
+    std::vector<double> pm((size_t)N * 18, 0.0), nd((size_t)N * 3, 0.0), am((size_t)n_agg * 36, 0.0);
+    std::vector<uint8_t> nmask(N, 0);
     std::vector<int32_t> empty;
+    for (int i = 0; i < N; ++i)
+        for (int d = 0; d < 3; ++d) {
+            const size_t dof = (size_t)i * 3 + d;
+            const bool fixed = (ctx->h_fixmask.size() == (size_t)N) && (ctx->h_fixmask[i] >> d & 1);
+            if (!fixed && ctx->dofmap[dof] == (int32_t)dof) nmask[i] |= (uint8_t)(1u << d);
+        }
     for (int a = 0; a < n_agg; ++a) {
         const int s0 = agg0[a], n = agg0[a + 1] - s0;
-        if (n <= 0) {
-            for (int q = 0; q < 6; ++q) empty.push_back(6 * a + q);
-            continue;
-        }
         double c[3] = {0, 0, 0};
         for (int i = 0; i < n; ++i)
             for (int d = 0; d < 3; ++d) c[d] += X[(size_t)(s0 + i) * 3 + d] / n;
+        // the masked modes B_i = [I | (d_i x)] as explicit columns over the aggregate's DoFs
         const size_t len = (size_t)3 * n;
         std::vector<double> B(6 * len, 0.0);
         for (int i = 0; i < n; ++i) {
-            const double dx = X[(size_t)(s0 + i) * 3] - c[0], dy = X[(size_t)(s0 + i) * 3 + 1] - c[1],
-                         dz = X[(size_t)(s0 + i) * 3 + 2] - c[2];
-            for (int q = 0; q < 3; ++q) B[q * len + 3 * i + q] = 1.0;
-            B[3 * len + 3 * i + 1] = -dz, B[3 * len + 3 * i + 2] = dy;   // rotation about x
-            B[4 * len + 3 * i + 0] = dz, B[4 * len + 3 * i + 2] = -dx;   // about y
-            B[5 * len + 3 * i + 0] = -dy, B[5 * len + 3 * i + 1] = dx;   // about z
-            for (int d = 0; d < 3; ++d) {
-                const size_t dof = (size_t)(s0 + i) * 3 + d;
-                const bool fixed = (ctx->h_fixmask.size() == (size_t)N) && (ctx->h_fixmask[s0 + i] >> d & 1);
-                if (fixed || ctx->dofmap[dof] != (int32_t)dof)
-                    for (int q = 0; q < 6; ++q) B[q * len + 3 * i + d] = 0.0;
-            }
+            const int node = s0 + i;
+            double dd[3];
+            for (int d = 0; d < 3; ++d) dd[d] = nd[(size_t)node * 3 + d] = X[(size_t)node * 3 + d] - c[d];
+            const double Bi[3][6] = {{1, 0, 0, 0, dd[2], -dd[1]}, {0, 1, 0, -dd[2], 0, dd[0]}, {0, 0, 1, dd[1], -dd[0], 0}};
+            for (int d = 0; d < 3; ++d)
+                if (nmask[node] >> d & 1)
+                    for (int q = 0; q < 6; ++q) B[q * len + 3 * i + d] = Bi[d][q];
         }
-        std::vector<char> kept(6, 0);
+        // modified Gram-Schmidt (two passes) on the explicit columns, the same operations applied
+        // to coefficient vectors, so that the orthonormal columns are B m_q; a mode whose norm
+        // falls below 1e-6 of its initial norm is dropped
+        double M[36] = {0};
+        bool kept[6] = {false, false, false, false, false, false};
+        double cols[6][6] = {{0}};
         for (int q = 0; q < 6; ++q) {
             double* bq = &B[q * len];
+            double v[6] = {0, 0, 0, 0, 0, 0};
+            v[q] = 1.0;
             double n0 = 0.0;
             for (size_t r = 0; r < len; ++r) n0 += bq[r] * bq[r];
             n0 = std::sqrt(n0);
@@ -736,18 +749,24 @@ int build_coarse(tf_ctx* ctx) {
                     double dot = 0.0;
                     for (size_t r = 0; r < len; ++r) dot += bp[r] * bq[r];
                     for (size_t r = 0; r < len; ++r) bq[r] -= dot * bp[r];
+                    for (int r = 0; r < 6; ++r) v[r] -= dot * cols[p][r];
                 }
             double nq = 0.0;
             for (size_t r = 0; r < len; ++r) nq += bq[r] * bq[r];
             nq = std::sqrt(nq);
-            if (n0 == 0.0 || nq <= 1e-10 * n0) {
+            if (n == 0 || n0 == 0.0 || nq <= 1e-6 * n0) {
                 for (size_t r = 0; r < len; ++r) bq[r] = 0.0;
                 empty.push_back(6 * a + q);
                 continue;
             }
-            kept[q] = 1;
+            kept[q] = true;
             for (size_t r = 0; r < len; ++r) bq[r] /= nq;
+            for (int r = 0; r < 6; ++r) cols[q][r] = v[r] / nq;
         }
+        for (int p = 0; p < 6; ++p)
+            for (int q = 0; q < 6; ++q) M[p * 6 + q] = kept[q] ? cols[q][p] : 0.0;  // M[p][q] = (m_q)_p
+        for (int k = 0; k < 36; ++k) am[(size_t)a * 36 + k] = M[k];
+        // explicit modes for the coarse-operator assembly: P_i = mask_i o (B_i M)
         for (int i = 0; i < n; ++i)
             for (int d = 0; d < 3; ++d)
                 for (int q = 0; q < 6; ++q) pm[(size_t)(s0 + i) * 18 + d * 6 + q] = B[q * len + 3 * i + d];
@@ -782,6 +801,9 @@ int build_coarse(tf_ctx* ctx) {
         return e;
     };
     TF_CK(up(ctx->pmode_d, pm.data(), sizeof(double) * pm.size()));
+    TF_CK(up(ctx->node_d, nd.data(), sizeof(double) * nd.size()));
+    TF_CK(up(ctx->node_mask, nmask.data(), nmask.size()));
+    TF_CK(up(ctx->agg_m, am.data(), sizeof(double) * am.size()));
     TF_CK(up(ctx->ca_agg_slot_ptr, agg_slot_ptr.data(), sizeof(int32_t) * agg_slot_ptr.size()));
     TF_CK(up(ctx->ca_slot_agg, slot_agg.data(), sizeof(int32_t) * slot_agg.size()));
     TF_CK(up(ctx->ca_slot_ptr, slot_ptr.data(), sizeof(int32_t) * slot_ptr.size()));
@@ -808,6 +830,8 @@ int build_coarse(tf_ctx* ctx) {
     ctx->n_coarse = nc;
     ctx->n_coarse_empty = (int)empty.size();
     ctx->coarse_m = m;
+    ctx->coarse_age = 0;
+    ctx->coarse_ok = false;
     return TF_OK;
 }
 
@@ -862,8 +886,17 @@ int krylov_solve(tf_ctx* ctx) {
                 const int crc = build_coarse(ctx);
                 if (crc != TF_OK) return crc;
             }
-            const int crc = coarse_setup(ctx);
-            if (crc != TF_OK) return crc;
+            // The coarse operator is refreshed from the current J when it is missing, after
+            // kCoarseMaxAge solves, or when the last solve needed 1.3x the iterations of the
+            // first solve after the refresh; in between the previous inverse preconditions (any
+            // fixed operator is a valid preconditioner: convergence is tested on the residual).
+            const bool stale = !ctx->coarse_ok || ctx->coarse_age >= kCoarseMaxAge ||
+                               (ctx->coarse_age > 1 && ctx->last_solve_iters * 10 > ctx->coarse_base_iters * 13);
+            if (ctx->coarse_m > 0 && stale) {
+                const int crc = coarse_setup(ctx);
+                if (crc != TF_OK) return crc;
+                ctx->coarse_age = 0;
+            }
         }
         const BatchPlan plan = make_plan(ctx);
         TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
@@ -887,6 +920,11 @@ int krylov_solve(tf_ctx* ctx) {
             return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
         }
         *ctx->h_sc = ctx->h_tsc[0];
+        ctx->last_solve_iters = ctx->h_sc->iter;
+        if (ctx->coarse_m > 0 && ctx->coarse_ok) {
+            if (ctx->coarse_age == 0) ctx->coarse_base_iters = ctx->h_sc->iter;
+            ++ctx->coarse_age;
+        }
         return TF_OK;
     }
     const bool ilu = ctx->params.precond == TF_PRECOND_ILU0;
@@ -1336,7 +1374,7 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->ilu_lo_idx, &ctx->ilu_up_ptr, &ctx->ilu_up_idx, &ctx->ilu_lu, &ctx->ilu_uinv, &ctx->ilu_y};
     for (DevBuf* b : adj) dfree(*b);
     if (ctx->ilu_graph) cudaGraphExecDestroy(ctx->ilu_graph);
-    DevBuf* coarse[] = {&ctx->pmode_d, &ctx->coarse_a, &ctx->coarse_inv, &ctx->coarse_r, &ctx->coarse_ipiv,
+    DevBuf* coarse[] = {&ctx->node_d, &ctx->node_mask, &ctx->agg_m, &ctx->pmode_d, &ctx->coarse_a, &ctx->coarse_inv, &ctx->coarse_r, &ctx->coarse_ipiv,
                         &ctx->coarse_info, &ctx->coarse_work, &ctx->ca_agg_slot_ptr, &ctx->ca_slot_agg,
                         &ctx->ca_slot_ptr, &ctx->ca_blk, &ctx->ca_blk_row, &ctx->ca_empty};
     for (DevBuf* b : coarse) dfree(*b);

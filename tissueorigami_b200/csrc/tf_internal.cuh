@@ -117,14 +117,20 @@ struct BatchPlan {
     // two-level preconditioner of a single tissue (agg_per_cta = 0: block-Jacobi only). Each
     // CTA's rows [r0, r1) split into agg_per_cta aggregates [r0 + L k / m, r0 + L (k+1) / m);
     // aggregate a (CTA lc, local k: a = lc m + k) owns coarse unknowns 6a .. 6a+5.
+    // The modes of node i in aggregate a are P_i = mask_i o (B_i M_a), B_i = [I | (d_i x)]
+    // (translations, rotations about the aggregate centroid, d_i = X_i - centroid), mask_i the
+    // node's free DoFs (bit d), M_a a 6x6 orthonormalising transform (dropped modes: zero columns).
     int32_t agg_per_cta;
     int32_t n_coarse;            // 6 x aggregates
-    const double* pmode;         // [N][3][6] coarse modes of each node's DoFs
+    const double* node_d;        // [N][3] d_i
+    const uint8_t* node_mask;    // [N]
+    const double* agg_m;         // [aggregates][6][6] M_a, row-major
     const double* coarse_inv;    // [n_coarse][n_coarse] row-major inverse of P^T J P
     double* coarse_r;            // [n_coarse] restricted vector
 };
 
 constexpr int kMaxAggPerCta = 4;
+constexpr int kMaxCoarse = 3072;  // coarse unknowns the persistent solve stages in shared memory
 
 // --- element assembly (tf_element.cu) ---------------------------------------------------
 // mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class)

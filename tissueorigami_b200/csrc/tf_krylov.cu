@@ -458,11 +458,11 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
 // out = M^-1 in on the CTA's rows [r0, r1): block-Jacobi D^-1, plus with a coarse space
 // (plan.agg_per_cta = m > 0) the additive correction P (P^T J P)^-1 P^T in. The restriction
 // of the CTA's m aggregates is summed inside the CTA (fixed order), written to coarse_r, and
-// after a group barrier every CTA multiplies its 6m rows of the dense coarse inverse with the
-// whole restricted vector and prolongs the result onto its own rows. Returns false when the
-// group barrier timed out.
+// after a group barrier every CTA stages the whole restricted vector in shared memory,
+// multiplies its 6m rows of the dense coarse inverse with it and prolongs the result onto its
+// own rows. Returns false when the group barrier timed out.
 __device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, const double* in,
-                              double* out, GridBarrier* bar, int nct, double* red, double* ys) {
+                              double* out, GridBarrier* bar, int nct, double* red, double* ys, double* cs) {
     const int m = plan.agg_per_cta;
     if (m == 0) {
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
@@ -471,8 +471,9 @@ __device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc
     const int L = r1 - r0;
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
     __syncthreads();  // the restriction below reads rows of `in` written by other threads of the CTA
-    // restriction: the CTA's warps split evenly over its m aggregates; lanes stride the rows,
-    // then a warp sum and a fixed-order sum over the aggregate's warps
+    // restriction: B_i^T (mask_i o in_i) = (u, d_i x u) summed per aggregate - the CTA's warps
+    // split evenly over its m aggregates, lanes stride the rows, then a warp sum and a
+    // fixed-order sum over the aggregate's warps - and M_a^T applied
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int wpa = nw / m;
     {
@@ -481,10 +482,16 @@ __device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc
         if (k < m) {
             const int a0 = r0 + (int)((long long)L * k / m), a1 = r0 + (int)((long long)L * (k + 1) / m);
             for (int n = a0 + wi * 32 + lane; n < a1; n += wpa * 32) {
-                const double* P = plan.pmode + (size_t)n * 18;
-                const double a = in[n * 3], b = in[n * 3 + 1], c = in[n * 3 + 2];
-#pragma unroll
-                for (int q = 0; q < 6; ++q) acc[q] += P[q] * a + P[6 + q] * b + P[12 + q] * c;
+                const int mk = plan.node_mask[n];
+                const double u0 = (mk & 1) ? in[n * 3] : 0.0, u1 = (mk & 2) ? in[n * 3 + 1] : 0.0,
+                             u2 = (mk & 4) ? in[n * 3 + 2] : 0.0;
+                const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+                acc[0] += u0;
+                acc[1] += u1;
+                acc[2] += u2;
+                acc[3] += dy * u2 - dz * u1;
+                acc[4] += dz * u0 - dx * u2;
+                acc[5] += dx * u1 - dy * u0;
             }
         }
 #pragma unroll
@@ -498,35 +505,70 @@ __device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc
     __syncthreads();
     if (threadIdx.x < 6 * m) {
         const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
+        const double* M = plan.agg_m + (size_t)(lc * m + k) * 36;
         double sum = 0.0;
-        for (int wi = 0; wi < wpa; ++wi) sum += red[(k * wpa + wi) * 6 + q];
+        for (int p = 0; p < 6; ++p) {
+            double t = 0.0;
+            for (int wi = 0; wi < wpa; ++wi) t += red[(k * wpa + wi) * 6 + p];
+            sum += M[p * 6 + q] * t;
+        }
         plan.coarse_r[6 * lc * m + threadIdx.x] = sum;
     }
     if (!group_barrier(bar, nct, w.dflags)) return false;
-    // this CTA's 6m rows of the coarse inverse times the restricted vector, one warp per row
+    // stage the restricted vector, then this CTA's 6m rows of the coarse inverse times it: the
+    // warps split as evenly as possible over the rows, each row's columns over its warps
     const int nc = plan.n_coarse;
-    for (int j = warp; j < 6 * m; j += nw) {
-        const double* row = plan.coarse_inv + (size_t)(6 * lc * m + j) * nc;
-        double sum = 0.0;
-        for (int c = lane; c < nc; c += 32) sum += __ldcg(row + c) * __ldcg(plan.coarse_r + c);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-        if (lane == 0) ys[j] = sum;
-    }
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) cs[c] = __ldcg(plan.coarse_r + c);
     __syncthreads();
+    const int rows = 6 * m;
+    const int wpr = nw >= rows ? nw / rows : 1;  // warps per row
+    {
+        double* part = red;  // reused: [rows][wpr] partial sums (rows * wpr <= nw <= 32)
+        for (int j0 = 0; j0 < rows; j0 += nw / wpr) {
+            const int j = j0 + warp / wpr, pw = warp % wpr;
+            if (warp / wpr >= nw / wpr || j >= rows) continue;
+            const double* row = plan.coarse_inv + (size_t)(6 * lc * m + j) * nc;
+            double s0 = 0.0, s1 = 0.0;
+            int c = (pw * 32 + lane);
+            for (; c + 32 * wpr < nc; c += 64 * wpr) {
+                s0 += __ldcg(row + c) * cs[c];
+                s1 += __ldcg(row + c + 32 * wpr) * cs[c + 32 * wpr];
+            }
+            if (c < nc) s0 += __ldcg(row + c) * cs[c];
+            s0 += s1;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+            if (lane == 0) part[j * wpr + pw] = s0;
+        }
+        __syncthreads();
+        if (threadIdx.x < rows) {
+            double t = 0.0;
+            for (int pw = 0; pw < wpr; ++pw) t += part[threadIdx.x * wpr + pw];
+            ys[threadIdx.x] = t;
+        }
+        __syncthreads();
+        // z_a = M_a y_a: translation and rotation of each aggregate's correction
+        if (threadIdx.x < rows) {
+            const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
+            const double* M = plan.agg_m + (size_t)(lc * m + k) * 36;
+            double z = 0.0;
+            for (int p = 0; p < 6; ++p) z += M[q * 6 + p] * ys[6 * k + p];
+            part[threadIdx.x] = z;
+        }
+        __syncthreads();
+    }
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
         int k = 0;
         while (k + 1 < m && n >= r0 + (int)((long long)L * (k + 1) / m)) ++k;
-        const double* P = plan.pmode + (size_t)n * 18;
-        const double* y = ys + 6 * k;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double v = 0.0;
-#pragma unroll
-            for (int q = 0; q < 6; ++q) v += P[d * 6 + q] * y[q];
-            out[n * 3 + d] += v;
-        }
+        const double* z = red + 6 * k;
+        const int mk = plan.node_mask[n];
+        const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+        // t + omega x d
+        if (mk & 1) out[n * 3] += z[0] + z[4] * dz - z[5] * dy;
+        if (mk & 2) out[n * 3 + 1] += z[1] + z[5] * dx - z[3] * dz;
+        if (mk & 4) out[n * 3 + 2] += z[2] + z[3] * dy - z[4] * dx;
     }
+    __syncthreads();  // red is reused by the next restriction
     return true;
 }
 
@@ -565,6 +607,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     __shared__ double sb[2];
     __shared__ double red[32 * 6];
     __shared__ double ys[kMaxAggPerCta * 6];
+    __shared__ double cs[kMaxCoarse];
     const int t = plan.cta_tissue[blockIdx.x];
     if (!plan.active[t]) return;
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
@@ -611,7 +654,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
             }
         }
-        if (!precond_apply(w, plan, lc, r0, r1, w.p, w.phat, bar, nct, red, ys)) return;
+        if (!precond_apply(w, plan, lc, r0, r1, w.p, w.phat, bar, nct, red, ys, cs)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
@@ -639,7 +682,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 w.s[d] = w.r[d] - alpha * w.v[d];
             }
         }
-        if (!precond_apply(w, plan, lc, r0, r1, w.s, w.shat, bar, nct, red, ys)) return;
+        if (!precond_apply(w, plan, lc, r0, r1, w.s, w.shat, bar, nct, red, ys, cs)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
