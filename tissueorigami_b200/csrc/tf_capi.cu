@@ -689,6 +689,9 @@ int build_coarse(tf_ctx* ctx) {
     if (nct <= 0) return TF_OK;
     int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
     while (m > 1 && N / (nct * m) < 8) --m;
+    // each CTA's 6m rows of the n_coarse = 6 nct m inverse must fit its shared-memory block
+    while (m > 1 && (size_t)36 * nct * m * m * sizeof(double) > (size_t)kCoarseSmemBytes) --m;
+    if ((size_t)36 * nct * m * m * sizeof(double) > (size_t)kCoarseSmemBytes) return TF_OK;
     const int nw = ctx->persist_threads / 32;
     while (m > 1 && nw / m < 1) --m;
     const int n_agg = nct * m, nc = 6 * n_agg;
@@ -1274,7 +1277,10 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         // in a batch many tissues each with their own CTAs)
         int sms = 0;
         TF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-        ctx->persist_threads = (T == 1 && (int64_t)ctx->N >= (int64_t)sms * 256) ? 768 : 256;
+        ctx->persist_threads = (T == 1 && ((int64_t)ctx->N >= (int64_t)sms * 256 ||
+                                           ctx->params.precond == TF_PRECOND_TWO_LEVEL))
+                                   ? 768
+                                   : 256;
         ctx->persistent_grid_max = coop ? persistent_max_grid(ctx->device, ctx->persist_threads) : 0;
     }
     TF_CK(cudaMemset(ctx->sc.p, 0, sizeof(KrylovScalars)));

@@ -125,12 +125,15 @@ struct BatchPlan {
     const double* node_d;        // [N][3] d_i
     const uint8_t* node_mask;    // [N]
     const double* agg_m;         // [aggregates][6][6] M_a, row-major
-    const double* coarse_inv;    // [n_coarse][n_coarse] row-major inverse of P^T J P
+    const double* coarse_inv;    // [n_coarse][n_coarse] row-major inverse of P^T J P (read once per solve)
     double* coarse_r;            // [n_coarse] restricted vector
 };
 
 constexpr int kMaxAggPerCta = 4;
 constexpr int kMaxCoarse = 3072;  // coarse unknowns the persistent solve stages in shared memory
+// Each CTA keeps its 6m rows of the coarse inverse in dynamic shared memory for the whole solve
+// (6m x n_coarse doubles); the two-level solve runs one 768-thread CTA per SM.
+constexpr int kCoarseSmemBytes = 172 * 1024;
 
 // --- element assembly (tf_element.cu) ---------------------------------------------------
 // mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class)
@@ -228,7 +231,7 @@ cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca
                                    cudaStream_t s);
 cudaError_t launch_set_identity(double* m, int n, cudaStream_t s);
 cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
-                                    int threads, cudaStream_t s);
+                                    int threads, cudaStream_t s);  // dynamic smem: the plan's coarse row block
 // uk += du on active tissues, du[slave] = du[master], per-tissue ||du||^2 into plan.du2
 cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
                                          const int32_t* slaves, const int32_t* masters, int32_t n_pairs,

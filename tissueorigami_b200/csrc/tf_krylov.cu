@@ -462,7 +462,8 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
 // multiplies its 6m rows of the dense coarse inverse with it and prolongs the result onto its
 // own rows. Returns false when the group barrier timed out.
 __device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, const double* in,
-                              double* out, GridBarrier* bar, int nct, double* red, double* ys, double* cs) {
+                              double* out, GridBarrier* bar, int nct, double* red, double* ys, double* cs,
+                              const double* cinv) {
     const int m = plan.agg_per_cta;
     if (m == 0) {
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
@@ -515,48 +516,44 @@ __device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc
         plan.coarse_r[6 * lc * m + threadIdx.x] = sum;
     }
     if (!group_barrier(bar, nct, w.dflags)) return false;
-    // stage the restricted vector, then this CTA's 6m rows of the coarse inverse times it: the
-    // warps split as evenly as possible over the rows, each row's columns over its warps
+    // stage the restricted vector, then this CTA's 6m rows of the coarse inverse (held in shared
+    // memory) times it, one aggregate (6 rows) at a time: every thread takes a stripe of
+    // columns; warp sums, then a fixed-order sum over the warps
     const int nc = plan.n_coarse;
     for (int c = threadIdx.x; c < nc; c += blockDim.x) cs[c] = __ldcg(plan.coarse_r + c);
     __syncthreads();
-    const int rows = 6 * m;
-    const int wpr = nw >= rows ? nw / rows : 1;  // warps per row
-    {
-        double* part = red;  // reused: [rows][wpr] partial sums (rows * wpr <= nw <= 32)
-        for (int j0 = 0; j0 < rows; j0 += nw / wpr) {
-            const int j = j0 + warp / wpr, pw = warp % wpr;
-            if (warp / wpr >= nw / wpr || j >= rows) continue;
-            const double* row = plan.coarse_inv + (size_t)(6 * lc * m + j) * nc;
-            double s0 = 0.0, s1 = 0.0;
-            int c = (pw * 32 + lane);
-            for (; c + 32 * wpr < nc; c += 64 * wpr) {
-                s0 += __ldcg(row + c) * cs[c];
-                s1 += __ldcg(row + c + 32 * wpr) * cs[c + 32 * wpr];
-            }
-            if (c < nc) s0 += __ldcg(row + c) * cs[c];
-            s0 += s1;
+    for (int k = 0; k < m; ++k) {
+        const double* rb = cinv + (size_t)(6 * k) * nc;
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+            const double x = cs[c];
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, off);
-            if (lane == 0) part[j * wpr + pw] = s0;
+            for (int q = 0; q < 6; ++q) acc[q] += rb[(size_t)q * nc + c] * x;
         }
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) red[warp * 6 + q] = acc[q];
         __syncthreads();
-        if (threadIdx.x < rows) {
+        if (threadIdx.x < 6) {
             double t = 0.0;
-            for (int pw = 0; pw < wpr; ++pw) t += part[threadIdx.x * wpr + pw];
-            ys[threadIdx.x] = t;
-        }
-        __syncthreads();
-        // z_a = M_a y_a: translation and rotation of each aggregate's correction
-        if (threadIdx.x < rows) {
-            const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
-            const double* M = plan.agg_m + (size_t)(lc * m + k) * 36;
-            double z = 0.0;
-            for (int p = 0; p < 6; ++p) z += M[q * 6 + p] * ys[6 * k + p];
-            part[threadIdx.x] = z;
+            for (int wi = 0; wi < nw; ++wi) t += red[wi * 6 + threadIdx.x];
+            ys[6 * k + threadIdx.x] = t;
         }
         __syncthreads();
     }
+    // z_a = M_a y_a: translation and rotation of each aggregate's correction
+    if (threadIdx.x < 6 * m) {
+        const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
+        const double* M = plan.agg_m + (size_t)(lc * m + k) * 36;
+        double z = 0.0;
+        for (int p = 0; p < 6; ++p) z += M[q * 6 + p] * ys[6 * k + p];
+        red[threadIdx.x] = z;
+    }
+    __syncthreads();
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
         int k = 0;
         while (k + 1 < m && n >= r0 + (int)((long long)L * (k + 1) / m)) ++k;
@@ -608,6 +605,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     __shared__ double red[32 * 6];
     __shared__ double ys[kMaxAggPerCta * 6];
     __shared__ double cs[kMaxCoarse];
+    extern __shared__ double cinv_s[];  // this CTA's 6m rows of the coarse inverse
     const int t = plan.cta_tissue[blockIdx.x];
     if (!plan.active[t]) return;
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
@@ -618,6 +616,11 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     GridBarrier* bar = plan.barriers + t;
     double* part[2] = {w.partials + 4 * c0, w.partials + 4 * c0 + 2 * nct};
     int pb = 0;
+    if (plan.agg_per_cta > 0) {
+        const size_t cnt = (size_t)6 * plan.agg_per_cta * plan.n_coarse;
+        const double* src = plan.coarse_inv + (size_t)6 * lc * plan.agg_per_cta * plan.n_coarse;
+        for (size_t i = threadIdx.x; i < cnt; i += blockDim.x) cinv_s[i] = src[i];
+    }
     // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2
     double v1[1] = {0.0};
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
@@ -654,7 +657,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
             }
         }
-        if (!precond_apply(w, plan, lc, r0, r1, w.p, w.phat, bar, nct, red, ys, cs)) return;
+        if (!precond_apply(w, plan, lc, r0, r1, w.p, w.phat, bar, nct, red, ys, cs, cinv_s)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
@@ -682,7 +685,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 w.s[d] = w.r[d] - alpha * w.v[d];
             }
         }
-        if (!precond_apply(w, plan, lc, r0, r1, w.s, w.shat, bar, nct, red, ys, cs)) return;
+        if (!precond_apply(w, plan, lc, r0, r1, w.s, w.shat, bar, nct, red, ys, cs, cinv_s)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
@@ -1001,7 +1004,17 @@ int persistent_max_grid(int device, int threads) {
     int sms = 0, occ = 0;
     if (threads != 256 && threads != 768) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_bicgstab_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemBytes) !=
+        cudaSuccess)
+        return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_batched, threads, 0) != cudaSuccess) return 0;
+    if (threads == 768) {  // the two-level solve adds its coarse row block: still one CTA per SM
+        int occ_c = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_bicgstab_batched, threads, kCoarseSmemBytes) !=
+                cudaSuccess ||
+            occ_c < 1)
+            return 0;
+    }
     const int want = kPersistThreadsMax / threads;  // the kernel is built for 768 threads per SM
     return sms * (occ < want ? occ : want);
 }
@@ -1011,8 +1024,10 @@ cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, 
     KrylovWork wc = w;
     BatchPlan pc = plan;
     void* args[] = {&wc, &pc, &rtol, &max_iter};
+    const size_t smem = plan.agg_per_cta > 0 ? sizeof(double) * 6 * plan.agg_per_cta * (size_t)plan.n_coarse : 0;
+    if (smem > (size_t)kCoarseSmemBytes) return cudaErrorInvalidValue;
     return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_batched), dim3(plan.n_cta), dim3(threads),
-                                       args, 0, s);
+                                       args, smem, s);
 }
 
 cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
