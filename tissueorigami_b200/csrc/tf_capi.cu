@@ -690,8 +690,8 @@ int build_coarse(tf_ctx* ctx) {
     int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
     while (m > 1 && N / (nct * m) < 8) --m;
     // each CTA's 6m rows of the n_coarse = 6 nct m inverse must fit its shared-memory block
-    while (m > 1 && (size_t)36 * nct * m * m * sizeof(double) > (size_t)kCoarseSmemBytes) --m;
-    if ((size_t)36 * nct * m * m * sizeof(double) > (size_t)kCoarseSmemBytes) return TF_OK;
+    while (m > 1 && (size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) --m;
+    if ((size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) return TF_OK;
     const int nw = ctx->persist_threads / 32;
     while (m > 1 && nw / m < 1) --m;
     const int n_agg = nct * m, nc = 6 * n_agg;

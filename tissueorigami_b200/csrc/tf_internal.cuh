@@ -130,10 +130,13 @@ struct BatchPlan {
 };
 
 constexpr int kMaxAggPerCta = 4;
-constexpr int kMaxCoarse = 3072;  // coarse unknowns the persistent solve stages in shared memory
-// Each CTA keeps its 6m rows of the coarse inverse in dynamic shared memory for the whole solve
-// (6m x n_coarse doubles); the two-level solve runs one 768-thread CTA per SM.
-constexpr int kCoarseSmemBytes = 172 * 1024;
+constexpr int kMaxCoarse = 2048;  // coarse unknowns the persistent solve stages in shared memory
+// Each CTA keeps its 6m rows of the coarse inverse in dynamic shared memory for the whole solve,
+// rounded to FP32 (6m x n_coarse floats; the correction is accumulated in FP64 and the solve's
+// convergence test is on the FP64 residual, so this only changes the fixed preconditioner).
+// The block stays small enough that the SM keeps most of its L1 for the SpMV's matrix reuse.
+// The two-level solve runs one 768-thread CTA per SM.
+constexpr int kCoarseSmemBytes = 96 * 1024;
 
 // --- element assembly (tf_element.cu) ---------------------------------------------------
 // mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class)

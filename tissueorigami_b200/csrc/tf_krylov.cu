@@ -455,117 +455,117 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
     D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
-// out = M^-1 in on the CTA's rows [r0, r1): block-Jacobi D^-1, plus with a coarse space
-// (plan.agg_per_cta = m > 0) the additive correction P (P^T J P)^-1 P^T in. The restriction
-// of the CTA's m aggregates is summed inside the CTA (fixed order), written to coarse_r, and
-// after a group barrier every CTA stages the whole restricted vector in shared memory,
-// multiplies its 6m rows of the dense coarse inverse with it and prolongs the result onto its
-// own rows. Returns false when the group barrier timed out.
-__device__ bool precond_apply(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, const double* in,
-                              double* out, GridBarrier* bar, int nct, double* red, double* ys, double* cs,
-                              const double* cinv) {
-    const int m = plan.agg_per_cta;
-    if (m == 0) {
-        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
-        return true;
-    }
-    const int L = r1 - r0;
-    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) apply_dinv(w.dinv, n, in, out);
-    __syncthreads();  // the restriction below reads rows of `in` written by other threads of the CTA
-    // restriction: B_i^T (mask_i o in_i) = (u, d_i x u) summed per aggregate - the CTA's warps
-    // split evenly over its m aggregates, lanes stride the rows, then a warp sum and a
-    // fixed-order sum over the aggregate's warps - and M_a^T applied
+// Phase A (PH 0: p = r + beta (p - omega v), phat = M^-1 p) or C (PH 1: s = r - alpha v,
+// shat = M^-1 s) of an iteration on the CTA's rows [r0, r1), with the two-level
+// preconditioner M^-1 = D^-1 + P (P^T J P)^-1 P^T (plan.agg_per_cta = m > 0). The CTA's warps
+// split evenly over its m aggregates and keep one row mapping throughout, so the vector
+// update, D^-1, the restriction (mask o u, d x (mask o u)) and later the prolongation touch
+// each row from the same thread. The restriction is summed in fixed order (warp sums, then over
+// the aggregate's warps), multiplied by M_a^T and written to coarse_r; after a group barrier
+// every CTA stages the whole restricted vector, multiplies its 6m rows of the coarse inverse
+// (held in shared memory) with it, forms z_a = M_a y_a and adds t + omega x d to its rows.
+// Returns false when the group barrier timed out.
+template <int PH>
+__device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, double alpha,
+                              double beta, double omega, GridBarrier* bar, int nct, double* red, double* ys,
+                              double* cs, const float* cinv, const double* Ms) {
+    double* vin = PH == 0 ? w.p : w.s;
+    double* out = PH == 0 ? w.phat : w.shat;
+    const int m = plan.agg_per_cta, L = r1 - r0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int wpa = nw / m;
-    {
-        const int k = warp / wpa, wi = warp - k * wpa;
-        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (k < m) {
-            const int a0 = r0 + (int)((long long)L * k / m), a1 = r0 + (int)((long long)L * (k + 1) / m);
-            for (int n = a0 + wi * 32 + lane; n < a1; n += wpa * 32) {
-                const int mk = plan.node_mask[n];
-                const double u0 = (mk & 1) ? in[n * 3] : 0.0, u1 = (mk & 2) ? in[n * 3 + 1] : 0.0,
-                             u2 = (mk & 4) ? in[n * 3 + 2] : 0.0;
-                const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
-                acc[0] += u0;
-                acc[1] += u1;
-                acc[2] += u2;
-                acc[3] += dy * u2 - dz * u1;
-                acc[4] += dz * u0 - dx * u2;
-                acc[5] += dx * u1 - dy * u0;
+    const int k = warp / wpa, wi = warp - k * wpa;
+    const int a0 = r0 + (int)((long long)L * k / m), a1 = r0 + (int)((long long)L * (k + 1) / m);
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (k < m) {
+        for (int n = a0 + wi * 32 + lane; n < a1; n += wpa * 32) {
+            double u[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                u[i] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+                vin[d] = u[i];
             }
+            const double* D = w.dinv + (size_t)n * 9;
+            out[n * 3 + 0] = D[0] * u[0] + D[1] * u[1] + D[2] * u[2];
+            out[n * 3 + 1] = D[3] * u[0] + D[4] * u[1] + D[5] * u[2];
+            out[n * 3 + 2] = D[6] * u[0] + D[7] * u[1] + D[8] * u[2];
+            const int mk = plan.node_mask[n];
+            const double u0 = (mk & 1) ? u[0] : 0.0, u1 = (mk & 2) ? u[1] : 0.0, u2 = (mk & 4) ? u[2] : 0.0;
+            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+            acc[0] += u0;
+            acc[1] += u1;
+            acc[2] += u2;
+            acc[3] += dy * u2 - dz * u1;
+            acc[4] += dz * u0 - dx * u2;
+            acc[5] += dx * u1 - dy * u0;
         }
-#pragma unroll
-        for (int q = 0; q < 6; ++q)
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
-        if (lane == 0 && k < m)
-#pragma unroll
-            for (int q = 0; q < 6; ++q) red[warp * 6 + q] = acc[q];
     }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    if (lane == 0 && k < m)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) red[warp * 6 + q] = acc[q];
     __syncthreads();
     if (threadIdx.x < 6 * m) {
-        const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
-        const double* M = plan.agg_m + (size_t)(lc * m + k) * 36;
+        const int kk = threadIdx.x / 6, q = threadIdx.x - 6 * kk;
+        const double* M = Ms + kk * 36;
         double sum = 0.0;
         for (int p = 0; p < 6; ++p) {
             double t = 0.0;
-            for (int wi = 0; wi < wpa; ++wi) t += red[(k * wpa + wi) * 6 + p];
+            for (int j = 0; j < wpa; ++j) t += red[(kk * wpa + j) * 6 + p];
             sum += M[p * 6 + q] * t;
         }
         plan.coarse_r[6 * lc * m + threadIdx.x] = sum;
     }
     if (!group_barrier(bar, nct, w.dflags)) return false;
-    // stage the restricted vector, then this CTA's 6m rows of the coarse inverse (held in shared
-    // memory) times it, one aggregate (6 rows) at a time: every thread takes a stripe of
-    // columns; warp sums, then a fixed-order sum over the warps
     const int nc = plan.n_coarse;
     for (int c = threadIdx.x; c < nc; c += blockDim.x) cs[c] = __ldcg(plan.coarse_r + c);
     __syncthreads();
-    for (int k = 0; k < m; ++k) {
-        const double* rb = cinv + (size_t)(6 * k) * nc;
-        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int kk = 0; kk < m; ++kk) {
+        const float* rb = cinv + (size_t)(6 * kk) * nc;
+        double sacc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int c = threadIdx.x; c < nc; c += blockDim.x) {
             const double x = cs[c];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) acc[q] += rb[(size_t)q * nc + c] * x;
+            for (int q = 0; q < 6; ++q) sacc[q] += (double)rb[(size_t)q * nc + c] * x;
         }
 #pragma unroll
         for (int q = 0; q < 6; ++q)
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+            for (int off = 16; off > 0; off >>= 1) sacc[q] += __shfl_xor_sync(0xffffffffu, sacc[q], off);
         if (lane == 0)
 #pragma unroll
-            for (int q = 0; q < 6; ++q) red[warp * 6 + q] = acc[q];
+            for (int q = 0; q < 6; ++q) red[warp * 6 + q] = sacc[q];
         __syncthreads();
         if (threadIdx.x < 6) {
             double t = 0.0;
-            for (int wi = 0; wi < nw; ++wi) t += red[wi * 6 + threadIdx.x];
-            ys[6 * k + threadIdx.x] = t;
+            for (int j = 0; j < nw; ++j) t += red[j * 6 + threadIdx.x];
+            ys[6 * kk + threadIdx.x] = t;
         }
         __syncthreads();
     }
-    // z_a = M_a y_a: translation and rotation of each aggregate's correction
     if (threadIdx.x < 6 * m) {
-        const int k = threadIdx.x / 6, q = threadIdx.x - 6 * k;
-        const double* M = plan.agg_m + (size_t)(lc * m + k) * 36;
+        const int kk = threadIdx.x / 6, q = threadIdx.x - 6 * kk;
+        const double* M = Ms + kk * 36;
         double z = 0.0;
-        for (int p = 0; p < 6; ++p) z += M[q * 6 + p] * ys[6 * k + p];
+        for (int p = 0; p < 6; ++p) z += M[q * 6 + p] * ys[6 * kk + p];
         red[threadIdx.x] = z;
     }
     __syncthreads();
-    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
-        int k = 0;
-        while (k + 1 < m && n >= r0 + (int)((long long)L * (k + 1) / m)) ++k;
+    if (k < m) {
         const double* z = red + 6 * k;
-        const int mk = plan.node_mask[n];
-        const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
-        // t + omega x d
-        if (mk & 1) out[n * 3] += z[0] + z[4] * dz - z[5] * dy;
-        if (mk & 2) out[n * 3 + 1] += z[1] + z[5] * dx - z[3] * dz;
-        if (mk & 4) out[n * 3 + 2] += z[2] + z[3] * dy - z[4] * dx;
+        for (int n = a0 + wi * 32 + lane; n < a1; n += wpa * 32) {
+            const int mk = plan.node_mask[n];
+            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+            // t + omega x d
+            if (mk & 1) out[n * 3] += z[0] + z[4] * dz - z[5] * dy;
+            if (mk & 2) out[n * 3 + 1] += z[1] + z[5] * dx - z[3] * dz;
+            if (mk & 4) out[n * 3 + 2] += z[2] + z[3] * dy - z[4] * dx;
+        }
     }
-    __syncthreads();  // red is reused by the next restriction
     return true;
 }
 
@@ -602,10 +602,11 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                                                                       int max_iter) {
     __shared__ double smem[32 * 2];
     __shared__ double sb[2];
-    __shared__ double red[32 * 6];
+    __shared__ double red[32 * 6];  // per-warp partial sums of the coarse steps
     __shared__ double ys[kMaxAggPerCta * 6];
+    __shared__ double Ms[kMaxAggPerCta * 36];  // M_a of the CTA's aggregates
     __shared__ double cs[kMaxCoarse];
-    extern __shared__ double cinv_s[];  // this CTA's 6m rows of the coarse inverse
+    extern __shared__ float cinv_s[];  // this CTA's 6m rows of the coarse inverse (FP32)
     const int t = plan.cta_tissue[blockIdx.x];
     if (!plan.active[t]) return;
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
@@ -619,7 +620,9 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     if (plan.agg_per_cta > 0) {
         const size_t cnt = (size_t)6 * plan.agg_per_cta * plan.n_coarse;
         const double* src = plan.coarse_inv + (size_t)6 * lc * plan.agg_per_cta * plan.n_coarse;
-        for (size_t i = threadIdx.x; i < cnt; i += blockDim.x) cinv_s[i] = src[i];
+        for (size_t i = threadIdx.x; i < cnt; i += blockDim.x) cinv_s[i] = (float)src[i];
+        for (int i = threadIdx.x; i < 36 * plan.agg_per_cta; i += blockDim.x)
+            Ms[i] = plan.agg_m[(size_t)lc * plan.agg_per_cta * 36 + i];
     }
     // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2
     double v1[1] = {0.0};
@@ -650,14 +653,18 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     while (status == KS_RUNNING) {
         // A: p = r + beta (p - omega v); phat = M^-1 p
         const double beta = (rho / rho_prev) * (alpha / omega);
-        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        if (plan.agg_per_cta > 0) {
+            if (!precond_phase<0>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms)) return;
+        } else {
+            for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int d = n * 3 + i;
-                w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
+                for (int i = 0; i < 3; ++i) {
+                    const int d = n * 3 + i;
+                    w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
+                }
+                apply_dinv(w.dinv, n, w.p, w.phat);
             }
         }
-        if (!precond_apply(w, plan, lc, r0, r1, w.p, w.phat, bar, nct, red, ys, cs, cinv_s)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
@@ -678,14 +685,18 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
         }
         alpha = rho / t1[0];
         // C: s = r - alpha v; shat = M^-1 s
-        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        if (plan.agg_per_cta > 0) {
+            if (!precond_phase<1>(w, plan, lc, r0, r1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms)) return;
+        } else {
+            for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int d = n * 3 + i;
-                w.s[d] = w.r[d] - alpha * w.v[d];
+                for (int i = 0; i < 3; ++i) {
+                    const int d = n * 3 + i;
+                    w.s[d] = w.r[d] - alpha * w.v[d];
+                }
+                apply_dinv(w.dinv, n, w.s, w.shat);
             }
         }
-        if (!precond_apply(w, plan, lc, r0, r1, w.s, w.shat, bar, nct, red, ys, cs, cinv_s)) return;
         if (!group_barrier(bar, nct, w.dflags)) return;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
@@ -1024,7 +1035,7 @@ cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, 
     KrylovWork wc = w;
     BatchPlan pc = plan;
     void* args[] = {&wc, &pc, &rtol, &max_iter};
-    const size_t smem = plan.agg_per_cta > 0 ? sizeof(double) * 6 * plan.agg_per_cta * (size_t)plan.n_coarse : 0;
+    const size_t smem = plan.agg_per_cta > 0 ? sizeof(float) * 6 * plan.agg_per_cta * (size_t)plan.n_coarse : 0;
     if (smem > (size_t)kCoarseSmemBytes) return cudaErrorInvalidValue;
     return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_batched), dim3(plan.n_cta), dim3(threads),
                                        args, smem, s);
