@@ -564,7 +564,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")
-    ap.add_argument("--precond", choices=["block_jacobi", "ilu0", "two_level"], default="block_jacobi",
+    ap.add_argument("--precond", choices=["block_jacobi", "ilu0", "two_level"], default="two_level",
                     help="Krylov preconditioner of the single-tissue workloads")
     ap.add_argument("--persistent", type=int, choices=[0, 1], default=1,
                     help="solve path of the single-tissue workloads (tf_params.persistent)")

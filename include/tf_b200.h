@@ -49,9 +49,10 @@ extern "C" {
 /* ---- options ------------------------------------------------------------------------- */
 #define TF_PRECOND_BLOCK_JACOBI 0 /* 3x3 node-block inverse of the diagonal               */
 #define TF_PRECOND_ILU0 1         /* ILU(0) on the BSR3 pattern, multicolour ordered      */
-#define TF_PRECOND_TWO_LEVEL 2    /* block-Jacobi + additive coarse correction on node-     */
-                                  /* range aggregates with rigid-body modes (one tissue,    */
-                                  /* persistent solve)                                      */
+#define TF_PRECOND_TWO_LEVEL 2    /* default: block-Jacobi + additive coarse correction on  */
+                                  /* node-range aggregates with rigid-body modes; one       */
+                                  /* tissue with the persistent solve, elsewhere (batches,  */
+                                  /* persistent = 0) block-Jacobi is used instead           */
 
 #define TF_SCATTER_AUTO 0     /* pick by the autotuner's cached choice                   */
 #define TF_SCATTER_ATOMIC 1   /* FP64 atomics into the fixed BSR3 pattern                */
