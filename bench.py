@@ -280,6 +280,12 @@ def run_b200(args) -> None:
         direct = {"skipped": f"{nnz_scalar} scalar non-zeros: beyond a single cusolverSp factorisation"}
     direct["krylov_ms_per_solve"] = solve_ms / max(solve_launches, 1)
 
+    # the preconditioner as built by the solves (two-level stands down to block-Jacobi when it cannot help)
+    pc_eff, n_coarse, refreshes = s.preconditioner()
+    sched["precond_effective"] = {0: "block_jacobi", 1: "ilu0", 2: "two_level"}.get(pc_eff, pc_eff)
+    sched["coarse_unknowns"] = n_coarse
+    sched["coarse_refreshes"] = refreshes
+
     # kernel timings for the roofline
     ms_el, ms_spmv = s.time_kernels(20)
     nnzb = int(s.pattern()[1].shape[0])
@@ -310,6 +316,12 @@ def run_b200(args) -> None:
     # x/r: x,phat,shat,s,t,rhat -> x,r); plus one setup pass (diagonal inverses, r, rhat, p, v)
     per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 72 + 4 * 24 + 72 + 8 * 24)
     per_setup = N * (72.0 + 72 + 24 + 4 * 24)
+    if args.precond == "two_level" and sched.get("coarse_unknowns", 0) > 0:
+        # two applications of the coarse correction per iteration, each reading the node modes
+        # (d_i, mask) in the restriction and the prolongation and updating the preconditioned
+        # vector once more; the coarse inverse is read once per solve into shared memory
+        per_iter += 2.0 * N * (25 + 25 + 48)
+        per_setup += 8.0 * sched["coarse_unknowns"] ** 2
     if solve_launches > 0:
         bytes_solve = (kry * per_iter + solve_launches * per_setup) / solve_launches
         r_solve = roof("bicgstab_persistent", bytes_solve, solve_ms / solve_launches)

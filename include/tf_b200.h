@@ -220,6 +220,12 @@ int tf_time_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x
 /* Number of element colours and the chosen scatter / teams-per-CTA after autotuning. */
 int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* elems_per_block);
 
+/* The preconditioner the context actually uses (TF_PRECOND_TWO_LEVEL stands down to
+ * TF_PRECOND_BLOCK_JACOBI for batches and the non-persistent path), the number of coarse
+ * unknowns of the two-level space (0 until the first solve, and 0 when the tissue's aggregates
+ * would be too large to help), and how many times the coarse operator has been refactorised. */
+int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes);
+
 /* Time the assembly variants on the context's current state and keep the fastest
  * (scatter mode x teams per CTA). Returns the chosen pair through tf_get_schedule. */
 int tf_autotune(tf_ctx* ctx, const double* x_n, double dt);

@@ -37,6 +37,8 @@ def test_batch_matches_single_tissue_runs():
             singles.append(x)
             its_single.append(its)
     with BatchSolver(ts, krylov_rtol=1e-14) as b:
+        # the default two-level preconditioner stands down to block-Jacobi in a batch
+        assert b.preconditioner()[0] == capi.TF_PRECOND_BLOCK_JACOBI
         x = b.join([t.x for t in ts])
         its_batch = [[] for _ in ts]
         for _ in range(n_steps):

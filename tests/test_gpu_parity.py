@@ -257,6 +257,10 @@ def test_two_level_solve_matches_direct_with_fewer_iterations():
     for pc in (capi.TF_PRECOND_BLOCK_JACOBI, capi.TF_PRECOND_TWO_LEVEL):
         with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, precond=pc) as s:
             du, rc, it, rr = s.solveForDeltaU(vals, g)
+            pc_eff, n_coarse, refreshes = s.preconditioner()
+        assert pc_eff == pc
+        if pc == capi.TF_PRECOND_TWO_LEVEL:
+            assert n_coarse > 0 and refreshes == 1
         assert rc == capi.TF_OK and rr <= 1e-13
         assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
         assert np.all(du[fixed] == 0.0)

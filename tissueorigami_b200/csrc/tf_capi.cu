@@ -92,6 +92,7 @@ struct tf_ctx {
     DevBuf node_d, node_mask, agg_m;
     int coarse_age = 0, coarse_base_iters = 0;  // solves since the last coarse refresh; iterations of the first
     int last_solve_iters = 0;
+    int32_t coarse_refreshes = 0;
     DevBuf ca_agg_slot_ptr, ca_slot_agg, ca_slot_ptr, ca_blk, ca_blk_row, ca_empty;
     cusolverDnHandle_t dn = nullptr;
     int32_t* h_coarse_info = nullptr;  // pinned
@@ -903,6 +904,7 @@ int krylov_solve(tf_ctx* ctx) {
                 const int crc = coarse_setup(ctx);
                 if (crc != TF_OK) return crc;
                 ctx->coarse_age = 0;
+                ++ctx->coarse_refreshes;
             }
         }
         const BatchPlan plan = make_plan(ctx);
@@ -1621,6 +1623,14 @@ int tf_time_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x
 
 int tf_time_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out, tf_step_stats* stats) {
     return step_entry(ctx, x_n, dt, x_out, stats, true, true);
+}
+
+int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes) {
+    if (!ctx) return TF_ERR_ARGUMENT;
+    if (precond) *precond = ctx->params.precond;
+    if (n_coarse) *n_coarse = ctx->coarse_m > 0 ? ctx->n_coarse : 0;
+    if (coarse_refreshes) *coarse_refreshes = ctx->coarse_refreshes;
+    return TF_OK;
 }
 
 int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* elems_per_block) {

@@ -185,6 +185,16 @@ class NewtonRaphsonSolver:
         self._L.tf_get_schedule(self._h, ctypes.byref(nc), ctypes.byref(sc), ctypes.byref(t))
         return {"n_colours": nc.value, "scatter": sc.value, "elems_per_block": t.value}
 
+    def preconditioner(self):
+        """(effective preconditioner, coarse unknowns, coarse refactorisations so far)."""
+        pc, nc, rf = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        capi.check(self._L.tf_get_preconditioner(self._h, ctypes.byref(pc), ctypes.byref(nc), ctypes.byref(rf)),
+                   "tf_get_preconditioner", self._h)
+        return pc.value, nc.value, rf.value
+
+    def coarse_unknowns(self) -> int:
+        return self.preconditioner()[1]
+
     def autotune(self, x_n, dt: float):
         capi.check(self._L.tf_autotune(self._h, capi.dptr(_f64(x_n).reshape(-1)), float(dt)), "tf_autotune", self._h)
         return self.schedule()
