@@ -12,6 +12,11 @@
  * (ShapeBase.cpp:3154-3160, 3193-3199), the dense Jacobian and its 1e-13 drop
  * (NewtonRaphsonSolver.cpp:766-787) and the transposed solve (iparm[11]=1, :716-723).
  * GSL is replaced by plain loops; the sums run in the same index order as GSL's dgemm.
+ *
+ * Pinning: the growth prologue (tfo_grow) reproduces the reference's own recorded growth
+ * tensors of its no-Pardiso regression run 07008 bit for bit (tests/test_golden_growth.py);
+ * the element, Jacobian and Newton-step functions have no reference output to pin against
+ * (parity unpinned there) and are checked by finite differences and internal consistency.
  */
 #include "tf_oracle.h"
 
