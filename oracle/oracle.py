@@ -3,8 +3,9 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
 ``cpu_baseline`` / ``--impl reference`` legs of bench.py. The product never imports this module.
 The oracle restates TissueOrigami's Newton-Raphson path in plain C++ (see tf_oracle.cpp for the
-reference file:line of every function). Its growth prologue is pinned to the reference's recorded
-output (tests/golden/run07008_growth.npz); the Newton step itself is parity unpinned.
+reference file:line of every function). It is pinned to the reference's recorded runs: the growth
+prologue (tests/golden/run07008_growth.npz) and the first Newton step of the Pardiso run 07008
+(tests/golden/run07008_newton_step1.npz).
 """
 from __future__ import annotations
 

@@ -13,10 +13,13 @@
  * (NewtonRaphsonSolver.cpp:766-787) and the transposed solve (iparm[11]=1, :716-723).
  * GSL is replaced by plain loops; the sums run in the same index order as GSL's dgemm.
  *
- * Pinning: the growth prologue (tfo_grow) reproduces the reference's own recorded growth
- * tensors of its no-Pardiso regression run 07008 bit for bit (tests/test_golden_growth.py);
- * the element, Jacobian and Newton-step functions have no reference output to pin against
- * (parity unpinned there) and are checked by finite differences and internal consistency.
+ * Pinning: against the reference's own recorded regression runs. The growth prologue
+ * (tfo_grow) reproduces the growth tensors of the no-Pardiso run 07008 bit for bit
+ * (tests/test_golden_growth.py); the Newton step (element forces and tangents, drag, fixed and
+ * bound DoFs, Newton loop) reproduces the first step of the Pardiso run 07008 - positions to the
+ * recording's 10 digits, the ||dU|| trace to its printed digits (tests/test_golden_newton.py).
+ * The viscous (eta != 0) terms, which those runs do not exercise, are checked by finite
+ * differences.
  */
 #include "tf_oracle.h"
 
