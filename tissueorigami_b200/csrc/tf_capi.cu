@@ -29,7 +29,7 @@ using namespace tfb;
 namespace {
 
 constexpr int kChunk = 32;  // BiCGStab iterations per graph replay / status poll
-constexpr int kCoarseMaxAge = 16;  // solves between refreshes of the two-level coarse operator
+constexpr int kCoarseMaxAge = 64;  // solves between refreshes of the two-level coarse operator
 constexpr int kMaxAggNodes = 2048;  // largest useful two-level aggregate (nodes)
 
 struct DevBuf {
@@ -864,7 +864,7 @@ int coarse_setup(tf_ctx* ctx) {
     int32_t* ipiv = dptr<int32_t>(ctx->coarse_ipiv);
     int32_t* info = dptr<int32_t>(ctx->coarse_info);
     TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), A, ctx->stream));
-    ctx->launches += 2;
+    ctx->launches += 1 + (ca.n_empty > 0 ? 1 : 0);  // this library's kernels only (not cuSOLVER's)
     if (cusolverDnDgetrf(ctx->dn, nc, nc, A, nc, dptr<double>(ctx->coarse_work), ipiv, info) != CUSOLVER_STATUS_SUCCESS)
         return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrf");
     TF_CK(cudaMemcpyAsync(ctx->h_coarse_info, info, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -874,7 +874,7 @@ int coarse_setup(tf_ctx* ctx) {
     TF_CK(launch_set_identity(inv, nc, ctx->stream));
     if (cusolverDnDgetrs(ctx->dn, CUBLAS_OP_T, nc, nc, A, nc, ipiv, inv, nc, info) != CUSOLVER_STATUS_SUCCESS)
         return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrs");
-    ctx->launches += 1;
+    ctx->launches += 1;  // k_set_identity
     ctx->coarse_ok = true;
     return TF_OK;
 }
