@@ -23,8 +23,8 @@ The fixture keeps the step-1 inputs and the recorded step-1 results:
   * fixed DoFs: y of every node with |y| < 0.1 (setupYsymmetricity, Simulation.cpp:9557-9567);
   * the binding pairs. Save_NodeBinding leaves out pairs whose master is node 0 (its writer keeps
     slaveTo[i] > 0, Simulation.cpp:8553), although the run binds node 0's column like every other
-    circumference column (the recorded x of nodes 0, 36, 72, 108 coincide); those pairs - x and y
-    of the nodes above node 0 - are restored here;
+    circumference column (the recorded x of nodes 0, 36, 72, 108 coincide); those pairs - x of the
+    nodes above node 0; their y is fixed like node 0's - are restored here;
   * exposed surfaces: basal face of the elements whose three basal nodes are basal, apical face
     of those whose three apical nodes are apical;
   * growth as in the no-Pardiso fixture (single-precision rates and angle, columnar elements);
@@ -94,12 +94,19 @@ def main():
     tok = open(os.path.join(OUT, "Save_NodeBinding")).read().split()
     nb = int(tok[0])
     pairs = [tuple(map(int, tok[1 + 2 * k:3 + 2 * k])) for k in range(nb)]
-    # restore the bindings whose master is node 0 (left out of the file by its writer)
-    col0 = [k for k in range(N) if k != 0 and np.allclose(x[k, :2], x[0, :2])]
-    pairs += [(3 * k + d, d) for k in col0 for d in (0, 1)]
-    pairs = np.array(sorted(pairs), np.int32)
     fixed = np.zeros((N, 3), np.uint8)
     fixed[np.abs(x[:, 1]) < 0.1, 1] = 1
+    # restore the bindings whose master is node 0 (left out of the file by its writer): x and y of
+    # the nodes above node 0, except where the master is fixed - then the reference fixes the
+    # slave instead of binding it (bindCircumferenceXY, Simulation.cpp:1382-1396)
+    col0 = [k for k in range(N) if k != 0 and np.allclose(x[k, :2], x[0, :2])]
+    for k in col0:
+        for d in (0, 1):
+            if fixed[0, d]:
+                fixed[k, d] = 1
+            else:
+                pairs.append((3 * k + d, d))
+    pairs = np.array(sorted(pairs), np.int32)
     exposed = np.zeros(E, np.uint8)
     for e in range(E):
         if (place[conn[e, :3]] == 0).all():
@@ -114,7 +121,7 @@ def main():
     np.savez_compressed(out, x=x, place=place, circ=circ, conn=conn, xref=xref, young=elem[:, 0], eta=elem[:, 1],
                         ecm=ecm, ext_visc=ext_visc, pairs=pairs, fixed=fixed, exposed=exposed, grown=g["grown"],
                         rates=g["rates"], angle=g["angle"], dt=g["dt"], x_step1=frames[0][1], du_trace=np.array(trace))
-    print(f"wrote {out}: {N} nodes, {E} prisms, {len(pairs)} binding pairs ({len(col0) * 2} restored), "
+    print(f"wrote {out}: {N} nodes, {E} prisms, {len(pairs)} binding pairs ({len(col0)} restored), "
           f"{int(ecm.sum())} ECM prisms, step-1 trace {trace}")
 
 
