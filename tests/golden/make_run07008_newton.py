@@ -28,7 +28,8 @@ The fixture keeps the step-1 inputs and the recorded step-1 results:
   * exposed surfaces: basal face of the elements whose three basal nodes are basal, apical face
     of those whose three apical nodes are apical;
   * growth as in the no-Pardiso fixture (single-precision rates and angle, columnar elements);
-  * the recorded positions after step 1 and the recorded ||dU|| trace of step 1.
+  * the recorded positions after step 1 and the recorded ||dU|| trace of step 1;
+  * the model input file's tokens (for the test of tissueorigami_b200.modelinput).
 
 Run from the repository root with the reference at REFERENCE_ROOT (default /root/reference):
     python tests/golden/make_run07008_newton.py
@@ -118,7 +119,10 @@ def main():
     assert frames[0][0] == 3600.0
     trace = _du_traces(os.path.join(OUT, "tmp"))[0]
     out = os.path.join(HERE, "run07008_newton_step1.npz")
-    np.savez_compressed(out, x=x, place=place, circ=circ, conn=conn, xref=xref, young=elem[:, 0], eta=elem[:, 1],
+    # the model input itself, as whitespace-separated tokens, for the model-input loader's test
+    tokens = np.array(open(os.path.join(INP, "modelinput07008")).read().split())
+    np.savez_compressed(out, x=x, place=place, ttype=ttype, circ=circ, conn=conn, xref=xref, young=elem[:, 0], eta=elem[:, 1],
+                        modelinput_tokens=tokens,
                         ecm=ecm, ext_visc=ext_visc, pairs=pairs, fixed=fixed, exposed=exposed, grown=g["grown"],
                         rates=g["rates"], angle=g["angle"], dt=g["dt"], x_step1=frames[0][1], du_trace=np.array(trace))
     print(f"wrote {out}: {N} nodes, {E} prisms, {len(pairs)} binding pairs ({len(col0)} restored), "
