@@ -29,7 +29,8 @@ The fixture keeps the step-1 inputs and the recorded step-1 results:
     of those whose three apical nodes are apical;
   * growth as in the no-Pardiso fixture (single-precision rates and angle, columnar elements);
   * the recorded positions after step 1 and the recorded ||dU|| trace of step 1;
-  * the model input file's tokens (for the test of tissueorigami_b200.modelinput).
+  * the model input file's tokens (for the test of tissueorigami_b200.modelinput) and the first
+    Save_Frame block verbatim (for the test of the Save_Frame writer).
 
 Run from the repository root with the reference at REFERENCE_ROOT (default /root/reference):
     python tests/golden/make_run07008_newton.py
@@ -121,8 +122,12 @@ def main():
     out = os.path.join(HERE, "run07008_newton_step1.npz")
     # the model input itself, as whitespace-separated tokens, for the model-input loader's test
     tokens = np.array(open(os.path.join(INP, "modelinput07008")).read().split())
+    # the first Save_Frame block verbatim, to check that this library writes the same format
+    lines = open(os.path.join(OUT, "Save_Frame")).read().splitlines(keepends=True)
+    end = next(i for i, l in enumerate(lines) if l.startswith("=============== END OF TIME:"))
+    frame_text = "".join(lines[:end + 1])
     np.savez_compressed(out, x=x, place=place, ttype=ttype, circ=circ, conn=conn, xref=xref, young=elem[:, 0], eta=elem[:, 1],
-                        modelinput_tokens=tokens,
+                        modelinput_tokens=tokens, frame_text=np.array(frame_text),
                         ecm=ecm, ext_visc=ext_visc, pairs=pairs, fixed=fixed, exposed=exposed, grown=g["grown"],
                         rates=g["rates"], angle=g["angle"], dt=g["dt"], x_step1=frames[0][1], du_trace=np.array(trace))
     print(f"wrote {out}: {N} nodes, {E} prisms, {len(pairs)} binding pairs ({len(col0)} restored), "

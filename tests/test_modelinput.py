@@ -74,3 +74,32 @@ def test_loaded_input_gives_the_recorded_first_step_on_the_gpu():
     assert stats[0]["rc"] == 0
     assert np.abs(xs[0] - z["x_step1"]).max() <= 1e-8
     assert stats[0]["newton_iters"] == len(z["du_trace"])
+
+
+def test_save_frame_writer_reproduces_the_reference_file():
+    """Writing the recorded first frame back gives the reference's Save_Frame text byte for byte."""
+    from tissueorigami_b200 import mesh
+
+    st, z = _load()
+    text = str(z["frame_text"])
+    (time_s, x, flags, conn), = mesh.read_save_frame(text, is_text=True)
+    assert time_s == 3600.0
+    np.testing.assert_array_equal(conn, z["conn"])
+    np.testing.assert_array_equal(x, z["x_step1"])
+    block = mesh.save_frame_block(time_s, x, flags[:, 0], flags[:, 1], flags[:, 2], conn, z["xref"])
+    assert block == text
+
+
+def test_save_frame_round_trip(tmp_path):
+    from tissueorigami_b200 import mesh
+
+    st, z = _load()
+    t = st.tissue
+    p = tmp_path / "Save_Frame"
+    frames = [(3600.0, z["x_step1"]), (7200.0, z["x_step1"] + 1e-3)]
+    mesh.write_save_frame(str(p), frames, t)
+    back = mesh.read_save_frame(str(p))
+    assert [f[0] for f in back] == [3600.0, 7200.0]
+    for (tm, x), (tb, xb, flags, conn) in zip(frames, back):
+        assert np.abs(xb - x).max() <= 1e-9 * np.abs(x).max()  # 10 significant digits
+        np.testing.assert_array_equal(flags[:, 2], t.at_circumference)

@@ -469,3 +469,60 @@ def read_mesh(path: str):
         xref[e] = [float(v) for v in tok[p + 7:p + 25]]
         p += 25
     return x, place, ttype, circ, conn, xref
+
+
+def _g(v: float, precision: int, width: int) -> str:
+    """A value as a C++ ostream in its default float format prints it with the given precision
+    and field width (the %g rules: shortest of fixed / scientific, no trailing zeros)."""
+    return f"{float(v):>{width}.{precision}g}"
+
+
+def save_frame_block(time_s: float, x, node_placement, tissue_type, at_circumference, conn, xref) -> str:
+    """One time block of the reference's ``Save_Frame`` text format (Simulation::writeSaveFileStepHeader,
+    writeNodes, writeElements, writeSaveFileStepFooter; Simulation.cpp:8445-8520): header with the
+    time, the node count, each node's position (precision 10, width 20) with its placement,
+    tissue type and circumference flag (width 4), the element count, each prism's shape type,
+    ablation flag, node ids (width 9) and reference positions (precision 4, width 15), footer."""
+    x = np.asarray(x, np.float64).reshape(-1, 3)
+    conn = np.asarray(conn).reshape(-1, 6)
+    xref = np.asarray(xref, np.float64).reshape(-1, 18)
+    out = [f"=============== TIME: {_g(time_s, 6, 10)}===================================================\n",
+           f"{x.shape[0]}\n"]
+    for i in range(x.shape[0]):
+        out.append("".join(_g(v, 10, 20) for v in x[i]) + f"{int(node_placement[i]):>4d}{int(tissue_type[i]):>4d}"
+                   f"{int(at_circumference[i]):>4d}\n")
+    out.append(f"{conn.shape[0]}\n")
+    for e in range(conn.shape[0]):
+        out.append(f"{1:>4d}{0:>4d}" + "".join(f"{int(v):>9d}" for v in conn[e]) + "".join(_g(v, 4, 15) for v in xref[e]) + "\n")
+    out.append(f"=============== END OF TIME: {_g(time_s, 6, 10)}============================================\n")
+    return "".join(out)
+
+
+def write_save_frame(path: str, frames, t: "Tissue", tissue_type=None) -> None:
+    """Write ``frames`` [(time in s, positions [N,3]), ...] as a reference ``Save_Frame`` file."""
+    ttype = np.zeros(t.n_nodes, np.int32) if tissue_type is None else tissue_type
+    with open(path, "w") as fh:
+        for time_s, x in frames:
+            fh.write(save_frame_block(time_s, x, t.node_placement, ttype, t.at_circumference, t.conn, t.xref))
+
+
+def read_save_frame(path_or_text: str, is_text: bool = False):
+    """Read a reference ``Save_Frame`` file: [(time in s, positions [N,3], node flags [N,3],
+    conn [E,6]), ...] with the flags (placement, tissue type, circumference) of every frame."""
+    text = path_or_text if is_text else open(path_or_text).read()
+    lines = text.splitlines()
+    frames, i = [], 0
+    while i < len(lines):
+        if lines[i].startswith("=============== TIME:"):
+            time_s = float(lines[i].split(":", 1)[1].split("=")[0])
+            n = int(lines[i + 1])
+            rows = [lines[i + 2 + k].split() for k in range(n)]
+            x = np.array([[float(v) for v in r[:3]] for r in rows])
+            flags = np.array([[int(v) for v in r[3:6]] for r in rows], np.int32)
+            m = int(lines[i + 2 + n])
+            conn = np.array([[int(v) for v in lines[i + 3 + n + e].split()[2:8]] for e in range(m)], np.int32)
+            frames.append((time_s, x, flags, conn))
+            i += 3 + n + m
+        else:
+            i += 1
+    return frames
