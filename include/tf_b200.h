@@ -252,7 +252,8 @@ int tf_adjoint_forward(tf_ctx* ctx, const double* x0, int32_t n_steps, double dt
 int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drates, double* dL_dx0,
                         tf_step_stats* stats);
 
-/* Text of the last error recorded on the context (no reference counterpart). */
+/* Text of the last error recorded on the context (no reference counterpart); with ctx = NULL,
+ * the reason the calling thread's last tf_create / tf_batch_create failed. */
 const char* tf_last_error(tf_ctx* ctx);
 
 /* No counterpart in the reference. The linear solve of tf_solve (block-Jacobi BiCGStab on

@@ -185,8 +185,8 @@ def check(code, where, ctx=None):
     """Raise on errors (< 0); pass numerical outcomes (>= 0) back to the caller."""
     if code < 0:
         detail = ""
-        if ctx:
-            msg = load().tf_last_error(ctx)
+        if ctx or where in ("tf_create", "tf_batch_create"):
+            msg = load().tf_last_error(ctx if ctx else None)
             detail = msg.decode() if msg else ""
         raise TFError(code, where, detail)
     return code

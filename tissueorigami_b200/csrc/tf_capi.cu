@@ -75,8 +75,9 @@ struct tf_ctx {
     // [tissue_elem0[t], tissue_elem0[t+1]); a single tissue is T = 1.
     int32_t T = 1;
     std::vector<int32_t> tissue_node0, tissue_elem0;
-    std::vector<int32_t> plan_cta_tissue, plan_cta0, plan_ncta;
-    DevBuf node_tissue_d, plan_cta_tissue_d, plan_cta0_d, plan_ncta_d, plan_row0_d, active_d, tbarriers, tscalars, tdu2;
+    std::vector<int32_t> plan_list_ptr, plan_list, plan_cta0, plan_ncta;
+    DevBuf node_tissue_d, plan_list_ptr_d, plan_list_d, plan_cta0_d, plan_ncta_d, plan_row0_d, active_d, tbarriers, tscalars,
+        tdu2;
     int32_t* h_active = nullptr;     // pinned [T]
     double* h_du2 = nullptr;         // pinned [T]
     KrylovScalars* h_tsc = nullptr;  // pinned [T]
@@ -127,8 +128,17 @@ struct tf_ctx {
 
 namespace {
 
+// The message of the last failed tf_create / tf_batch_create on this thread (the context itself
+// is gone by then); tf_last_error(NULL) returns it.
+thread_local char g_create_error[256] = {0};
+
 int set_error(tf_ctx* c, int code, const char* msg) {
     if (c) std::snprintf(c->last_error, sizeof(c->last_error), "%s", msg);
+    return code;
+}
+
+int set_error(tf_ctx* c, int code, const char* msg, const char* where) {
+    if (c) std::snprintf(c->last_error, sizeof(c->last_error), "%s (%s)", msg, where);
     return code;
 }
 
@@ -138,7 +148,7 @@ int set_error(tf_ctx* c, int code, const char* msg) {
         if (err__ != cudaSuccess) {                                                   \
             cudaGetLastError();                                                       \
             return set_error(ctx, err__ == cudaErrorMemoryAllocation ? TF_ERR_OUT_OF_MEMORY : TF_ERR_CUDA, \
-                             cudaGetErrorString(err__));                              \
+                             cudaGetErrorString(err__), #call);                       \
         }                                                                             \
     } while (0)
 
@@ -515,11 +525,14 @@ AssembleArgs make_assemble(tf_ctx* c, double dt) {
     return a;
 }
 
-// CTA plan of the persistent solve. Every active tissue gets at least one CTA; the rest of the
-// cooperative grid is shared in proportion to weight[t] (expected work: rows x BiCGStab
-// iterations), keeping at least 64 rows per CTA. Inactive tissues get none. The plan is rebuilt
-// every Newton round of a batch, so that the tissues still iterating take over the CTAs of the
-// converged ones and the largest solves get the most CTAs.
+// CTA plan of the persistent solve. A tissue's expected work is weight[t] (rows x BiCGStab
+// iterations); with W the active total and C the co-resident CTAs, a tissue whose work is at least
+// one CTA's share q = W / C gets a group of about weight / q CTAs (at least 64 rows each) and runs
+// with group barriers; the smaller tissues are packed into the remaining CTAs by longest-first bin
+// packing and each packing CTA solves its tissues one after another (CTA-level barriers only).
+// The slowest tissues thereby get the most CTAs instead of every small tissue holding one for the
+// whole launch. Inactive tissues get none. The plan is rebuilt every Newton round of a batch with
+// the last Krylov iteration counts as weights.
 int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* active) {
     const int T = ctx->T;
     const int cmax = std::max(ctx->persistent_grid_max, 1);
@@ -533,37 +546,100 @@ int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* ac
             ++n_act;
         }
     }
-    std::vector<int32_t> n(T, 0);
-    if (ctx->persistent_grid_max > 0) {
-        if (n_act > cmax) return set_error(ctx, TF_ERR_UNSUPPORTED, "more active tissues than co-resident CTAs");
-        const int spare = cmax - n_act;
-        int used = 0;
+    std::vector<int32_t> n(T, 0);                 // CTAs of a group tissue (0: packed or inactive)
+    std::vector<std::vector<int32_t>> lists;      // tissues of every CTA
+    if (ctx->persistent_grid_max > 0 && n_act > 0) {
+        const double q = wsum / cmax;
+        std::vector<int> small;
+        int group_ctas = 0;
         for (int t = 0; t < T; ++t) {
             if (!active[t]) continue;
             const int64_t cap = std::max<int64_t>(1, (rows[t] + 63) / 64);
-            const int64_t want = 1 + (wsum > 0 ? (int64_t)((double)spare * weight[t] / wsum) : 0);
-            n[t] = (int32_t)std::min(want, cap);
-            used += n[t];
+            const int64_t want = q > 0 ? (int64_t)(weight[t] / q) : 1;
+            if (want >= 2 && cap >= 2) {
+                n[t] = (int32_t)std::min(want, cap);
+                group_ctas += n[t];
+            } else {
+                small.push_back(t);
+            }
         }
-        (void)used;
+        double small_w = 0.0;
+        for (int t : small) small_w += weight[t];
+        int bins = small.empty() ? 0 : std::max(1, (int)std::ceil(small_w / std::max(q, 1e-300) - 1e-9));
+        bins = std::min<int>(bins, (int)small.size());
+        // the groups shrink in proportion if groups and bins together exceed the grid
+        if (group_ctas + bins > cmax && group_ctas > 0) {
+            const double f = (double)(cmax - bins) / group_ctas;
+            group_ctas = 0;
+            for (int t = 0; t < T; ++t)
+                if (n[t] > 0) {
+                    n[t] = std::max(2, (int)(n[t] * f));
+                    group_ctas += n[t];
+                }
+            while (group_ctas + bins > cmax) {  // still over: take CTAs from the largest groups
+                int tm = -1;
+                for (int t = 0; t < T; ++t)
+                    if (n[t] > 2 && (tm < 0 || n[t] > n[tm])) tm = t;
+                if (tm < 0) break;
+                --n[tm];
+                --group_ctas;
+            }
+            if (group_ctas + bins > cmax)
+                return set_error(ctx, TF_ERR_UNSUPPORTED, "tissues do not fit the co-resident CTAs");
+        }
+        for (int t = 0; t < T; ++t) {
+            ctx->plan_cta0.resize(T);
+            if (n[t] > 0) {
+                ctx->plan_cta0[t] = (int32_t)lists.size();
+                for (int k = 0; k < n[t]; ++k) lists.push_back({t});
+            }
+        }
+        if (bins > 0) {
+            std::sort(small.begin(), small.end(), [&](int a, int b) { return weight[a] > weight[b] || (weight[a] == weight[b] && a < b); });
+            const int base = (int)lists.size();
+            std::vector<double> load(bins, 0.0);
+            lists.resize(base + bins);
+            for (int t : small) {
+                int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+                lists[base + k].push_back(t);
+                load[k] += weight[t];
+                ctx->plan_cta0[t] = base + k;
+                n[t] = 1;
+            }
+        }
     } else {
-        for (int t = 0; t < T; ++t) n[t] = active[t] ? 1 : 0;
+        for (int t = 0; t < T; ++t)
+            if (active[t]) {
+                n[t] = 1;
+                lists.push_back({t});
+            }
     }
-    ctx->plan_cta0.assign(T, 0);
+    ctx->plan_cta0.resize(T, 0);
+    if (ctx->persistent_grid_max == 0)
+        for (int t = 0, k = 0; t < T; ++t)
+            if (active[t]) ctx->plan_cta0[t] = k++;
     ctx->plan_ncta = n;
-    ctx->plan_cta_tissue.clear();
-    for (int t = 0; t < T; ++t) {
-        ctx->plan_cta0[t] = (int32_t)ctx->plan_cta_tissue.size();
-        for (int k = 0; k < n[t]; ++k) ctx->plan_cta_tissue.push_back(t);
+    ctx->plan_list_ptr.assign(1, 0);
+    ctx->plan_list.clear();
+    for (auto& l : lists) {
+        for (int32_t t : l) ctx->plan_list.push_back(t);
+        ctx->plan_list_ptr.push_back((int32_t)ctx->plan_list.size());
     }
-    const size_t C = std::max<size_t>(1, ctx->plan_cta_tissue.size());
-    if (ctx->plan_cta_tissue.empty()) ctx->plan_cta_tissue.push_back(0);  // keeps a valid launch shape
-    TF_CK(dalloc(ctx->plan_cta_tissue_d, sizeof(int32_t) * (size_t)cmax));
+    if (lists.empty()) {  // keeps a valid launch shape: one CTA with nothing to do
+        ctx->plan_list_ptr.push_back(0);
+    }
+    const size_t C = ctx->plan_list_ptr.size() - 1;
+    TF_CK(dalloc(ctx->plan_list_ptr_d, sizeof(int32_t) * ((size_t)cmax + 2)));
+    // every CTA of a group lists its tissue once; a packed tissue appears once in its bin
+    TF_CK(dalloc(ctx->plan_list_d, sizeof(int32_t) * ((size_t)cmax + T + 1)));
     TF_CK(dalloc(ctx->plan_cta0_d, sizeof(int32_t) * T));
     TF_CK(dalloc(ctx->plan_ncta_d, sizeof(int32_t) * T));
     TF_CK(dalloc(ctx->plan_row0_d, sizeof(int32_t) * (T + 1)));
-    TF_CK(cudaMemcpyAsync(ctx->plan_cta_tissue_d.p, ctx->plan_cta_tissue.data(), sizeof(int32_t) * C,
+    TF_CK(cudaMemcpyAsync(ctx->plan_list_ptr_d.p, ctx->plan_list_ptr.data(), sizeof(int32_t) * (C + 1),
                           cudaMemcpyHostToDevice, ctx->stream));
+    if (!ctx->plan_list.empty())
+        TF_CK(cudaMemcpyAsync(ctx->plan_list_d.p, ctx->plan_list.data(), sizeof(int32_t) * ctx->plan_list.size(),
+                              cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemcpyAsync(ctx->plan_cta0_d.p, ctx->plan_cta0.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemcpyAsync(ctx->plan_ncta_d.p, ctx->plan_ncta.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemcpyAsync(ctx->plan_row0_d.p, ctx->tissue_node0.data(), sizeof(int32_t) * (T + 1), cudaMemcpyHostToDevice,
@@ -600,8 +676,9 @@ BatchPlan make_plan(tf_ctx* c) {
     p.coarse_inv = dptr<double>(c->coarse_inv);
     p.coarse_r = dptr<double>(c->coarse_r);
     p.n_tissues = c->T;
-    p.n_cta = (int32_t)c->plan_cta_tissue.size();
-    p.cta_tissue = dptr<int32_t>(c->plan_cta_tissue_d);
+    p.n_cta = (int32_t)c->plan_list_ptr.size() - 1;
+    p.cta_list_ptr = dptr<int32_t>(c->plan_list_ptr_d);
+    p.cta_list = dptr<int32_t>(c->plan_list_d);
     p.cta0 = dptr<int32_t>(c->plan_cta0_d);
     p.ncta = dptr<int32_t>(c->plan_ncta_d);
     p.row0 = dptr<int32_t>(c->plan_row0_d);
@@ -1213,6 +1290,14 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
                 if (v < node0[t] || v >= node0[t + 1]) return TF_ERR_ARGUMENT;
             }
     std::unique_ptr<tf_ctx, CtxDeleter> holder(new (std::nothrow) tf_ctx());
+    // on failure, keep the context's last message for tf_last_error(NULL) before it is destroyed
+    struct KeepMessage {
+        std::unique_ptr<tf_ctx, CtxDeleter>& h;
+        ~KeepMessage() {
+            if (h) std::snprintf(g_create_error, sizeof(g_create_error), "%s", h->last_error);
+        }
+    } keep{holder};
+    g_create_error[0] = 0;
     tf_ctx* ctx = holder.get();
     if (!ctx) return TF_ERR_OUT_OF_MEMORY;
     ctx->T = T;
@@ -1382,7 +1467,7 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
                      &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier};
     for (DevBuf* b : all) dfree(*b);
-    DevBuf* batch[] = {&ctx->node_tissue_d, &ctx->plan_cta_tissue_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d,
+    DevBuf* batch[] = {&ctx->node_tissue_d, &ctx->plan_list_ptr_d, &ctx->plan_list_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d,
                        &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
     for (DevBuf* b : batch) dfree(*b);
     for (auto* v : {&ctx->cp_x, &ctx->cp_fg, &ctx->seg_x, &ctx->seg_fg})
@@ -1880,6 +1965,6 @@ int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drate
     return rc2 != TF_OK ? rc2 : st->status;
 }
 
-const char* tf_last_error(tf_ctx* ctx) { return ctx ? ctx->last_error : "null context"; }
+const char* tf_last_error(tf_ctx* ctx) { return ctx ? ctx->last_error : g_create_error; }
 
 }  // extern "C"

@@ -106,7 +106,8 @@ struct NodeArgs {
 struct BatchPlan {
     int32_t n_tissues;
     int32_t n_cta;
-    const int32_t* cta_tissue;   // [n_cta]
+    const int32_t* cta_list_ptr; // [n_cta+1] tissues of each CTA in cta_list: one for a CTA of a
+    const int32_t* cta_list;     //   multi-CTA group, several small tissues for a packing CTA
     const int32_t* cta0;         // [T]
     const int32_t* ncta;         // [T]
     const int32_t* row0;         // [T+1]

@@ -598,17 +598,13 @@ __device__ bool restart(const KrylovWork& w, int r0, int r1, double& rho, double
     return rho > 0.0 && isfinite(rho);
 }
 
-__global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
-                                                                      int max_iter) {
-    __shared__ double smem[32 * 2];
-    __shared__ double sb[2];
-    __shared__ double red[32 * 6];  // per-warp partial sums of the coarse steps
-    __shared__ double ys[kMaxAggPerCta * 6];
-    __shared__ double Ms[kMaxAggPerCta * 36];  // M_a of the CTA's aggregates
-    __shared__ double cs[kMaxCoarse];
-    extern __shared__ float cinv_s[];  // this CTA's 6m rows of the coarse inverse (FP32)
-    const int t = plan.cta_tissue[blockIdx.x];
-    if (!plan.active[t]) return;
+// The whole block-Jacobi (or two-level) BiCGStab solve of tissue t by this CTA, which is CTA lc of
+// the tissue's group (nct = 1: the tissue is one of several packed into this CTA, solved one after
+// another with CTA-level barriers only). Returns false when a group barrier timed out.
+__device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, double rtol, int max_iter,
+                             double* smem, double* sb, double* red, double* ys, double* Ms, double* cs,
+                             float* cinv_s) {
+    if (!plan.active[t]) return true;
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
     const int lc = blockIdx.x - c0;
     const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
@@ -641,7 +637,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
         }
     }
     write_partials<1>(v1, part[pb], lc, smem);
-    if (!group_barrier(bar, nct, w.dflags)) return;
+    if (!group_barrier(bar, nct, w.dflags)) return false;
     double t1[1], t2[2];
     sum_partials<1>(part[pb], nct, t1, smem, sb);
     pb ^= 1;
@@ -654,7 +650,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
         // A: p = r + beta (p - omega v); phat = M^-1 p
         const double beta = (rho / rho_prev) * (alpha / omega);
         if (plan.agg_per_cta > 0) {
-            if (!precond_phase<0>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms)) return;
+            if (!precond_phase<0>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
         } else {
             for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -665,13 +661,13 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 apply_dinv(w.dinv, n, w.p, w.phat);
             }
         }
-        if (!group_barrier(bar, nct, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
         spmv_rows<1>(w, r0, r1, w.phat, w.v, d0, d1);
         v1[0] = d0;
         write_partials<1>(v1, part[pb], lc, smem);
-        if (!group_barrier(bar, nct, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
         sum_partials<1>(part[pb], nct, t1, smem, sb);
         pb ^= 1;
         if (!isfinite(t1[0])) { status = KS_NONFINITE; break; }
@@ -686,7 +682,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
         alpha = rho / t1[0];
         // C: s = r - alpha v; shat = M^-1 s
         if (plan.agg_per_cta > 0) {
-            if (!precond_phase<1>(w, plan, lc, r0, r1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms)) return;
+            if (!precond_phase<1>(w, plan, lc, r0, r1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
         } else {
             for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -697,14 +693,14 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
                 apply_dinv(w.dinv, n, w.s, w.shat);
             }
         }
-        if (!group_barrier(bar, nct, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
         d1 = 0.0;
         spmv_rows<2>(w, r0, r1, w.shat, w.t, d0, d1);
         double v2[2] = {d0, d1};
         write_partials<2>(v2, part[pb], lc, smem);
-        if (!group_barrier(bar, nct, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
         sum_partials<2>(part[pb], nct, t2, smem, sb);
         pb ^= 1;
         if (!isfinite(t2[0]) || !isfinite(t2[1])) { status = KS_NONFINITE; break; }
@@ -724,7 +720,7 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
         }
         double v3[2] = {e0, e1};
         write_partials<2>(v3, part[pb], lc, smem);
-        if (!group_barrier(bar, nct, w.dflags)) return;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
         sum_partials<2>(part[pb], nct, t2, smem, sb);
         pb ^= 1;
         rho_prev = rho;
@@ -756,6 +752,22 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
         sc->max_iter = max_iter;
         sc->status = status;
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
+                                                                      int max_iter) {
+
+    __shared__ double smem[32 * 2];
+    __shared__ double sb[2];
+    __shared__ double red[32 * 6];  // per-warp partial sums of the coarse steps
+    __shared__ double ys[kMaxAggPerCta * 6];
+    __shared__ double Ms[kMaxAggPerCta * 36];  // M_a of the CTA's aggregates
+    __shared__ double cs[kMaxCoarse];
+    extern __shared__ float cinv_s[];  // this CTA's 6m rows of the coarse inverse (FP32)
+    // a CTA of a multi-CTA group has one tissue; a packing CTA solves its small tissues in turn
+    for (int j = plan.cta_list_ptr[blockIdx.x]; j < plan.cta_list_ptr[blockIdx.x + 1]; ++j)
+        if (!solve_tissue(w, plan, plan.cta_list[j], rtol, max_iter, smem, sb, red, ys, Ms, cs, cinv_s)) return;
 }
 
 // Newton update of a batch: du[slave] = du[master] first (separate kernel), then per CTA of
@@ -765,34 +777,38 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
 __global__ void k_newton_update_batched(KrylovWork w, BatchPlan plan, double* uk) {
     __shared__ double smem[32];
     __shared__ bool last;
-    const int t = plan.cta_tissue[blockIdx.x];
-    if (!plan.active[t]) return;
-    const int c0 = plan.cta0[t], nct = plan.ncta[t];
-    const int lc = blockIdx.x - c0;
-    const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
-    const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
-    const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
-    double v[1] = {0.0};
-    for (int d = r0 * 3 + threadIdx.x; d < r1 * 3; d += blockDim.x) {
-        const double du = w.x[d];
-        v[0] += du * du;
-        uk[d] = uk[d] + du;
+    for (int j = plan.cta_list_ptr[blockIdx.x]; j < plan.cta_list_ptr[blockIdx.x + 1]; ++j) {
+        const int t = plan.cta_list[j];
+        if (!plan.active[t]) continue;
+        const int c0 = plan.cta0[t], nct = plan.ncta[t];
+        const int lc = blockIdx.x - c0;
+        const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
+        const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
+        const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+        double v[1] = {0.0};
+        for (int d = r0 * 3 + threadIdx.x; d < r1 * 3; d += blockDim.x) {
+            const double du = w.x[d];
+            v[0] += du * du;
+            uk[d] = uk[d] + du;
+        }
+        block_sum<1>(v, smem);
+        double* part = w.partials + 4 * c0;
+        if (threadIdx.x == 0) {
+            part[lc] = v[0];
+            __threadfence();
+            const uint32_t k = atomicAdd(&plan.barriers[t].count, 1u);
+            last = (k == (uint32_t)nct - 1);
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            __threadfence();
+            double sum = 0.0;
+            for (int i = 0; i < nct; ++i) sum += __ldcg(part + i);
+            plan.du2[t] = sum;
+            plan.barriers[t].count = 0u;
+        }
+        __syncthreads();
     }
-    block_sum<1>(v, smem);
-    double* part = w.partials + 4 * c0;
-    if (threadIdx.x == 0) {
-        part[lc] = v[0];
-        __threadfence();
-        const uint32_t k = atomicAdd(&plan.barriers[t].count, 1u);
-        last = (k == (uint32_t)nct - 1);
-    }
-    __syncthreads();
-    if (!last || threadIdx.x != 0) return;
-    __threadfence();
-    double sum = 0.0;
-    for (int i = 0; i < nct; ++i) sum += __ldcg(part + i);
-    plan.du2[t] = sum;
-    plan.barriers[t].count = 0u;
 }
 
 // ---- multicolour block ILU(0) ---------------------------------------------------------------
