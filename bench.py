@@ -403,7 +403,9 @@ def run_batch(args) -> None:
     L = capi.load()
     ts = mesh.batch_tissues(n_tissues=args.n_tissues)
     E_all = float(sum(t.n_elems for t in ts))
-    sb = ShardedBatch(ts, rank, world, lambda tl: BatchSolver(tl, device=local))
+    pc = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0,
+          "two_level": capi.TF_PRECOND_TWO_LEVEL}[args.precond]
+    sb = ShardedBatch(ts, rank, world, lambda tl: BatchSolver(tl, device=local, precond=pc))
     b = sb.solver
     dev = f"cuda:{local}"
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
@@ -443,6 +445,7 @@ def run_batch(args) -> None:
     if dist:
         dist.barrier()
     clk = clocks.stop()
+    pc_info = b.preconditioner() if b is not None else (pc, 0, 0)
     sb.close()
     t_dev = ms / 1000.0
     if dist:
@@ -457,7 +460,7 @@ def run_batch(args) -> None:
         # sequential baseline: the same tissues one after another, one context each, same steps
         seq_ms, seq_units = 0.0, 0.0
         for t in ts:
-            with NewtonRaphsonSolver.from_tissue(t) as s:
+            with NewtonRaphsonSolver.from_tissue(t, precond=pc) as s:
                 xx = t.x.copy()
                 for _ in range(args.warmup):
                     xx, _, _ = s.runOneStep(xx, t.dt)
@@ -476,7 +479,10 @@ def run_batch(args) -> None:
                        "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": f"{world} rank(s), whole tissues per rank (greedy bin packing), "
                                       "no collective on the data path",
-                       "tissues_per_rank": [len(s_) for s_ in sb.shards]},
+                       "tissues_per_rank": [len(s_) for s_ in sb.shards],
+                       "precond": args.precond,
+                       "precond_effective": {0: "block_jacobi", 1: "ilu0", 2: "two_level"}.get(pc_info[0], pc_info[0]),
+                       "coarse_unknowns": pc_info[1], "coarse_refreshes": pc_info[2]},
             "tissue_steps_per_s": len(ts) * args.steps / t_dev,
             "gpu_launches": int(launches), "clocks": clk, "status_worst": int(worst),
         }

@@ -50,9 +50,9 @@ extern "C" {
 #define TF_PRECOND_BLOCK_JACOBI 0 /* 3x3 node-block inverse of the diagonal               */
 #define TF_PRECOND_ILU0 1         /* ILU(0) on the BSR3 pattern, multicolour ordered      */
 #define TF_PRECOND_TWO_LEVEL 2    /* default: block-Jacobi + additive coarse correction on  */
-                                  /* node-range aggregates with rigid-body modes; one       */
-                                  /* tissue with the persistent solve, elsewhere (batches,  */
-                                  /* persistent = 0) block-Jacobi is used instead           */
+                                  /* node-range aggregates with rigid-body modes, one coarse */
+                                  /* operator per tissue; needs the persistent solve (a one- */
+                                  /* tissue context with persistent = 0 uses block-Jacobi)  */
 
 #define TF_SCATTER_AUTO 0     /* pick by the autotuner's cached choice                   */
 #define TF_SCATTER_ATOMIC 1   /* FP64 atomics into the fixed BSR3 pattern                */
@@ -221,9 +221,10 @@ int tf_time_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x
 int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* elems_per_block);
 
 /* The preconditioner the context actually uses (TF_PRECOND_TWO_LEVEL stands down to
- * TF_PRECOND_BLOCK_JACOBI for batches and the non-persistent path), the number of coarse
- * unknowns of the two-level space (0 until the first solve, and 0 when the tissue's aggregates
- * would be too large to help), and how many times the coarse operator has been refactorised. */
+ * TF_PRECOND_BLOCK_JACOBI on the non-persistent path), the number of coarse unknowns of the
+ * two-level space summed over the tissues (0 until the first solve, and 0 when a single tissue's
+ * aggregates would be too large to help), and how many times the coarse operators have been
+ * refactorised. */
 int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes);
 
 /* Time the assembly variants on the context's current state and keep the fastest

@@ -22,7 +22,9 @@ def _tissues():
     return out
 
 
-def test_batch_matches_single_tissue_runs():
+@pytest.mark.parametrize("precond", ["two_level", "block_jacobi"])
+def test_batch_matches_single_tissue_runs(precond):
+    pc = {"two_level": capi.TF_PRECOND_TWO_LEVEL, "block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI}[precond]
     ts = _tissues()
     n_steps = 3
     singles, its_single = [], []
@@ -36,9 +38,8 @@ def test_batch_matches_single_tissue_runs():
                 its.append(st["newton_iters"])
             singles.append(x)
             its_single.append(its)
-    with BatchSolver(ts, krylov_rtol=1e-14) as b:
-        # the default two-level preconditioner stands down to block-Jacobi in a batch
-        assert b.preconditioner()[0] == capi.TF_PRECOND_BLOCK_JACOBI
+    with BatchSolver(ts, krylov_rtol=1e-14, precond=pc) as b:
+        assert b.preconditioner()[0] == pc
         x = b.join([t.x for t in ts])
         its_batch = [[] for _ in ts]
         for _ in range(n_steps):
@@ -49,14 +50,22 @@ def test_batch_matches_single_tissue_runs():
             for i in range(len(ts)):
                 its_batch[i].append(int(stats["newton_iters"][i]))
         xs = b.split(x)
+        pc_used, n_coarse, refreshes = b.preconditioner()
+        if pc == capi.TF_PRECOND_TWO_LEVEL:
+            # one coarse space per tissue: at least one aggregate (six modes) each
+            assert n_coarse >= 6 * len(ts) and refreshes >= 1
+        else:
+            assert n_coarse == 0
     assert its_batch == its_single
     for t, xb, xsng in zip(ts, xs, singles):
         assert np.abs(xb - xsng).max() <= 1e-9 * t.size
 
 
-def test_batch_tissue_matches_oracle():
+@pytest.mark.parametrize("precond", ["two_level", "block_jacobi"])
+def test_batch_tissue_matches_oracle(precond):
+    pc = {"two_level": capi.TF_PRECOND_TWO_LEVEL, "block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI}[precond]
     ts = _tissues()[:3]
-    with BatchSolver(ts, krylov_rtol=1e-14) as b:
+    with BatchSolver(ts, krylov_rtol=1e-14, precond=pc) as b:
         x = b.join([t.x for t in ts])
         for _ in range(2):
             x, rc, st = b.runOneStep(x, ts[0].dt)

@@ -8,6 +8,7 @@
 // Newton iteration. The linear solve runs as graph-replayed chunks of BiCGStab iterations
 // whose scalars never leave the device.
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -31,6 +32,7 @@ namespace {
 constexpr int kChunk = 32;  // BiCGStab iterations per graph replay / status poll
 constexpr int kCoarseMaxAge = 64;  // solves between refreshes of the two-level coarse operator
 constexpr int kMaxAggNodes = 2048;  // largest useful two-level aggregate (nodes)
+constexpr int kBatchAggNodes = 256;  // aggregate size of a batch tissue's two-level space
 
 struct DevBuf {
     void* p = nullptr;
@@ -97,6 +99,15 @@ struct tf_ctx {
     DevBuf ca_agg_slot_ptr, ca_slot_agg, ca_slot_ptr, ca_blk, ca_blk_row, ca_empty;
     cusolverDnHandle_t dn = nullptr;
     int32_t* h_coarse_info = nullptr;  // pinned
+    // two-level preconditioner of a batch: fixed aggregates per tissue, padded per-tissue coarse
+    // matrices (leading dimension bc_ld) inverted together by batched LU
+    bool bc_active = false;
+    int bc_ld = 0;
+    int64_t bc_n_unit = 0;
+    std::vector<int32_t> bc_tissue_agg0;
+    DevBuf bc_tissue_agg0_d, bc_agg_node0_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_ptr_a_d, bc_ptr_c_d, bc_info_d,
+        bc_piv_d;
+    cublasHandle_t cb = nullptr;
 
     // multicolour block ILU(0) (precond == TF_PRECOND_ILU0)
     std::vector<int32_t> ilu_colour_ptr;
@@ -554,7 +565,9 @@ int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* ac
         int group_ctas = 0;
         for (int t = 0; t < T; ++t) {
             if (!active[t]) continue;
-            const int64_t cap = std::max<int64_t>(1, (rows[t] + 63) / 64);
+            int64_t cap = std::max<int64_t>(1, (rows[t] + 63) / 64);
+            if (ctx->bc_active && (int)ctx->bc_tissue_agg0.size() == T + 1)  // every CTA owns whole aggregates
+                cap = std::min<int64_t>(cap, ctx->bc_tissue_agg0[t + 1] - ctx->bc_tissue_agg0[t]);
             const int64_t want = q > 0 ? (int64_t)(weight[t] / q) : 1;
             if (want >= 2 && cap >= 2) {
                 n[t] = (int32_t)std::min(want, cap);
@@ -675,6 +688,11 @@ BatchPlan make_plan(tf_ctx* c) {
     p.agg_m = dptr<double>(c->agg_m);
     p.coarse_inv = dptr<double>(c->coarse_inv);
     p.coarse_r = dptr<double>(c->coarse_r);
+    p.batch_coarse = (c->bc_active && c->coarse_ok) ? 1 : 0;
+    p.coarse_ld = c->bc_ld;
+    p.tissue_agg0 = dptr<int32_t>(c->bc_tissue_agg0_d);
+    p.agg_node0 = dptr<int32_t>(c->bc_agg_node0_d);
+    p.coarse_base = dptr<int64_t>(c->bc_base_d);
     p.n_tissues = c->T;
     p.n_cta = (int32_t)c->plan_list_ptr.size() - 1;
     p.cta_list_ptr = dptr<int32_t>(c->plan_list_ptr_d);
@@ -760,37 +778,19 @@ int krylov_status_to_tf(int ks) {
 // vanishes there (below 1e-10 of its initial norm) is dropped and its coarse unknown gets a
 // unit diagonal. The coarse operator P^T J P is assembled on the device every solve and
 // inverted explicitly (LU, cuSOLVER), so an application is a dense row-block product.
-int build_coarse(tf_ctx* ctx) {
-    ctx->coarse_dirty = false;
-    ctx->coarse_m = 0;
-    if (ctx->params.precond != TF_PRECOND_TWO_LEVEL || ctx->T != 1 || ctx->plan_ncta.empty()) return TF_OK;
-    const int N = ctx->N, nct = ctx->plan_ncta[0];
-    if (nct <= 0) return TF_OK;
-    int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
-    while (m > 1 && N / (nct * m) < 8) --m;
-    // each CTA's 6m rows of the n_coarse = 6 nct m inverse must fit its shared-memory block
-    while (m > 1 && (size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) --m;
-    if ((size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) return TF_OK;
-    // aggregates much larger than this no longer cut the iteration count (measured on the 2 M-node
-    // slab: 6,800-node aggregates left it unchanged); such tissues solve with block-Jacobi alone
-    if (N / (nct * m) > kMaxAggNodes) return TF_OK;
-    const int nw = ctx->persist_threads / 32;
-    while (m > 1 && nw / m < 1) --m;
-    const int n_agg = nct * m, nc = 6 * n_agg;
-    if (nc > kMaxCoarse) return TF_OK;  // plan too large for a staged coarse vector: block-Jacobi only
+// Modes (translations, rotations about the centroid in reference coordinates; fixed and slave
+// DoFs zeroed; two-pass modified Gram-Schmidt with the coefficient transform tracked; a mode
+// below 1e-6 of its initial norm dropped and listed in `empty`) of the aggregates with node
+// boundaries agg0, the per-aggregate block lists of the coarse assembly, all uploaded.
+int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg0, std::vector<int32_t>& empty) {
+    const int N = ctx->N, n_agg = (int)agg0.size() - 1;
     std::vector<double> X((size_t)N * 3, 0.0);
     for (int e = 0; e < ctx->E; ++e)
         for (int a = 0; a < 6; ++a)
             for (int d = 0; d < 3; ++d) X[(size_t)ctx->conn[(size_t)e * 6 + a] * 3 + d] = ctx->xref[(size_t)e * 18 + a * 3 + d];
-    std::vector<int32_t> agg0(n_agg + 1);
-    for (int lc = 0; lc < nct; ++lc) {
-        const int r0 = (int)((long long)N * lc / nct), r1 = (int)((long long)N * (lc + 1) / nct), L = r1 - r0;
-        for (int k = 0; k < m; ++k) agg0[lc * m + k] = r0 + (int)((long long)L * k / m);
-    }
-    agg0[n_agg] = N;
     std::vector<double> pm((size_t)N * 18, 0.0), nd((size_t)N * 3, 0.0), am((size_t)n_agg * 36, 0.0);
     std::vector<uint8_t> nmask(N, 0);
-    std::vector<int32_t> empty;
+    empty.clear();
     for (int i = 0; i < N; ++i)
         for (int d = 0; d < 3; ++d) {
             const size_t dof = (size_t)i * 3 + d;
@@ -895,6 +895,44 @@ int build_coarse(tf_ctx* ctx) {
     TF_CK(up(ctx->ca_blk, blk.data(), sizeof(int32_t) * blk.size()));
     TF_CK(up(ctx->ca_blk_row, blk_row.data(), sizeof(int32_t) * blk_row.size()));
     TF_CK(up(ctx->ca_empty, empty.data(), sizeof(int32_t) * empty.size()));
+    ctx->n_coarse_empty = (int)empty.size();
+    return TF_OK;
+}
+
+int build_batch_coarse(tf_ctx* ctx);
+
+int build_coarse(tf_ctx* ctx) {
+    ctx->coarse_dirty = false;
+    ctx->coarse_m = 0;
+    ctx->bc_active = false;
+    if (ctx->params.precond != TF_PRECOND_TWO_LEVEL) return TF_OK;
+    if (ctx->T > 1) return build_batch_coarse(ctx);
+    if (ctx->plan_ncta.empty()) return TF_OK;
+    const int N = ctx->N, nct = ctx->plan_ncta[0];
+    if (nct <= 0) return TF_OK;
+    int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
+    while (m > 1 && N / (nct * m) < 8) --m;
+    // each CTA's 6m rows of the n_coarse = 6 nct m inverse must fit its shared-memory block
+    while (m > 1 && (size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) --m;
+    if ((size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) return TF_OK;
+    // aggregates much larger than this no longer cut the iteration count (measured on the 2 M-node
+    // slab: 6,800-node aggregates left it unchanged); such tissues solve with block-Jacobi alone
+    if (N / (nct * m) > kMaxAggNodes) return TF_OK;
+    const int nw = ctx->persist_threads / 32;
+    while (m > 1 && nw / m < 1) --m;
+    const int n_agg = nct * m, nc = 6 * n_agg;
+    if (nc > kMaxCoarse) return TF_OK;  // plan too large for a staged coarse vector: block-Jacobi only
+    std::vector<int32_t> agg0(n_agg + 1);
+    for (int lc = 0; lc < nct; ++lc) {
+        const int r0 = (int)((long long)N * lc / nct), r1 = (int)((long long)N * (lc + 1) / nct), L = r1 - r0;
+        for (int k = 0; k < m; ++k) agg0[lc * m + k] = r0 + (int)((long long)L * k / m);
+    }
+    agg0[n_agg] = N;
+    std::vector<int32_t> empty;
+    {
+        const int rc = coarse_space_upload(ctx, agg0, empty);
+        if (rc != TF_OK) return rc;
+    }
     TF_CK(dalloc(ctx->coarse_a, sizeof(double) * (size_t)nc * nc));
     TF_CK(dalloc(ctx->coarse_inv, sizeof(double) * (size_t)nc * nc));
     TF_CK(dalloc(ctx->coarse_r, sizeof(double) * (size_t)nc));
@@ -920,10 +958,123 @@ int build_coarse(tf_ctx* ctx) {
     return TF_OK;
 }
 
+// Coarse space of a batch: every tissue's nodes split into contiguous aggregates of about
+// kBatchAggNodes nodes (at least one, at most kMaxCoarse / 6). Tissue t's coarse matrix (6 na_t
+// unknowns) sits at t ld^2 in a batch of ld x ld matrices, written transposed so that the batched
+// LU inverse comes out row-major; dropped modes and the padding rows get unit diagonals.
+int build_batch_coarse(tf_ctx* ctx) {
+    const int T = ctx->T;
+    std::vector<int32_t> agg0, tagg0(T + 1, 0), agg_tissue;
+    int ld = 6;
+    for (int t = 0; t < T; ++t) {
+        const int n0 = ctx->tissue_node0[t], nt = ctx->tissue_node0[t + 1] - n0;
+        int na = std::max(1, (int)std::lround((double)nt / kBatchAggNodes));
+        na = std::min(na, std::max(1, nt / 8));
+        na = std::min(na, kMaxCoarse / 6);
+        for (int k = 0; k < na; ++k) {
+            agg0.push_back(n0 + (int)((long long)nt * k / na));
+            agg_tissue.push_back(t);
+        }
+        tagg0[t + 1] = tagg0[t] + na;
+        ld = std::max(ld, 6 * na);
+    }
+    agg0.push_back(ctx->N);
+    std::vector<int32_t> empty;
+    {
+        const int rc = coarse_space_upload(ctx, agg0, empty);
+        if (rc != TF_OK) return rc;
+    }
+    const size_t ld2 = (size_t)ld * ld;
+    std::vector<int64_t> base(T), unit;
+    for (int t = 0; t < T; ++t) base[t] = (int64_t)t * (int64_t)ld2;
+    for (int32_t q : empty) {
+        const int a = q / 6;
+        const int t = agg_tissue[a];
+        const int local = q - 6 * tagg0[t];
+        unit.push_back(base[t] + (int64_t)local * (ld + 1));
+    }
+    for (int t = 0; t < T; ++t)
+        for (int local = 6 * (tagg0[t + 1] - tagg0[t]); local < ld; ++local) unit.push_back(base[t] + (int64_t)local * (ld + 1));
+    auto up = [&](DevBuf& b, const void* h, size_t bytes) -> cudaError_t {
+        cudaError_t e = dalloc(b, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess && bytes) e = cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice);
+        return e;
+    };
+    TF_CK(dalloc(ctx->coarse_a, sizeof(double) * ld2 * T));
+    TF_CK(dalloc(ctx->coarse_inv, sizeof(double) * ld2 * T));
+    TF_CK(dalloc(ctx->coarse_r, sizeof(double) * 6 * (size_t)tagg0[T]));
+    TF_CK(dalloc(ctx->bc_piv_d, sizeof(int32_t) * (size_t)ld * T));
+    TF_CK(dalloc(ctx->bc_info_d, sizeof(int32_t) * (size_t)T));
+    std::vector<double*> pa(T), pc(T);
+    for (int t = 0; t < T; ++t) {
+        pa[t] = dptr<double>(ctx->coarse_a) + base[t];
+        pc[t] = dptr<double>(ctx->coarse_inv) + base[t];
+    }
+    TF_CK(up(ctx->bc_ptr_a_d, pa.data(), sizeof(double*) * T));
+    TF_CK(up(ctx->bc_ptr_c_d, pc.data(), sizeof(double*) * T));
+    TF_CK(up(ctx->bc_tissue_agg0_d, tagg0.data(), sizeof(int32_t) * tagg0.size()));
+    TF_CK(up(ctx->bc_agg_node0_d, agg0.data(), sizeof(int32_t) * agg0.size()));
+    TF_CK(up(ctx->bc_agg_tissue_d, agg_tissue.data(), sizeof(int32_t) * agg_tissue.size()));
+    TF_CK(up(ctx->bc_base_d, base.data(), sizeof(int64_t) * base.size()));
+    TF_CK(up(ctx->bc_unit_d, unit.data(), sizeof(int64_t) * unit.size()));
+    if (!ctx->cb) {
+        if (cublasCreate(&ctx->cb) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, TF_ERR_CUDA, "cublasCreate");
+        if (cublasSetStream(ctx->cb, ctx->stream) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, TF_ERR_CUDA, "cublasSetStream");
+    }
+    if (!ctx->h_coarse_info) TF_CK(cudaMallocHost(&ctx->h_coarse_info, sizeof(int32_t)));
+    ctx->bc_tissue_agg0 = tagg0;
+    ctx->bc_ld = ld;
+    ctx->bc_n_unit = (int64_t)unit.size();
+    ctx->n_agg = tagg0[T];
+    ctx->n_coarse = 6 * tagg0[T];
+    ctx->bc_active = true;
+    ctx->coarse_age = 0;
+    ctx->coarse_ok = false;
+    return TF_OK;
+}
+
+int batch_coarse_setup(tf_ctx* ctx) {
+    const int T = ctx->T, ld = ctx->bc_ld;
+    CoarseAssembly ca;
+    ca.n_agg = ctx->n_agg;
+    ca.n_coarse = ctx->n_coarse;
+    ca.agg_slot_ptr = dptr<int32_t>(ctx->ca_agg_slot_ptr);
+    ca.slot_agg = dptr<int32_t>(ctx->ca_slot_agg);
+    ca.slot_ptr = dptr<int32_t>(ctx->ca_slot_ptr);
+    ca.blk = dptr<int32_t>(ctx->ca_blk);
+    ca.blk_row = dptr<int32_t>(ctx->ca_blk_row);
+    ca.empty = nullptr;
+    ca.n_empty = (int32_t)ctx->bc_n_unit;
+    ca.agg_tissue = dptr<int32_t>(ctx->bc_agg_tissue_d);
+    ca.tissue_agg0 = dptr<int32_t>(ctx->bc_tissue_agg0_d);
+    ca.tissue_base = dptr<int64_t>(ctx->bc_base_d);
+    ca.ld = ld;
+    ca.empty_offsets = dptr<int64_t>(ctx->bc_unit_d);
+    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), dptr<double>(ctx->coarse_a),
+                                 (size_t)ld * ld * T, ctx->stream));
+    ctx->launches += 1 + (ca.n_empty > 0 ? 1 : 0);  // this library's kernels only (not cuBLAS's)
+    double** pa = dptr<double*>(ctx->bc_ptr_a_d);
+    double** pc = dptr<double*>(ctx->bc_ptr_c_d);
+    int32_t* piv = dptr<int32_t>(ctx->bc_piv_d);
+    int32_t* info = dptr<int32_t>(ctx->bc_info_d);
+    if (cublasDgetrfBatched(ctx->cb, ld, pa, ld, piv, info, T) != CUBLAS_STATUS_SUCCESS)
+        return set_error(ctx, TF_ERR_CUDA, "cublasDgetrfBatched");
+    if (cublasDgetriBatched(ctx->cb, ld, (const double* const*)pa, ld, piv, pc, ld, info, T) != CUBLAS_STATUS_SUCCESS)
+        return set_error(ctx, TF_ERR_CUDA, "cublasDgetriBatched");
+    std::vector<int32_t> h_info(T);
+    TF_CK(cudaMemcpyAsync(h_info.data(), info, sizeof(int32_t) * T, cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    for (int32_t v : h_info)
+        if (v != 0) return TF_OK;  // a singular coarse operator: block-Jacobi only
+    ctx->coarse_ok = true;
+    return TF_OK;
+}
+
 // Assemble P^T J P for the current J and invert it; on a singular coarse operator the solve
 // runs with block-Jacobi alone (coarse_ok = false).
 int coarse_setup(tf_ctx* ctx) {
     ctx->coarse_ok = false;
+    if (ctx->bc_active) return batch_coarse_setup(ctx);
     if (ctx->coarse_m == 0) return TF_OK;
     const int nc = ctx->n_coarse;
     CoarseAssembly ca;
@@ -936,11 +1087,16 @@ int coarse_setup(tf_ctx* ctx) {
     ca.blk_row = dptr<int32_t>(ctx->ca_blk_row);
     ca.empty = dptr<int32_t>(ctx->ca_empty);
     ca.n_empty = ctx->n_coarse_empty;
+    ca.agg_tissue = nullptr;
+    ca.tissue_agg0 = nullptr;
+    ca.tissue_base = nullptr;
+    ca.ld = nc;
+    ca.empty_offsets = nullptr;
     double* A = dptr<double>(ctx->coarse_a);
     double* inv = dptr<double>(ctx->coarse_inv);
     int32_t* ipiv = dptr<int32_t>(ctx->coarse_ipiv);
     int32_t* info = dptr<int32_t>(ctx->coarse_info);
-    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), A, ctx->stream));
+    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), A, (size_t)nc * nc, ctx->stream));
     ctx->launches += 1 + (ca.n_empty > 0 ? 1 : 0);  // this library's kernels only (not cuSOLVER's)
     if (cusolverDnDgetrf(ctx->dn, nc, nc, A, nc, dptr<double>(ctx->coarse_work), ipiv, info) != CUSOLVER_STATUS_SUCCESS)
         return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrf");
@@ -977,7 +1133,7 @@ int krylov_solve(tf_ctx* ctx) {
             // fixed operator is a valid preconditioner: convergence is tested on the residual).
             const bool stale = !ctx->coarse_ok || ctx->coarse_age >= kCoarseMaxAge ||
                                (ctx->coarse_age > 1 && ctx->last_solve_iters * 10 > ctx->coarse_base_iters * 13);
-            if (ctx->coarse_m > 0 && stale) {
+            if ((ctx->coarse_m > 0 || ctx->bc_active) && stale) {
                 const int crc = coarse_setup(ctx);
                 if (crc != TF_OK) return crc;
                 ctx->coarse_age = 0;
@@ -1006,9 +1162,11 @@ int krylov_solve(tf_ctx* ctx) {
             return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
         }
         *ctx->h_sc = ctx->h_tsc[0];
-        ctx->last_solve_iters = ctx->h_sc->iter;
-        if (ctx->coarse_m > 0 && ctx->coarse_ok) {
-            if (ctx->coarse_age == 0) ctx->coarse_base_iters = ctx->h_sc->iter;
+        ctx->last_solve_iters = 0;
+        for (int t = 0; t < ctx->T; ++t)
+            if (ctx->T == 1 || ctx->h_active[t]) ctx->last_solve_iters = std::max(ctx->last_solve_iters, ctx->h_tsc[t].iter);
+        if ((ctx->coarse_m > 0 || ctx->bc_active) && ctx->coarse_ok) {
+            if (ctx->coarse_age == 0) ctx->coarse_base_iters = ctx->last_solve_iters;
             ++ctx->coarse_age;
         }
         return TF_OK;
@@ -1111,6 +1269,10 @@ int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
         for (int t = 0; t < T; ++t)
             weight[t] = (ctx->tissue_node0[t + 1] - ctx->tissue_node0[t]) * std::max(8.0, (double)ctx->last_krylov[t]);
     ctx->last_krylov.assign(T, 0);
+    if (T > 1 && persistent && ctx->params.precond == TF_PRECOND_TWO_LEVEL && ctx->coarse_dirty) {
+        const int crc = build_coarse(ctx);  // the batch plan gives every CTA whole aggregates
+        if (crc != TF_OK) return crc;
+    }
     while (n_active > 0) {
         if (T > 1 && persistent) {
             int rc = build_plan(ctx, weight, ctx->h_active);
@@ -1307,9 +1469,9 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         ctx->params = *params;
     else
         tf_default_params(&ctx->params);
-    // the two-level preconditioner needs one tissue and the persistent solve; elsewhere it
-    // stands down to block-Jacobi
-    if (ctx->params.precond == TF_PRECOND_TWO_LEVEL && (T > 1 || !ctx->params.persistent))
+    // the two-level preconditioner runs in the persistent solve (which a batch always uses); a
+    // single tissue solved in chunks stands down to block-Jacobi
+    if (ctx->params.precond == TF_PRECOND_TWO_LEVEL && T == 1 && !ctx->params.persistent)
         ctx->params.precond = TF_PRECOND_BLOCK_JACOBI;
     if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI && !(ctx->params.precond == TF_PRECOND_ILU0 && T == 1) &&
         ctx->params.precond != TF_PRECOND_TWO_LEVEL)
@@ -1481,6 +1643,10 @@ void tf_destroy(tf_ctx* ctx) {
                         &ctx->ca_slot_ptr, &ctx->ca_blk, &ctx->ca_blk_row, &ctx->ca_empty};
     for (DevBuf* b : coarse) dfree(*b);
     if (ctx->dn) cusolverDnDestroy(ctx->dn);
+    DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_node0_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
+                     &ctx->bc_ptr_a_d, &ctx->bc_ptr_c_d, &ctx->bc_info_d, &ctx->bc_piv_d};
+    for (DevBuf* b : bcb) dfree(*b);
+    if (ctx->cb) cublasDestroy(ctx->cb);
     if (ctx->h_coarse_info) cudaFreeHost(ctx->h_coarse_info);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);
     if (ctx->h_du2) cudaFreeHost(ctx->h_du2);
@@ -1713,7 +1879,7 @@ int tf_time_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out, tf_st
 int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes) {
     if (!ctx) return TF_ERR_ARGUMENT;
     if (precond) *precond = ctx->params.precond;
-    if (n_coarse) *n_coarse = ctx->coarse_m > 0 ? ctx->n_coarse : 0;
+    if (n_coarse) *n_coarse = (ctx->coarse_m > 0 || ctx->bc_active) ? ctx->n_coarse : 0;
     if (coarse_refreshes) *coarse_refreshes = ctx->coarse_refreshes;
     return TF_OK;
 }

@@ -128,6 +128,16 @@ struct BatchPlan {
     const double* agg_m;         // [aggregates][6][6] M_a, row-major
     const double* coarse_inv;    // [n_coarse][n_coarse] row-major inverse of P^T J P (read once per solve)
     double* coarse_r;            // [n_coarse] restricted vector
+    // two-level preconditioner of a batch (batch_coarse = 1; agg_per_cta = 0): every tissue has
+    // fixed aggregates, contiguous node ranges; CTA lc of tissue t's group of nct CTAs owns the
+    // aggregates [a0 + na lc / nct, a0 + na (lc + 1) / nct) of the tissue's na, and their rows.
+    // Aggregate a (global numbering) owns coarse unknowns 6a .. 6a+5 of coarse_r; tissue t's
+    // coarse inverse is row-major with leading dimension coarse_ld at coarse_inv + coarse_base[t].
+    int32_t batch_coarse;
+    int32_t coarse_ld;
+    const int32_t* tissue_agg0;  // [T+1]
+    const int32_t* agg_node0;    // [aggregates+1]
+    const int64_t* coarse_base;  // [T]
 };
 
 constexpr int kMaxAggPerCta = 4;
@@ -223,6 +233,14 @@ int persistent_max_grid(int device, int threads);
 // empty get a unit diagonal.
 struct CoarseAssembly {
     int32_t n_agg, n_coarse;
+    // batch: tissue t's matrix is written transposed (row-major for its inverse) into
+    // a_cm + tissue_base[t] with leading dimension ld, indices local to the tissue; the unit
+    // diagonal entries (modes without support, padding) are the offsets in `empty`
+    const int32_t* agg_tissue;     // [n_agg] or null (single tissue)
+    const int32_t* tissue_agg0;    // [T+1]
+    const int64_t* tissue_base;    // [T]
+    int32_t ld;
+    const int64_t* empty_offsets;  // [n_empty] batch unit-diagonal offsets
     const int32_t* agg_slot_ptr;   // [n_agg+1] slots of each aggregate
     const int32_t* slot_agg;       // [slots] neighbour aggregate of each slot
     const int32_t* slot_ptr;       // [slots+1] offsets into blk / blk_row
@@ -232,7 +250,7 @@ struct CoarseAssembly {
     int32_t n_empty;
 };
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
-                                   cudaStream_t s);
+                                   size_t a_cm_doubles, cudaStream_t s);
 cudaError_t launch_set_identity(double* m, int n, cudaStream_t s);
 cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
                                     int threads, cudaStream_t s);  // dynamic smem: the plan's coarse row block

@@ -569,6 +569,95 @@ __device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc
     return true;
 }
 
+// Phase A (PH 0) or C (PH 1) of a batch tissue with the two-level preconditioner: the CTA owns
+// the tissue's aggregates [a0, a1), one warp per aggregate. A warp updates its aggregate's rows,
+// applies D^-1, restricts ((mask o u, d x (mask o u)) summed in fixed order, M_a^T applied by
+// lanes 0-5) into coarse_r; after the group barrier the CTA stages the tissue's restricted vector,
+// and the same warp forms its aggregate's six rows of the tissue's coarse inverse times it,
+// z_a = M_a y_a, and adds t + omega x d to the same rows. Returns false when the barrier timed out.
+template <int PH>
+__device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t, int a0, int a1, double alpha,
+                              double beta, double omega, GridBarrier* bar, int nct, double* cs) {
+    double* vin = PH == 0 ? w.p : w.s;
+    double* out = PH == 0 ? w.phat : w.shat;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int a = a0 + warp; a < a1; a += nw) {
+        const int n0 = plan.agg_node0[a], n1 = plan.agg_node0[a + 1];
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int n = n0 + lane; n < n1; n += 32) {
+            double u[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                u[i] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+                vin[d] = u[i];
+            }
+            const double* D = w.dinv + (size_t)n * 9;
+            out[n * 3 + 0] = D[0] * u[0] + D[1] * u[1] + D[2] * u[2];
+            out[n * 3 + 1] = D[3] * u[0] + D[4] * u[1] + D[5] * u[2];
+            out[n * 3 + 2] = D[6] * u[0] + D[7] * u[1] + D[8] * u[2];
+            const int mk = plan.node_mask[n];
+            const double u0 = (mk & 1) ? u[0] : 0.0, u1 = (mk & 2) ? u[1] : 0.0, u2 = (mk & 4) ? u[2] : 0.0;
+            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+            acc[0] += u0;
+            acc[1] += u1;
+            acc[2] += u2;
+            acc[3] += dy * u2 - dz * u1;
+            acc[4] += dz * u0 - dx * u2;
+            acc[5] += dx * u1 - dy * u0;
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+        if (lane < 6) {
+            const double* M = plan.agg_m + (size_t)a * 36;
+            double c = 0.0;
+#pragma unroll
+            for (int p = 0; p < 6; ++p) c += M[p * 6 + lane] * acc[p];
+            plan.coarse_r[6 * (size_t)a + lane] = c;
+        }
+    }
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    const int g0 = plan.tissue_agg0[t];
+    const int nc = 6 * (plan.tissue_agg0[t + 1] - g0);
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) cs[c] = __ldcg(plan.coarse_r + 6 * (size_t)g0 + c);
+    __syncthreads();
+    const double* inv = plan.coarse_inv + plan.coarse_base[t];
+    const int ld = plan.coarse_ld;
+    for (int a = a0 + warp; a < a1; a += nw) {
+        const double* rows = inv + (size_t)(6 * (a - g0)) * ld;
+        double y[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int c = lane; c < nc; c += 32) {
+            const double x = cs[c];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) y[q] += __ldcg(rows + (size_t)q * ld + c) * x;
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) y[q] += __shfl_xor_sync(0xffffffffu, y[q], off);
+        const double* M = plan.agg_m + (size_t)a * 36;
+        double z[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            double v = 0.0;
+#pragma unroll
+            for (int p = 0; p < 6; ++p) v += M[q * 6 + p] * y[p];
+            z[q] = v;
+        }
+        const int n0 = plan.agg_node0[a], n1 = plan.agg_node0[a + 1];
+        for (int n = n0 + lane; n < n1; n += 32) {
+            const int mk = plan.node_mask[n];
+            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+            if (mk & 1) out[n * 3] += z[0] + z[4] * dz - z[5] * dy;
+            if (mk & 2) out[n * 3 + 1] += z[1] + z[5] * dx - z[3] * dz;
+            if (mk & 4) out[n * 3 + 2] += z[2] + z[3] * dy - z[4] * dx;
+        }
+    }
+    return true;
+}
+
 // BiCGStab restart after a breakdown: rhat = r, p = v = 0, rho = (r, r); at most kMaxRestarts
 // per solve. Returns false when the restarts are used up (the caller reports a breakdown).
 constexpr int kMaxRestarts = 8;
@@ -608,8 +697,16 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
     const int lc = blockIdx.x - c0;
     const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
-    const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
-    const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+    int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
+    int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+    int ba0 = 0, ba1 = 0;  // this CTA's aggregates of a batch tissue with the two-level preconditioner
+    if (plan.batch_coarse) {
+        const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
+        ba0 = g0 + (int)((long long)na * lc / nct);
+        ba1 = g0 + (int)((long long)na * (lc + 1) / nct);
+        r0 = plan.agg_node0[ba0];
+        r1 = plan.agg_node0[ba1];
+    }
     GridBarrier* bar = plan.barriers + t;
     double* part[2] = {w.partials + 4 * c0, w.partials + 4 * c0 + 2 * nct};
     int pb = 0;
@@ -651,6 +748,8 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
         const double beta = (rho / rho_prev) * (alpha / omega);
         if (plan.agg_per_cta > 0) {
             if (!precond_phase<0>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
+        } else if (plan.batch_coarse) {
+            if (!precond_batch<0>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs)) return false;
         } else {
             for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -683,6 +782,8 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
         // C: s = r - alpha v; shat = M^-1 s
         if (plan.agg_per_cta > 0) {
             if (!precond_phase<1>(w, plan, lc, r0, r1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
+        } else if (plan.batch_coarse) {
+            if (!precond_batch<1>(w, plan, t, ba0, ba1, alpha, 0.0, 0.0, bar, nct, cs)) return false;
         } else {
             for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -995,14 +1096,25 @@ __global__ void k_coarse_assemble(KrylovWork w, CoarseAssembly ca, const double*
             for (int d = 0; d < 3; ++d)
                 sum += Pi[d * 6 + r] * (__ldg(J + d * 3) * u0 + __ldg(J + d * 3 + 1) * u1 + __ldg(J + d * 3 + 2) * u2);
         }
-        const int R = 6 * a + r, C = 6 * ca.slot_agg[s] + c;
-        a_cm[(size_t)R + (size_t)C * ca.n_coarse] = sum;
+        if (ca.agg_tissue) {
+            const int tt = ca.agg_tissue[a], g0 = ca.tissue_agg0[tt];
+            const int R = 6 * (a - g0) + r, C = 6 * (ca.slot_agg[s] - g0) + c;
+            a_cm[ca.tissue_base[tt] + (size_t)C + (size_t)R * ca.ld] = sum;
+        } else {
+            const int R = 6 * a + r, C = 6 * ca.slot_agg[s] + c;
+            a_cm[(size_t)R + (size_t)C * ca.n_coarse] = sum;
+        }
     }
 }
 
 __global__ void k_coarse_empty(double* a_cm, int n, const int32_t* empty, int n_empty) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n_empty) a_cm[(size_t)empty[i] * (n + 1)] = 1.0;
+}
+
+__global__ void k_coarse_unit(double* a_cm, const int64_t* offsets, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a_cm[offsets[i]] = 1.0;
 }
 
 __global__ void k_set_identity(double* m, int n) {
@@ -1013,11 +1125,16 @@ __global__ void k_set_identity(double* m, int n) {
 }  // namespace
 
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
-                                   cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(a_cm, 0, sizeof(double) * (size_t)ca.n_coarse * ca.n_coarse, s);
+                                   size_t a_cm_doubles, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(a_cm, 0, sizeof(double) * a_cm_doubles, s);
     if (e != cudaSuccess) return e;
     if (ca.n_agg > 0) k_coarse_assemble<<<ca.n_agg, 256, 0, s>>>(w, ca, pmode, a_cm);
-    if (ca.n_empty > 0) k_coarse_empty<<<(ca.n_empty + 255) / 256, 256, 0, s>>>(a_cm, ca.n_coarse, ca.empty, ca.n_empty);
+    if (ca.n_empty > 0) {
+        if (ca.agg_tissue)
+            k_coarse_unit<<<(ca.n_empty + 255) / 256, 256, 0, s>>>(a_cm, ca.empty_offsets, ca.n_empty);
+        else
+            k_coarse_empty<<<(ca.n_empty + 255) / 256, 256, 0, s>>>(a_cm, ca.n_coarse, ca.empty, ca.n_empty);
+    }
     return cudaGetLastError();
 }
 
