@@ -105,7 +105,7 @@ struct tf_ctx {
     int bc_ld = 0;
     int64_t bc_n_unit = 0;
     std::vector<int32_t> bc_tissue_agg0;
-    DevBuf bc_tissue_agg0_d, bc_agg_node0_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_ptr_a_d, bc_ptr_c_d, bc_info_d,
+    DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_ptr_a_d, bc_ptr_c_d, bc_info_d,
         bc_piv_d;
     cublasHandle_t cb = nullptr;
 
@@ -537,13 +537,13 @@ AssembleArgs make_assemble(tf_ctx* c, double dt) {
 }
 
 // CTA plan of the persistent solve. A tissue's expected work is weight[t] (rows x BiCGStab
-// iterations); with W the active total and C the co-resident CTAs, a tissue whose work is at least
-// one CTA's share q = W / C gets a group of about weight / q CTAs (at least 64 rows each) and runs
-// with group barriers; the smaller tissues are packed into the remaining CTAs by longest-first bin
-// packing and each packing CTA solves its tissues one after another (CTA-level barriers only).
-// The slowest tissues thereby get the most CTAs instead of every small tissue holding one for the
-// whole launch. Inactive tissues get none. The plan is rebuilt every Newton round of a batch with
-// the last Krylov iteration counts as weights.
+// iterations). The plan minimises the largest per-CTA load Q over the C co-resident CTAs: every
+// tissue heavier than Q gets a group of ceil(weight / Q) CTAs (at least 64 rows each; with a
+// batch coarse space at most one CTA per aggregate) and runs with group barriers; the lighter
+// tissues are packed first-fit-decreasing into bins of capacity Q, and each bin's CTA solves its
+// tissues one after another (CTA-level barriers only). Q is the smallest value (by bisection)
+// whose groups and bins fit in C. Inactive tissues get none. The plan is rebuilt every Newton
+// round of a batch with the last Krylov iteration counts as weights.
 int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* active) {
     const int T = ctx->T;
     const int cmax = std::max(ctx->persistent_grid_max, 1);
@@ -560,65 +560,67 @@ int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* ac
     std::vector<int32_t> n(T, 0);                 // CTAs of a group tissue (0: packed or inactive)
     std::vector<std::vector<int32_t>> lists;      // tissues of every CTA
     if (ctx->persistent_grid_max > 0 && n_act > 0) {
-        const double q = wsum / cmax;
-        std::vector<int> small;
-        int group_ctas = 0;
+        std::vector<int64_t> cap(T, 1);  // most CTAs a tissue's group may have
+        std::vector<int> order;          // active tissues, heaviest first
         for (int t = 0; t < T; ++t) {
             if (!active[t]) continue;
-            int64_t cap = std::max<int64_t>(1, (rows[t] + 63) / 64);
+            cap[t] = std::max<int64_t>(1, (rows[t] + 63) / 64);
             if (ctx->bc_active && (int)ctx->bc_tissue_agg0.size() == T + 1)  // every CTA owns whole aggregates
-                cap = std::min<int64_t>(cap, ctx->bc_tissue_agg0[t + 1] - ctx->bc_tissue_agg0[t]);
-            const int64_t want = q > 0 ? (int64_t)(weight[t] / q) : 1;
-            if (want >= 2 && cap >= 2) {
-                n[t] = (int32_t)std::min(want, cap);
-                group_ctas += n[t];
-            } else {
-                small.push_back(t);
-            }
+                cap[t] = std::min<int64_t>(cap[t], ctx->bc_tissue_agg0[t + 1] - ctx->bc_tissue_agg0[t]);
+            order.push_back(t);
         }
-        double small_w = 0.0;
-        for (int t : small) small_w += weight[t];
-        int bins = small.empty() ? 0 : std::max(1, (int)std::ceil(small_w / std::max(q, 1e-300) - 1e-9));
-        bins = std::min<int>(bins, (int)small.size());
-        // the groups shrink in proportion if groups and bins together exceed the grid
-        if (group_ctas + bins > cmax && group_ctas > 0) {
-            const double f = (double)(cmax - bins) / group_ctas;
-            group_ctas = 0;
-            for (int t = 0; t < T; ++t)
-                if (n[t] > 0) {
-                    n[t] = std::max(2, (int)(n[t] * f));
-                    group_ctas += n[t];
+        std::sort(order.begin(), order.end(),
+                  [&](int a, int b) { return weight[a] > weight[b] || (weight[a] == weight[b] && a < b); });
+        // CTAs needed when no CTA should carry more than Q: a group of ceil(w / Q) CTAs for every
+        // tissue heavier than Q, first-fit-decreasing bins of capacity Q for the others
+        std::vector<double> load;
+        std::vector<std::vector<int32_t>> bins;
+        auto need = [&](double Q, bool keep) -> int64_t {
+            int64_t groups = 0;
+            load.clear();
+            bins.clear();
+            for (int t : order) {
+                const double w = std::max(weight[t], 0.0);
+                if (w > Q && cap[t] > 1) {
+                    const int64_t k = std::min<int64_t>(cap[t], std::max<int64_t>(2, (int64_t)std::ceil(w / Q)));
+                    if (keep) n[t] = (int32_t)k;
+                    groups += k;
+                    continue;
                 }
-            while (group_ctas + bins > cmax) {  // still over: take CTAs from the largest groups
-                int tm = -1;
-                for (int t = 0; t < T; ++t)
-                    if (n[t] > 2 && (tm < 0 || n[t] > n[tm])) tm = t;
-                if (tm < 0) break;
-                --n[tm];
-                --group_ctas;
+                size_t b = 0;
+                while (b < load.size() && load[b] + w > Q) ++b;
+                if (b == load.size()) {
+                    load.push_back(0.0);
+                    bins.emplace_back();
+                }
+                load[b] += w;
+                bins[b].push_back(t);
             }
-            if (group_ctas + bins > cmax)
-                return set_error(ctx, TF_ERR_UNSUPPORTED, "tissues do not fit the co-resident CTAs");
+            return groups + (int64_t)load.size();
+        };
+        // the smallest per-CTA load that fits the co-resident CTAs (bisection; Q = W always fits)
+        double lo = wsum / cmax, hi = std::max(wsum, 1e-300);
+        if (need(lo, false) <= cmax) hi = lo;
+        for (int it = 0; it < 60 && hi > lo * (1.0 + 1e-9); ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if (need(mid, false) <= cmax)
+                hi = mid;
+            else
+                lo = mid;
         }
-        for (int t = 0; t < T; ++t) {
-            ctx->plan_cta0.resize(T);
+        need(hi, true);
+        ctx->plan_cta0.resize(T);
+        for (int t : order)
             if (n[t] > 0) {
                 ctx->plan_cta0[t] = (int32_t)lists.size();
                 for (int k = 0; k < n[t]; ++k) lists.push_back({t});
             }
-        }
-        if (bins > 0) {
-            std::sort(small.begin(), small.end(), [&](int a, int b) { return weight[a] > weight[b] || (weight[a] == weight[b] && a < b); });
-            const int base = (int)lists.size();
-            std::vector<double> load(bins, 0.0);
-            lists.resize(base + bins);
-            for (int t : small) {
-                int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-                lists[base + k].push_back(t);
-                load[k] += weight[t];
-                ctx->plan_cta0[t] = base + k;
+        for (auto& bin : bins) {
+            for (int32_t t : bin) {
+                ctx->plan_cta0[t] = (int32_t)lists.size();
                 n[t] = 1;
             }
+            lists.push_back(bin);
         }
     } else {
         for (int t = 0; t < T; ++t)
@@ -691,7 +693,8 @@ BatchPlan make_plan(tf_ctx* c) {
     p.batch_coarse = (c->bc_active && c->coarse_ok) ? 1 : 0;
     p.coarse_ld = c->bc_ld;
     p.tissue_agg0 = dptr<int32_t>(c->bc_tissue_agg0_d);
-    p.agg_node0 = dptr<int32_t>(c->bc_agg_node0_d);
+    p.agg_ptr = dptr<int32_t>(c->bc_agg_ptr_d);
+    p.agg_nodes = dptr<int32_t>(c->bc_agg_nodes_d);
     p.coarse_base = dptr<int64_t>(c->bc_base_d);
     p.n_tissues = c->T;
     p.n_cta = (int32_t)c->plan_list_ptr.size() - 1;
@@ -782,8 +785,9 @@ int krylov_status_to_tf(int ks) {
 // DoFs zeroed; two-pass modified Gram-Schmidt with the coefficient transform tracked; a mode
 // below 1e-6 of its initial norm dropped and listed in `empty`) of the aggregates with node
 // boundaries agg0, the per-aggregate block lists of the coarse assembly, all uploaded.
-int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg0, std::vector<int32_t>& empty) {
-    const int N = ctx->N, n_agg = (int)agg0.size() - 1;
+int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg_ptr, const std::vector<int32_t>& agg_nodes,
+                        std::vector<int32_t>& empty) {
+    const int N = ctx->N, n_agg = (int)agg_ptr.size() - 1;
     std::vector<double> X((size_t)N * 3, 0.0);
     for (int e = 0; e < ctx->E; ++e)
         for (int a = 0; a < 6; ++a)
@@ -798,15 +802,16 @@ int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg0, std::vect
             if (!fixed && ctx->dofmap[dof] == (int32_t)dof) nmask[i] |= (uint8_t)(1u << d);
         }
     for (int a = 0; a < n_agg; ++a) {
-        const int s0 = agg0[a], n = agg0[a + 1] - s0;
+        const int32_t* nodes = agg_nodes.data() + agg_ptr[a];
+        const int n = agg_ptr[a + 1] - agg_ptr[a];
         double c[3] = {0, 0, 0};
         for (int i = 0; i < n; ++i)
-            for (int d = 0; d < 3; ++d) c[d] += X[(size_t)(s0 + i) * 3 + d] / n;
+            for (int d = 0; d < 3; ++d) c[d] += X[(size_t)nodes[i] * 3 + d] / n;
         // the masked modes B_i = [I | (d_i x)] as explicit columns over the aggregate's DoFs
         const size_t len = (size_t)3 * n;
         std::vector<double> B(6 * len, 0.0);
         for (int i = 0; i < n; ++i) {
-            const int node = s0 + i;
+            const int node = nodes[i];
             double dd[3];
             for (int d = 0; d < 3; ++d) dd[d] = nd[(size_t)node * 3 + d] = X[(size_t)node * 3 + d] - c[d];
             const double Bi[3][6] = {{1, 0, 0, 0, dd[2], -dd[1]}, {0, 1, 0, -dd[2], 0, dd[0]}, {0, 0, 1, dd[1], -dd[0], 0}};
@@ -854,20 +859,22 @@ int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg0, std::vect
         // explicit modes for the coarse-operator assembly: P_i = mask_i o (B_i M)
         for (int i = 0; i < n; ++i)
             for (int d = 0; d < 3; ++d)
-                for (int q = 0; q < 6; ++q) pm[(size_t)(s0 + i) * 18 + d * 6 + q] = B[q * len + 3 * i + d];
+                for (int q = 0; q < 6; ++q) pm[(size_t)nodes[i] * 18 + d * 6 + q] = B[q * len + 3 * i + d];
     }
     // Jacobian blocks grouped by (row aggregate, column aggregate)
     std::vector<int32_t> aggof(N);
     for (int a = 0; a < n_agg; ++a)
-        for (int i = agg0[a]; i < agg0[a + 1]; ++i) aggof[i] = a;
+        for (int k = agg_ptr[a]; k < agg_ptr[a + 1]; ++k) aggof[agg_nodes[k]] = a;
     std::vector<int32_t> agg_slot_ptr(n_agg + 1, 0), slot_agg, slot_ptr(1, 0), blk, blk_row;
     blk.reserve(ctx->nnzb);
     blk_row.reserve(ctx->nnzb);
     std::vector<std::array<int32_t, 3>> items;
     for (int a = 0; a < n_agg; ++a) {
         items.clear();
-        for (int i = agg0[a]; i < agg0[a + 1]; ++i)
+        for (int q = agg_ptr[a]; q < agg_ptr[a + 1]; ++q) {
+            const int i = agg_nodes[q];
             for (int k = ctx->rowptr[i]; k < ctx->rowptr[i + 1]; ++k) items.push_back({aggof[ctx->colidx[k]], k, i});
+        }
         std::sort(items.begin(), items.end());
         for (size_t q = 0; q < items.size(); ++q) {
             if (q == 0 || items[q][0] != items[q - 1][0]) {
@@ -930,7 +937,9 @@ int build_coarse(tf_ctx* ctx) {
     agg0[n_agg] = N;
     std::vector<int32_t> empty;
     {
-        const int rc = coarse_space_upload(ctx, agg0, empty);
+        std::vector<int32_t> iota(N);
+        for (int k = 0; k < N; ++k) iota[k] = k;
+        const int rc = coarse_space_upload(ctx, agg0, iota, empty);
         if (rc != TF_OK) return rc;
     }
     TF_CK(dalloc(ctx->coarse_a, sizeof(double) * (size_t)nc * nc));
@@ -958,30 +967,88 @@ int build_coarse(tf_ctx* ctx) {
     return TF_OK;
 }
 
-// Coarse space of a batch: every tissue's nodes split into contiguous aggregates of about
-// kBatchAggNodes nodes (at least one, at most kMaxCoarse / 6). Tissue t's coarse matrix (6 na_t
-// unknowns) sits at t ld^2 in a batch of ld x ld matrices, written transposed so that the batched
-// LU inverse comes out row-major; dropped modes and the padding rows get unit diagonals.
+// Recursive coordinate bisection of the n nodes in `nodes` into `parts` spatial sets of nearly
+// equal size: each range is split across the longest side of its bounding box, in proportion to
+// the parts on either side; nodes at the same coordinate stay on one side where the split allows
+// (a prism column's nodes share x and y). On return nodes[cuts[k] .. cuts[k+1]) is part k.
+void bisect_nodes(const std::vector<double>& X, int32_t* nodes, int n, int parts, std::vector<int32_t>& cuts) {
+    cuts.assign(1, 0);
+    struct Range { int b, e, parts; };
+    std::vector<Range> stack{{0, n, parts}};
+    std::vector<std::pair<int, int>> done;  // (begin, end) of finished parts, in order of completion
+    while (!stack.empty()) {
+        const Range r = stack.back();
+        stack.pop_back();
+        if (r.parts <= 1 || r.e - r.b <= 1) {
+            done.push_back({r.b, r.e});
+            continue;
+        }
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int i = r.b; i < r.e; ++i)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], X[(size_t)nodes[i] * 3 + d]);
+                hi[d] = std::max(hi[d], X[(size_t)nodes[i] * 3 + d]);
+            }
+        int ax = 0;
+        for (int d = 1; d < 3; ++d)
+            if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+        std::sort(nodes + r.b, nodes + r.e, [&](int32_t u, int32_t v) {
+            const double cu = X[(size_t)u * 3 + ax], cv = X[(size_t)v * 3 + ax];
+            return cu < cv || (cu == cv && u < v);
+        });
+        const int p1 = r.parts / 2;
+        int k = r.b + (int)((long long)(r.e - r.b) * p1 / r.parts);
+        auto coord = [&](int i) { return X[(size_t)nodes[i] * 3 + ax]; };
+        int kf = k;
+        while (kf < r.e && kf > r.b && coord(kf) == coord(kf - 1)) ++kf;
+        if (kf < r.e && kf - k <= 8) {
+            k = kf;
+        } else {
+            int kb = k;
+            while (kb > r.b && coord(kb) == coord(kb - 1)) --kb;
+            if (kb > r.b && k - kb <= 8) k = kb;
+        }
+        k = std::min(std::max(k, r.b + 1), r.e - 1);
+        stack.push_back({k, r.e, r.parts - p1});  // popped after the left half: parts stay in order
+        stack.push_back({r.b, k, p1});
+    }
+    std::sort(done.begin(), done.end());
+    for (auto& d : done) cuts.push_back(d.second);
+    while ((int)cuts.size() < parts + 1) cuts.push_back(n);  // fewer nodes than parts: empty tails
+}
+
+// Coarse space of a batch: every tissue's nodes split into spatial aggregates of about
+// kBatchAggNodes nodes (at least one, at most kMaxCoarse / 6) by coordinate bisection, so that
+// the aggregates are compact whatever the mesh's node numbering. Tissue t's coarse matrix
+// (6 na_t unknowns) sits at t ld^2 in a batch of ld x ld matrices, written transposed so that the
+// batched LU inverse comes out row-major; dropped modes and the padding rows get unit diagonals.
 int build_batch_coarse(tf_ctx* ctx) {
     const int T = ctx->T;
-    std::vector<int32_t> agg0, tagg0(T + 1, 0), agg_tissue;
+    std::vector<double> X((size_t)ctx->N * 3, 0.0);  // reference positions of the nodes
+    for (int e = 0; e < ctx->E; ++e)
+        for (int a = 0; a < 6; ++a)
+            for (int d = 0; d < 3; ++d) X[(size_t)ctx->conn[(size_t)e * 6 + a] * 3 + d] = ctx->xref[(size_t)e * 18 + a * 3 + d];
+    std::vector<int32_t> agg_ptr(1, 0), agg_nodes(ctx->N), tagg0(T + 1, 0), agg_tissue;
     int ld = 6;
     for (int t = 0; t < T; ++t) {
         const int n0 = ctx->tissue_node0[t], nt = ctx->tissue_node0[t + 1] - n0;
         int na = std::max(1, (int)std::lround((double)nt / kBatchAggNodes));
         na = std::min(na, std::max(1, nt / 8));
         na = std::min(na, kMaxCoarse / 6);
+        for (int k = 0; k < nt; ++k) agg_nodes[n0 + k] = n0 + k;
+        std::vector<int32_t> cuts;
+        bisect_nodes(X, agg_nodes.data() + n0, nt, na, cuts);
         for (int k = 0; k < na; ++k) {
-            agg0.push_back(n0 + (int)((long long)nt * k / na));
+            std::sort(agg_nodes.begin() + n0 + cuts[k], agg_nodes.begin() + n0 + cuts[k + 1]);
+            agg_ptr.push_back(n0 + cuts[k + 1]);
             agg_tissue.push_back(t);
         }
         tagg0[t + 1] = tagg0[t] + na;
         ld = std::max(ld, 6 * na);
     }
-    agg0.push_back(ctx->N);
     std::vector<int32_t> empty;
     {
-        const int rc = coarse_space_upload(ctx, agg0, empty);
+        const int rc = coarse_space_upload(ctx, agg_ptr, agg_nodes, empty);
         if (rc != TF_OK) return rc;
     }
     const size_t ld2 = (size_t)ld * ld;
@@ -1013,7 +1080,8 @@ int build_batch_coarse(tf_ctx* ctx) {
     TF_CK(up(ctx->bc_ptr_a_d, pa.data(), sizeof(double*) * T));
     TF_CK(up(ctx->bc_ptr_c_d, pc.data(), sizeof(double*) * T));
     TF_CK(up(ctx->bc_tissue_agg0_d, tagg0.data(), sizeof(int32_t) * tagg0.size()));
-    TF_CK(up(ctx->bc_agg_node0_d, agg0.data(), sizeof(int32_t) * agg0.size()));
+    TF_CK(up(ctx->bc_agg_ptr_d, agg_ptr.data(), sizeof(int32_t) * agg_ptr.size()));
+    TF_CK(up(ctx->bc_agg_nodes_d, agg_nodes.data(), sizeof(int32_t) * agg_nodes.size()));
     TF_CK(up(ctx->bc_agg_tissue_d, agg_tissue.data(), sizeof(int32_t) * agg_tissue.size()));
     TF_CK(up(ctx->bc_base_d, base.data(), sizeof(int64_t) * base.size()));
     TF_CK(up(ctx->bc_unit_d, unit.data(), sizeof(int64_t) * unit.size()));
@@ -1643,7 +1711,7 @@ void tf_destroy(tf_ctx* ctx) {
                         &ctx->ca_slot_ptr, &ctx->ca_blk, &ctx->ca_blk_row, &ctx->ca_empty};
     for (DevBuf* b : coarse) dfree(*b);
     if (ctx->dn) cusolverDnDestroy(ctx->dn);
-    DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_node0_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
+    DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_ptr_d, &ctx->bc_agg_nodes_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
                      &ctx->bc_ptr_a_d, &ctx->bc_ptr_c_d, &ctx->bc_info_d, &ctx->bc_piv_d};
     for (DevBuf* b : bcb) dfree(*b);
     if (ctx->cb) cublasDestroy(ctx->cb);

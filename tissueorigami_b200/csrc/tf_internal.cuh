@@ -129,14 +129,17 @@ struct BatchPlan {
     const double* coarse_inv;    // [n_coarse][n_coarse] row-major inverse of P^T J P (read once per solve)
     double* coarse_r;            // [n_coarse] restricted vector
     // two-level preconditioner of a batch (batch_coarse = 1; agg_per_cta = 0): every tissue has
-    // fixed aggregates, contiguous node ranges; CTA lc of tissue t's group of nct CTAs owns the
-    // aggregates [a0 + na lc / nct, a0 + na (lc + 1) / nct) of the tissue's na, and their rows.
-    // Aggregate a (global numbering) owns coarse unknowns 6a .. 6a+5 of coarse_r; tissue t's
-    // coarse inverse is row-major with leading dimension coarse_ld at coarse_inv + coarse_base[t].
+    // fixed aggregates, spatial node sets (recursive coordinate bisection) listed in agg_nodes
+    // [agg_ptr[a], agg_ptr[a+1]); CTA lc of tissue t's group of nct CTAs applies the
+    // preconditioner on the aggregates [a0 + na lc / nct, a0 + na (lc + 1) / nct) of the tissue's
+    // na (its SpMV and vector rows stay the contiguous row range). Aggregate a (global numbering)
+    // owns coarse unknowns 6a .. 6a+5 of coarse_r; tissue t's coarse inverse is row-major with
+    // leading dimension coarse_ld at coarse_inv + coarse_base[t].
     int32_t batch_coarse;
     int32_t coarse_ld;
     const int32_t* tissue_agg0;  // [T+1]
-    const int32_t* agg_node0;    // [aggregates+1]
+    const int32_t* agg_ptr;      // [aggregates+1]
+    const int32_t* agg_nodes;    // [N] node ids, aggregate after aggregate
     const int64_t* coarse_base;  // [T]
 };
 

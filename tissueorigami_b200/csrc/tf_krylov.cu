@@ -570,7 +570,7 @@ __device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc
 }
 
 // Phase A (PH 0) or C (PH 1) of a batch tissue with the two-level preconditioner: the CTA owns
-// the tissue's aggregates [a0, a1), one warp per aggregate. A warp updates its aggregate's rows,
+// the tissue's aggregates [a0, a1), one warp per aggregate. A warp updates its aggregate's nodes,
 // applies D^-1, restricts ((mask o u, d x (mask o u)) summed in fixed order, M_a^T applied by
 // lanes 0-5) into coarse_r; after the group barrier the CTA stages the tissue's restricted vector,
 // and the same warp forms its aggregate's six rows of the tissue's coarse inverse times it,
@@ -582,9 +582,10 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
     double* out = PH == 0 ? w.phat : w.shat;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int a = a0 + warp; a < a1; a += nw) {
-        const int n0 = plan.agg_node0[a], n1 = plan.agg_node0[a + 1];
+        const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int n = n0 + lane; n < n1; n += 32) {
+        for (int k = k0 + lane; k < k1; k += 32) {
+            const int n = plan.agg_nodes[k];
             double u[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
@@ -646,8 +647,9 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
             for (int p = 0; p < 6; ++p) v += M[q * 6 + p] * y[p];
             z[q] = v;
         }
-        const int n0 = plan.agg_node0[a], n1 = plan.agg_node0[a + 1];
-        for (int n = n0 + lane; n < n1; n += 32) {
+        const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
+        for (int k = k0 + lane; k < k1; k += 32) {
+            const int n = plan.agg_nodes[k];
             const int mk = plan.node_mask[n];
             const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
             if (mk & 1) out[n * 3] += z[0] + z[4] * dz - z[5] * dy;
@@ -697,15 +699,13 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     const int c0 = plan.cta0[t], nct = plan.ncta[t];
     const int lc = blockIdx.x - c0;
     const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
-    int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
-    int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+    const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
+    const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
     int ba0 = 0, ba1 = 0;  // this CTA's aggregates of a batch tissue with the two-level preconditioner
     if (plan.batch_coarse) {
         const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
         ba0 = g0 + (int)((long long)na * lc / nct);
         ba1 = g0 + (int)((long long)na * (lc + 1) / nct);
-        r0 = plan.agg_node0[ba0];
-        r1 = plan.agg_node0[ba1];
     }
     GridBarrier* bar = plan.barriers + t;
     double* part[2] = {w.partials + 4 * c0, w.partials + 4 * c0 + 2 * nct};
