@@ -78,6 +78,8 @@ struct tf_ctx {
     int32_t T = 1;
     std::vector<int32_t> tissue_node0, tissue_elem0;
     std::vector<int32_t> plan_list_ptr, plan_list, plan_cta0, plan_ncta;
+    DevBuf plan_queue_d, queue_head_d;
+    std::vector<int32_t> plan_queue;
     DevBuf node_tissue_d, plan_list_ptr_d, plan_list_d, plan_cta0_d, plan_ncta_d, plan_row0_d, active_d, tbarriers, tscalars,
         tdu2;
     int32_t* h_active = nullptr;     // pinned [T]
@@ -407,7 +409,7 @@ int upload_structure(tf_ctx* ctx) {
     }
     ctx->coarse_dirty = true;
     const size_t np2 = std::max((size_t)std::max(spmv_grid(N), vec_grid(N)) * 2,
-                                (size_t)ctx->persistent_grid_max * 4) + 64;
+                                (size_t)ctx->persistent_grid_max * 8) + 64;
     TF_CK(dalloc(ctx->partials, sizeof(double) * np2));
     if (ctx->krylov_graph) {
         cudaGraphExecDestroy(ctx->krylov_graph);
@@ -622,11 +624,20 @@ int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* ac
             }
             lists.push_back(bin);
         }
+        // the solve takes the bins' tissues from a queue, heaviest first, on every CTA as it
+        // becomes free (the bins remain the static assignment of the Newton update); the grid is
+        // filled up to the co-resident CTAs
+        ctx->plan_queue.clear();
+        for (int t : order)
+            if (n[t] == 1) ctx->plan_queue.push_back(t);
+        while ((int)lists.size() < cmax && !ctx->plan_queue.empty()) lists.emplace_back();
     } else {
+        ctx->plan_queue.clear();
         for (int t = 0; t < T; ++t)
             if (active[t]) {
                 n[t] = 1;
                 lists.push_back({t});
+                ctx->plan_queue.push_back(t);
             }
     }
     ctx->plan_cta0.resize(T, 0);
@@ -648,6 +659,11 @@ int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* ac
     // every CTA of a group lists its tissue once; a packed tissue appears once in its bin
     TF_CK(dalloc(ctx->plan_list_d, sizeof(int32_t) * ((size_t)cmax + T + 1)));
     TF_CK(dalloc(ctx->plan_cta0_d, sizeof(int32_t) * T));
+    TF_CK(dalloc(ctx->plan_queue_d, sizeof(int32_t) * (T + 1)));
+    TF_CK(dalloc(ctx->queue_head_d, sizeof(int32_t) * 4));
+    if (!ctx->plan_queue.empty())
+        TF_CK(cudaMemcpyAsync(ctx->plan_queue_d.p, ctx->plan_queue.data(), sizeof(int32_t) * ctx->plan_queue.size(),
+                              cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(dalloc(ctx->plan_ncta_d, sizeof(int32_t) * T));
     TF_CK(dalloc(ctx->plan_row0_d, sizeof(int32_t) * (T + 1)));
     TF_CK(cudaMemcpyAsync(ctx->plan_list_ptr_d.p, ctx->plan_list_ptr.data(), sizeof(int32_t) * (C + 1),
@@ -660,7 +676,7 @@ int build_plan(tf_ctx* ctx, const std::vector<double>& weight, const int32_t* ac
     TF_CK(cudaMemcpyAsync(ctx->plan_row0_d.p, ctx->tissue_node0.data(), sizeof(int32_t) * (T + 1), cudaMemcpyHostToDevice,
                           ctx->stream));
     TF_CK(cudaStreamSynchronize(ctx->stream));  // the host vectors may change before the next round
-    const size_t need = 4 * (size_t)cmax + 64;
+    const size_t need = 8 * (size_t)cmax + 64;  // groups' slots, then every CTA's own queue slots
     if (ctx->partials.bytes < sizeof(double) * need) TF_CK(dalloc(ctx->partials, sizeof(double) * need));
     return TF_OK;
 }
@@ -704,6 +720,9 @@ BatchPlan make_plan(tf_ctx* c) {
     p.ncta = dptr<int32_t>(c->plan_ncta_d);
     p.row0 = dptr<int32_t>(c->plan_row0_d);
     p.active = dptr<int32_t>(c->active_d);
+    p.queue = dptr<int32_t>(c->plan_queue_d);
+    p.n_queue = (int32_t)c->plan_queue.size();
+    p.queue_head = dptr<int32_t>(c->queue_head_d);
     p.barriers = dptr<GridBarrier>(c->tbarriers);
     p.scalars = dptr<KrylovScalars>(c->tscalars);
     p.du2 = dptr<double>(c->tdu2);
@@ -1209,6 +1228,7 @@ int krylov_solve(tf_ctx* ctx) {
             }
         }
         const BatchPlan plan = make_plan(ctx);
+        TF_CK(cudaMemsetAsync(ctx->queue_head_d.p, 0, sizeof(int32_t), ctx->stream));
         TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
         TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
                                       ctx->persist_threads, ctx->stream));
@@ -1697,8 +1717,8 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
                      &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier};
     for (DevBuf* b : all) dfree(*b);
-    DevBuf* batch[] = {&ctx->node_tissue_d, &ctx->plan_list_ptr_d, &ctx->plan_list_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d,
-                       &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
+    DevBuf* batch[] = {&ctx->plan_queue_d, &ctx->queue_head_d, &ctx->node_tissue_d, &ctx->plan_list_ptr_d,
+                       &ctx->plan_list_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d, &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
     for (DevBuf* b : batch) dfree(*b);
     for (auto* v : {&ctx->cp_x, &ctx->cp_fg, &ctx->seg_x, &ctx->seg_fg})
         for (DevBuf& b : *v) dfree(b);

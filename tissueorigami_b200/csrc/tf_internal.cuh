@@ -112,6 +112,12 @@ struct BatchPlan {
     const int32_t* ncta;         // [T]
     const int32_t* row0;         // [T+1]
     const int32_t* active;       // [T]
+    // tissues solved by one CTA each (the packing CTAs' tissues), heaviest first: once its group
+    // tissue (if any) is solved, every CTA takes the next one (atomic ticket in queue_head, zeroed
+    // before each launch), so these tissues are spread over the CTAs as they become free
+    const int32_t* queue;        // [n_queue]
+    int32_t n_queue;
+    int32_t* queue_head;
     GridBarrier* barriers;       // [T]
     KrylovScalars* scalars;      // [T]
     double* du2;                 // [T] ||du||^2 of the last Newton update

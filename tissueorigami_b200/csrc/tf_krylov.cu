@@ -690,14 +690,14 @@ __device__ bool restart(const KrylovWork& w, int r0, int r1, double& rho, double
 }
 
 // The whole block-Jacobi (or two-level) BiCGStab solve of tissue t by this CTA, which is CTA lc of
-// the tissue's group (nct = 1: the tissue is one of several packed into this CTA, solved one after
-// another with CTA-level barriers only). Returns false when a group barrier timed out.
-__device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, double rtol, int max_iter,
-                             double* smem, double* sb, double* red, double* ys, double* Ms, double* cs,
+// the tissue's group (nct = 1: a tissue solved by this CTA alone, with CTA-level barriers only).
+// The group's per-CTA partial sums live at partials[4 pbase ..) (4 nct doubles). Returns false
+// when a group barrier timed out.
+__device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int pbase, double rtol,
+                             int max_iter, double* smem, double* sb, double* red, double* ys, double* Ms, double* cs,
                              float* cinv_s) {
     if (!plan.active[t]) return true;
-    const int c0 = plan.cta0[t], nct = plan.ncta[t];
-    const int lc = blockIdx.x - c0;
+    const int nct = plan.ncta[t];
     const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
     const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
     const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
@@ -708,7 +708,7 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
         ba1 = g0 + (int)((long long)na * (lc + 1) / nct);
     }
     GridBarrier* bar = plan.barriers + t;
-    double* part[2] = {w.partials + 4 * c0, w.partials + 4 * c0 + 2 * nct};
+    double* part[2] = {w.partials + 4 * pbase, w.partials + 4 * pbase + 2 * nct};
     int pb = 0;
     if (plan.agg_per_cta > 0) {
         const size_t cnt = (size_t)6 * plan.agg_per_cta * plan.n_coarse;
@@ -866,9 +866,28 @@ __global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(Kryl
     __shared__ double Ms[kMaxAggPerCta * 36];  // M_a of the CTA's aggregates
     __shared__ double cs[kMaxCoarse];
     extern __shared__ float cinv_s[];  // this CTA's 6m rows of the coarse inverse (FP32)
-    // a CTA of a multi-CTA group has one tissue; a packing CTA solves its small tissues in turn
-    for (int j = plan.cta_list_ptr[blockIdx.x]; j < plan.cta_list_ptr[blockIdx.x + 1]; ++j)
-        if (!solve_tissue(w, plan, plan.cta_list[j], rtol, max_iter, smem, sb, red, ys, Ms, cs, cinv_s)) return;
+    __shared__ int ticket;
+    // a CTA of a multi-CTA group solves its tissue first (partials at its group's slots)
+    const int j0 = plan.cta_list_ptr[blockIdx.x];
+    if (j0 < plan.cta_list_ptr[blockIdx.x + 1]) {
+        const int t = plan.cta_list[j0];
+        if (plan.ncta[t] > 1 &&
+            !solve_tissue(w, plan, t, blockIdx.x - plan.cta0[t], plan.cta0[t], rtol, max_iter, smem, sb, red, ys, Ms,
+                          cs, cinv_s))
+            return;
+    }
+    // then every CTA takes single-CTA tissues from the queue until it is empty; their partials use
+    // this CTA's own slots past the groups' (a group partner may still be reading the group's)
+    for (;;) {
+        if (threadIdx.x == 0) ticket = atomicAdd(plan.queue_head, 1);
+        __syncthreads();
+        const int q = ticket;
+        __syncthreads();
+        if (q >= plan.n_queue) break;
+        if (!solve_tissue(w, plan, plan.queue[q], 0, plan.n_cta + blockIdx.x, rtol, max_iter, smem, sb, red, ys, Ms, cs,
+                          cinv_s))
+            return;
+    }
 }
 
 // Newton update of a batch: du[slave] = du[master] first (separate kernel), then per CTA of
