@@ -456,7 +456,7 @@ def run_batch(args) -> None:
         units, launches, worst = tot.tolist()
         t_dev = tm.item()
     seq = None
-    if world == 1:
+    if world == 1 and not args.no_sequential:
         # sequential baseline: the same tissues one after another, one context each, same steps
         seq_ms, seq_units = 0.0, 0.0
         for t in ts:
@@ -581,6 +581,8 @@ def main():
     ap.add_argument("--workload", default="wing_disc")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sequential", action="store_true",
+                    help="batch workload: skip the sequential single-tissue comparison (profiling runs)")
     ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")
     ap.add_argument("--precond", choices=["block_jacobi", "ilu0", "two_level"], default="two_level",
                     help="Krylov preconditioner of the single-tissue workloads")
