@@ -197,7 +197,8 @@ def run_b200(args) -> None:
     t = make_tissue(args.workload)
     precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0,
                "two_level": capi.TF_PRECOND_TWO_LEVEL}[args.precond]
-    s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent)
+    s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent,
+                                        smoother_nodes=args.smoother_nodes)
     sched = s.autotune(t.x, t.dt)
     sched["precond"] = args.precond
     sched["solve"] = {0: "graph-replayed iteration kernels", 1: "persistent cooperative kernel"}[args.persistent]
@@ -285,6 +286,7 @@ def run_b200(args) -> None:
     sched["precond_effective"] = {0: "block_jacobi", 1: "ilu0", 2: "two_level"}.get(pc_eff, pc_eff)
     sched["coarse_unknowns"] = n_coarse
     sched["coarse_refreshes"] = refreshes
+    sched["smoother_block_nodes"] = s.smoother_block()
 
     # kernel timings for the roofline
     ms_el, ms_spmv = s.time_kernels(20)
@@ -314,8 +316,11 @@ def run_b200(args) -> None:
     # persistent solve: per BiCGStab iteration two SpMVs (each also reads one dot vector)
     # and three node-wise phases (p/phat: r,p,v,D -> p,phat; s/shat: r,v,D -> s,shat;
     # x/r: x,phat,shat,s,t,rhat -> x,r); plus one setup pass (diagonal inverses, r, rhat, p, v)
-    per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 72 + 4 * 24 + 72 + 8 * 24)
-    per_setup = N * (72.0 + 72 + 24 + 4 * 24)
+    # D^-1 is 72 G bytes per node with blocks of G nodes (a prism column's 3G x 3G inverse); with
+    # G > 1 it is set up by a separate kernel before the launch
+    G = sched.get("smoother_block_nodes", 1)
+    per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 72 * G + 4 * 24 + 72 * G + 8 * 24)
+    per_setup = N * ((72.0 + 72 if G == 1 else 0.0) + 24 + 4 * 24)
     if args.precond == "two_level" and sched.get("coarse_unknowns", 0) > 0:
         # two applications of the coarse correction per iteration, each reading the node modes
         # (d_i, mask) in the restriction and the prolongation and updating the preconditioned
@@ -581,6 +586,9 @@ def main():
     ap.add_argument("--workload", default="wing_disc")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--smoother-nodes", type=int, choices=[0, 1, 2, 3, 4], default=0,
+                    help="block-Jacobi block of a single tissue: 0 = a prism column when the mesh "
+                         "numbers it consecutively, 1 = one node")
     ap.add_argument("--no-sequential", action="store_true",
                     help="batch workload: skip the sequential single-tissue comparison (profiling runs)")
     ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")

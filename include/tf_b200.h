@@ -81,6 +81,10 @@ typedef struct tf_params {
     int32_t use_graphs;       /* capture the Krylov iteration in a CUDA graph (1) or not    */
     int32_t persistent;       /* whole solve in one cooperative persistent kernel (1) or    */
                               /* graph-replayed chunks of iteration kernels (0)             */
+    int32_t smoother_nodes;   /* block-Jacobi block of a single tissue's persistent solve:  */
+                              /* 0 = a prism column (its G <= 4 nodes) when the mesh numbers */
+                              /* every column's nodes consecutively, else one node; 1 = one */
+                              /* node (3x3); 2-4 = that many consecutive nodes              */
 } tf_params;
 
 typedef struct tf_step_stats {
@@ -226,6 +230,11 @@ int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* 
  * aggregates would be too large to help), and how many times the coarse operators have been
  * refactorised. */
 int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes);
+
+/* Nodes per block of the block-Jacobi smoother the context uses (1: 3x3 node blocks; G > 1:
+ * the 3G x 3G diagonal sub-block of G consecutive nodes, a prism column). No counterpart in the
+ * reference, whose Pardiso solve needs no smoother. */
+int tf_get_smoother_block(tf_ctx* ctx, int32_t* nodes);
 
 /* Time the assembly variants on the context's current state and keep the fastest
  * (scatter mode x teams per CTA). Returns the chosen pair through tf_get_schedule. */

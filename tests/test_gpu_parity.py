@@ -147,6 +147,75 @@ def test_time_steps_disc_matches_sparse_oracle(persistent):
     assert np.abs(x - x_ref).max() <= 1e-9 * t.size
 
 
+@pytest.mark.parametrize("precond", ["two_level", "block_jacobi"])
+def test_column_smoother_solve_matches_direct(precond):
+    """Block-Jacobi over a prism column's three nodes (9x9 blocks; the wing disc numbers each
+    column's nodes consecutively) against SuperLU and against 3x3 node blocks: 1e-8 relative in
+    ||du||, no more BiCGStab iterations than with node blocks."""
+    pc = {"two_level": capi.TF_PRECOND_TWO_LEVEL, "block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI}[precond]
+    t = mesh.wing_disc(n_surface_points=3000)
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
+    J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
+    du_ref = sla.spsolve(J, g)
+    iters = {}
+    for sn in (0, 1):
+        with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, precond=pc, smoother_nodes=sn) as s:
+            assert s.smoother_block() == (3 if sn == 0 else 1)
+            du, rc, iters[sn], rr = s.solveForDeltaU(vals, g)
+        assert rc == capi.TF_OK and rr <= 1e-13
+        assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
+        assert np.all(du[t.fixed.reshape(-1) != 0] == 0.0)
+    assert iters[0] <= iters[1]
+
+
+def test_column_smoother_steps_match_sparse_oracle():
+    """Implicit steps of a three-surface disc with the default (column) smoother: positions
+    within 1e-9 of the tissue size of the sparse oracle, the same Newton iteration counts."""
+    t = mesh.wing_disc(n_surface_points=1500, n_steps=2)
+    x_ref, fg_ref, it_ref, _ = O.simulate_sparse(t, n_steps=2)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+        assert s.smoother_block() == 3
+        x = t.x.copy()
+        its = []
+        for _ in range(2):
+            x, rc, st = s.runOneStep(x, t.dt)
+            assert rc == capi.TF_OK
+            its.append(st["newton_iters"])
+    assert its == list(it_ref)
+    assert np.abs(x - x_ref).max() <= 1e-9 * t.size
+
+
+@pytest.mark.parametrize("nodes", [2, 4])
+def test_forced_smoother_blocks_solve_matches_direct(nodes):
+    """Blocks of G consecutive nodes that are not columns (forced G = 2 and the largest, G = 4,
+    on a one-layer rectangle of 108 nodes) still precondition the same system: 1e-8 relative in
+    ||du|| against SuperLU."""
+    t = mesh.small_rectangle(nx=9, ny=6)
+    t, uk, un, inv = _state(t)
+    vs = O.viscosity_surfaces(t, uk)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, uk, un, vs, inv, rowptr, colidx)
+    du_ref = sla.spsolve(O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc(), g)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, smoother_nodes=nodes) as s:
+        assert s.smoother_block() == nodes
+        du, rc, iters, rr = s.solveForDeltaU(vals, g)
+    assert rc == capi.TF_OK and rr <= 1e-13
+    assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
+
+
+def test_smoother_nodes_argument_checks():
+    t = mesh.small_disc(7, 600, 1200.0)  # two surfaces: columns of two nodes
+    with NewtonRaphsonSolver.from_tissue(t) as s:
+        assert s.smoother_block() == 2
+    with NewtonRaphsonSolver.from_tissue(t, persistent=0) as s:
+        assert s.smoother_block() == 1  # the chunked path keeps node blocks
+    with pytest.raises(capi.TFError):
+        NewtonRaphsonSolver.from_tissue(t, smoother_nodes=5)
+
+
 def test_status_newton_cap():
     t = mesh.small_rectangle(nx=5, ny=4)
     with NewtonRaphsonSolver.from_tissue(t, max_newton_iters=0) as s:

@@ -48,7 +48,7 @@ EXPORTS = [
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
-    "tf_solve_direct", "tf_get_preconditioner",
+    "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block",
 ]
 
 
@@ -62,7 +62,8 @@ class Params(ctypes.Structure):
                 ("krylov_max_iters", ctypes.c_int32), ("krylov_rtol", ctypes.c_double),
                 ("precond", ctypes.c_int32), ("scatter", ctypes.c_int32),
                 ("elems_per_block", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32)]
+                ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32),
+                ("smoother_nodes", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):
@@ -129,6 +130,7 @@ def load(build_if_missing: bool = True):
     L.tf_time_step_device.argtypes = [_P, _P, c_double, _P, ctypes.POINTER(StepStats)]
     L.tf_get_schedule.argtypes = [_P, _I, _I, _I]
     L.tf_get_preconditioner.argtypes = [_P, _I, _I, _I]
+    L.tf_get_smoother_block.argtypes = [_P, _I]
     L.tf_autotune.argtypes = [_P, _D, c_double]
     L.tf_time_kernels.argtypes = [_P, c_int, _D, _D]
     L.tf_batch_create.argtypes = [c_int, ctypes.POINTER(MeshDesc), ctypes.POINTER(Params), ctypes.POINTER(_P)]

@@ -62,6 +62,7 @@ struct tf_ctx {
     std::vector<int32_t> colour_offsets;  // colour c: elements colour_list[off[c]..off[c+1])
     std::vector<int32_t> colour_list;     // colour-sorted element ids, routed ones at the end
     int32_t n_routed = 0;
+    int smooth_G = 1;  // smoother block: G consecutive nodes (single tissue, persistent solve)
     int n_colours = 0;
     bool has_visc = false;
 
@@ -720,6 +721,7 @@ BatchPlan make_plan(tf_ctx* c) {
     p.ncta = dptr<int32_t>(c->plan_ncta_d);
     p.row0 = dptr<int32_t>(c->plan_row0_d);
     p.active = dptr<int32_t>(c->active_d);
+    p.group = c->T == 1 ? c->smooth_G : 1;
     p.queue = dptr<int32_t>(c->plan_queue_d);
     p.n_queue = (int32_t)c->plan_queue.size();
     p.queue_head = dptr<int32_t>(c->queue_head_d);
@@ -949,9 +951,13 @@ int build_coarse(tf_ctx* ctx) {
     const int n_agg = nct * m, nc = 6 * n_agg;
     if (nc > kMaxCoarse) return TF_OK;  // plan too large for a staged coarse vector: block-Jacobi only
     std::vector<int32_t> agg0(n_agg + 1);
-    for (int lc = 0; lc < nct; ++lc) {
-        const int r0 = (int)((long long)N * lc / nct), r1 = (int)((long long)N * (lc + 1) / nct), L = r1 - r0;
-        for (int k = 0; k < m; ++k) agg0[lc * m + k] = r0 + (int)((long long)L * k / m);
+    for (int lc = 0; lc < nct; ++lc) {  // the persistent solve's CTA row ranges and aggregates
+        int r0, r1, a0, a1;
+        group_split(0, N, lc, nct, ctx->smooth_G, r0, r1);
+        for (int k = 0; k < m; ++k) {
+            group_split(r0, r1, k, m, ctx->smooth_G, a0, a1);
+            agg0[lc * m + k] = a0;
+        }
     }
     agg0[n_agg] = N;
     std::vector<int32_t> empty;
@@ -1228,6 +1234,10 @@ int krylov_solve(tf_ctx* ctx) {
             }
         }
         const BatchPlan plan = make_plan(ctx);
+        if (plan.group > 1) {
+            TF_CK(launch_group_jacobi_setup(w, plan.group, ctx->stream));
+            ctx->launches += 1;
+        }
         TF_CK(cudaMemsetAsync(ctx->queue_head_d.p, 0, sizeof(int32_t), ctx->stream));
         TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
         TF_CK(launch_bicgstab_batched(w, plan, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
@@ -1518,6 +1528,7 @@ void tf_default_params(tf_params* p) {
     p->device = 0;
     p->use_graphs = 1;
     p->persistent = 1;
+    p->smoother_nodes = 0;
 }
 
 const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
@@ -1528,6 +1539,30 @@ struct CtxDeleter {
 
 // Create a context over one mesh whose nodes and elements are split into T consecutive
 // tissues (node0 / elem0 hold T+1 offsets); T = 1 is the single-tissue context.
+// Nodes per prism column when the mesh numbers every column's nodes consecutively (all G nodes
+// of each group 0..G-1, G..2G-1, ... at the same reference x, y), trying G = 4, 3, 2; else 1.
+int column_size(tf_ctx* ctx) {
+    const int N = ctx->N;
+    std::vector<double> X((size_t)N * 3, 0.0);
+    for (int e = 0; e < ctx->E; ++e)
+        for (int a = 0; a < 6; ++a)
+            for (int d = 0; d < 3; ++d) X[(size_t)ctx->conn[(size_t)e * 6 + a] * 3 + d] = ctx->xref[(size_t)e * 18 + a * 3 + d];
+    double scale = 0.0;
+    for (double v : X) scale = std::max(scale, std::fabs(v));
+    const double tol = 1e-9 * std::max(scale, 1.0);
+    for (int G = 4; G >= 2; --G) {
+        if (N % G != 0) continue;
+        bool ok = true;
+        for (int g = 0; g < N / G && ok; ++g)
+            for (int j = 1; j < G && ok; ++j) {
+                const size_t a = (size_t)g * G, b = a + j;
+                ok = std::fabs(X[a * 3] - X[b * 3]) <= tol && std::fabs(X[a * 3 + 1] - X[b * 3 + 1]) <= tol;
+            }
+        if (ok) return G;
+    }
+    return 1;
+}
+
 static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t T, const int32_t* node0,
                       const int32_t* elem0, tf_ctx** out) {
     if (!out) return TF_ERR_ARGUMENT;
@@ -1656,6 +1691,14 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
     ctx->scatter = ctx->params.scatter == TF_SCATTER_AUTO ? TF_SCATTER_ATOMIC : ctx->params.scatter;
     ctx->teams = ctx->params.elems_per_block > 0 ? ctx->params.elems_per_block : 16;
     if (ctx->teams != 8 && ctx->teams != 16 && ctx->teams != 32) return TF_ERR_ARGUMENT;
+    {
+        const int sn = ctx->params.smoother_nodes;
+        if (sn < 0 || sn > 4) return TF_ERR_ARGUMENT;
+        if (sn >= 2 && N % sn != 0) return TF_ERR_ARGUMENT;
+        ctx->smooth_G = 1;
+        if (ctx->T == 1 && use_persistent(ctx)) ctx->smooth_G = sn >= 2 ? sn : (sn == 0 ? column_size(ctx) : 1);
+        if (ctx->smooth_G > 1) TF_CK(dalloc(ctx->dinv, sizeof(double) * 9 * (size_t)ctx->smooth_G * N));
+    }
     *out = holder.release();
     return TF_OK;
 }
@@ -1969,6 +2012,12 @@ int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int3
     if (precond) *precond = ctx->params.precond;
     if (n_coarse) *n_coarse = (ctx->coarse_m > 0 || ctx->bc_active) ? ctx->n_coarse : 0;
     if (coarse_refreshes) *coarse_refreshes = ctx->coarse_refreshes;
+    return TF_OK;
+}
+
+int tf_get_smoother_block(tf_ctx* ctx, int32_t* nodes) {
+    if (!ctx || !nodes) return TF_ERR_ARGUMENT;
+    *nodes = ctx->T == 1 && use_persistent(ctx) ? ctx->smooth_G : 1;
     return TF_OK;
 }
 

@@ -112,6 +112,12 @@ struct BatchPlan {
     const int32_t* ncta;         // [T]
     const int32_t* row0;         // [T+1]
     const int32_t* active;       // [T]
+    // smoother block of a single tissue: G consecutive nodes (a prism column when the mesh numbers
+    // a column's nodes consecutively). G = 1: the node's 3x3 inverse in dinv [N][9]; G > 1: the
+    // inverse of the 3G x 3G diagonal sub-block of group g in FP32, column-major at
+    // (float*)dinv + g (3G)^2, computed before the launch and applied one DoF per lane; row
+    // ranges and aggregates hold whole groups.
+    int32_t group;
     // tissues solved by one CTA each (the packing CTAs' tissues), heaviest first: once its group
     // tissue (if any) is solved, every CTA takes the next one (atomic ticket in queue_head, zeroed
     // before each launch), so these tissues are spread over the CTAs as they become free
@@ -261,6 +267,17 @@ struct CoarseAssembly {
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
                                    size_t a_cm_doubles, cudaStream_t s);
 cudaError_t launch_set_identity(double* m, int n, cudaStream_t s);
+// Rows [r0, r1) of part k of n of the rows [b0, b1), cut at multiples of G from b0 (G = 1: the
+// proportional split b0 + L k / n). The persistent solve's CTA row ranges and a single tissue's
+// two-level aggregates are cut this way, so a smoother group never straddles two of them.
+__host__ __device__ inline void group_split(int b0, int b1, int k, int n, int G, int& r0, int& r1) {
+    const long long ng = (b1 - b0 + G - 1) / G;
+    r0 = b0 + (int)(G * (ng * k / n));
+    const int e = b0 + (int)(G * (ng * (k + 1) / n));
+    r1 = e < b1 ? e : b1;
+}
+// Inverses of the 3G x 3G diagonal sub-blocks of J (G > 1 layout of BatchPlan::group).
+cudaError_t launch_group_jacobi_setup(const KrylovWork& w, int G, cudaStream_t s);
 cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, double rtol, int max_iter,
                                     int threads, cudaStream_t s);  // dynamic smem: the plan's coarse row block
 // uk += du on active tissues, du[slave] = du[master], per-tissue ||du||^2 into plan.du2

@@ -455,6 +455,34 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
     D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
+// Smoother groups of G > 1 nodes are handled one DoF per lane: a warp takes 32 / 3G groups at a
+// time (lanes gl * 3G + r, r < 3G; the remaining lanes idle), every lane updates its DoF (phase A:
+// u = p = r + beta (p - omega v); phase C: u = s = r - alpha v, written to vin) and forms its row of
+// out = D_g^-1 u, the group's other entries of u arriving by warp shuffles. D_g^-1 is stored
+// column-major per group in FP32 (k_group_jacobi_setup), so a warp's loads of one column are
+// contiguous; the products are summed in FP64.
+// Called by all 32 lanes of the warp; valid = this lane has a DoF. Returns u (0 when not valid).
+template <int PH>
+__device__ __forceinline__ double group_dof_update_apply(const KrylovWork& w, int g, int r, int n3, bool valid,
+                                                         double alpha, double beta, double omega, double* vin,
+                                                         double* out) {
+    const int d = g * n3 + r;
+    double u = 0.0;
+    if (valid) {
+        u = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+        vin[d] = u;
+    }
+    const int base = ((threadIdx.x & 31) / n3) * n3;
+    const float* D = reinterpret_cast<const float*>(w.dinv) + (size_t)g * n3 * n3 + r;
+    double o = 0.0;
+    for (int c = 0; c < n3; ++c) {
+        const double uc = __shfl_sync(0xffffffffu, u, min(base + c, 31));
+        if (valid) o += (double)D[c * n3] * uc;
+    }
+    if (valid) out[d] = o;
+    return u;
+}
+
 // Phase A (PH 0: p = r + beta (p - omega v), phat = M^-1 p) or C (PH 1: s = r - alpha v,
 // shat = M^-1 s) of an iteration on the CTA's rows [r0, r1), with the two-level
 // preconditioner M^-1 = D^-1 + P (P^T J P)^-1 P^T (plan.agg_per_cta = m > 0). The CTA's warps
@@ -471,13 +499,39 @@ __device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc
                               double* cs, const float* cinv, const double* Ms) {
     double* vin = PH == 0 ? w.p : w.s;
     double* out = PH == 0 ? w.phat : w.shat;
-    const int m = plan.agg_per_cta, L = r1 - r0;
+    const int m = plan.agg_per_cta, G = plan.group;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int wpa = nw / m;
     const int k = warp / wpa, wi = warp - k * wpa;
-    const int a0 = r0 + (int)((long long)L * k / m), a1 = r0 + (int)((long long)L * (k + 1) / m);
+    int a0, a1;
+    group_split(r0, r1, k, m, G, a0, a1);
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (k < m) {
+    if (k < m && G > 1) {
+        const int n3 = 3 * G, gpw = 32 / n3, gl = lane / n3, rr = lane - gl * n3;
+        const int g1 = a1 / G;
+        for (int gc = a0 / G + wi * gpw; gc < g1; gc += wpa * gpw) {
+            const int g = gc + gl;
+            const bool valid = gl < gpw && g < g1;
+            const double u = group_dof_update_apply<PH>(w, valid ? g : gc, rr, n3, valid, alpha, beta, omega, vin, out);
+            if (valid) {
+                // restriction of this DoF: translation i, and the rotations d x (mask o u)
+                const int n = g * G + rr / 3, i = rr % 3;
+                const double ui = ((plan.node_mask[n] >> i) & 1) ? u : 0.0;
+                const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+                acc[i] += ui;
+                if (i == 0) {
+                    acc[4] += dz * ui;
+                    acc[5] -= dy * ui;
+                } else if (i == 1) {
+                    acc[3] -= dz * ui;
+                    acc[5] += dx * ui;
+                } else {
+                    acc[3] += dy * ui;
+                    acc[4] -= dx * ui;
+                }
+            }
+        }
+    } else if (k < m) {
         for (int n = a0 + wi * 32 + lane; n < a1; n += wpa * 32) {
             double u[3];
 #pragma unroll
@@ -699,8 +753,8 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     if (!plan.active[t]) return true;
     const int nct = plan.ncta[t];
     const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
-    const int r0 = tr0 + (int)((long long)(tr1 - tr0) * lc / nct);
-    const int r1 = tr0 + (int)((long long)(tr1 - tr0) * (lc + 1) / nct);
+    int r0, r1;
+    group_split(tr0, tr1, lc, nct, plan.group, r0, r1);
     int ba0 = 0, ba1 = 0;  // this CTA's aggregates of a batch tissue with the two-level preconditioner
     if (plan.batch_coarse) {
         const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
@@ -720,7 +774,7 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2
     double v1[1] = {0.0};
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
-        block_jacobi_row(w, n);
+        if (plan.group == 1) block_jacobi_row(w, n);  // G > 1: inverses set up before the launch
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const int d = n * 3 + i;
@@ -750,6 +804,14 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
             if (!precond_phase<0>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
         } else if (plan.batch_coarse) {
             if (!precond_batch<0>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs)) return false;
+        } else if (plan.group > 1) {
+            const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
+            const int g1 = r1 / plan.group;
+            for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
+                const bool valid = gl < gpw && gc + gl < g1;
+                group_dof_update_apply<0>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, beta, omega, w.p,
+                                          w.phat);
+            }
         } else {
             for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -784,6 +846,14 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
             if (!precond_phase<1>(w, plan, lc, r0, r1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
         } else if (plan.batch_coarse) {
             if (!precond_batch<1>(w, plan, t, ba0, ba1, alpha, 0.0, 0.0, bar, nct, cs)) return false;
+        } else if (plan.group > 1) {
+            const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
+            const int g1 = r1 / plan.group;
+            for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
+                const bool valid = gl < gpw && gc + gl < g1;
+                group_dof_update_apply<1>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, 0.0, 0.0, w.s,
+                                          w.shat);
+            }
         } else {
             for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
 #pragma unroll
@@ -1094,6 +1164,75 @@ cudaError_t launch_bicgstab_iteration_ilu(const KrylovWork& w, const IluPlan& il
 
 namespace {
 
+// One thread per smoother group g of G nodes: gathers the 3G x 3G diagonal sub-block of J from
+// the BSR3 rows (the group's diagonal blocks and the blocks that couple its nodes), inverts it by
+// Gauss-Jordan elimination with partial pivoting (FP64) and writes the inverse column-major,
+// rounded to FP32: it only preconditions (the solve tests convergence on the FP64 residual), and
+// half the bytes keep the apply's loads near those of the 3x3 node blocks. A singular sub-block (zero or non-finite pivot) sets DF_SINGULAR_DIAG and leaves the
+// identity, as the 3x3 block-Jacobi does.
+__global__ void __launch_bounds__(128) k_group_jacobi_setup(KrylovWork w, int G) {
+    const int NG = w.n_nodes / G;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= NG) return;
+    const int n3 = 3 * G, gs = g * G;
+    double A[12][12], B[12][12];
+    for (int r = 0; r < n3; ++r)
+        for (int c = 0; c < n3; ++c) {
+            A[r][c] = 0.0;
+            B[r][c] = r == c ? 1.0 : 0.0;
+        }
+    for (int i = 0; i < G; ++i) {
+        const int n = gs + i;
+        for (int k = w.rowptr[n]; k < w.rowptr[n + 1]; ++k) {
+            const int c = w.colidx[k];
+            if (c < gs || c >= gs + G) continue;
+            const double* blk = w.vals + (size_t)k * 9;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) A[3 * i + a][3 * (c - gs) + b] = blk[a * 3 + b];
+        }
+    }
+    bool ok = true;
+    for (int col = 0; col < n3 && ok; ++col) {
+        int piv = col;
+        double best = fabs(A[col][col]);
+        for (int r = col + 1; r < n3; ++r)
+            if (fabs(A[r][col]) > best) {
+                best = fabs(A[r][col]);
+                piv = r;
+            }
+        if (!(best > 0.0) || !isfinite(best)) {
+            ok = false;
+            break;
+        }
+        if (piv != col)
+            for (int c = 0; c < n3; ++c) {
+                const double ta = A[col][c], tb = B[col][c];
+                A[col][c] = A[piv][c];
+                B[col][c] = B[piv][c];
+                A[piv][c] = ta;
+                B[piv][c] = tb;
+            }
+        const double inv = 1.0 / A[col][col];
+        for (int c = 0; c < n3; ++c) {
+            A[col][c] *= inv;
+            B[col][c] *= inv;
+        }
+        for (int r = 0; r < n3; ++r) {
+            if (r == col) continue;
+            const double f = A[r][col];
+            if (f == 0.0) continue;
+            for (int c = 0; c < n3; ++c) {
+                A[r][c] -= f * A[col][c];
+                B[r][c] -= f * B[col][c];
+            }
+        }
+    }
+    if (!ok) atomicOr(w.dflags, DF_SINGULAR_DIAG);
+    for (int r = 0; r < n3; ++r)
+        for (int c = 0; c < n3; ++c)
+            reinterpret_cast<float*>(w.dinv)[(size_t)g * n3 * n3 + c * n3 + r] = (float)(ok ? B[r][c] : (r == c ? 1.0 : 0.0));
+}
+
 // One CTA per aggregate a; thread t of a slot s computes entry e = (r, c) of the 6x6 coarse
 // block (a, slot_agg[s]) by summing its Jacobian blocks in list order.
 __global__ void k_coarse_assemble(KrylovWork w, CoarseAssembly ca, const double* __restrict__ pmode,
@@ -1154,6 +1293,13 @@ cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca
         else
             k_coarse_empty<<<(ca.n_empty + 255) / 256, 256, 0, s>>>(a_cm, ca.n_coarse, ca.empty, ca.n_empty);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_jacobi_setup(const KrylovWork& w, int G, cudaStream_t s) {
+    if (G < 2 || G > 4 || w.n_nodes % G != 0) return cudaErrorInvalidValue;
+    const int NG = w.n_nodes / G;
+    if (NG > 0) k_group_jacobi_setup<<<(NG + 127) / 128, 128, 0, s>>>(w, G);
     return cudaGetLastError();
 }
 

@@ -192,6 +192,13 @@ class NewtonRaphsonSolver:
                    "tf_get_preconditioner", self._h)
         return pc.value, nc.value, rf.value
 
+    def smoother_block(self) -> int:
+        """Nodes per block of the block-Jacobi smoother (1: 3x3 node blocks; 3: a prism column of
+        three nodes, 9x9)."""
+        g = ctypes.c_int32()
+        capi.check(self._L.tf_get_smoother_block(self._h, ctypes.byref(g)), "tf_get_smoother_block", self._h)
+        return g.value
+
     def coarse_unknowns(self) -> int:
         return self.preconditioner()[1]
 
