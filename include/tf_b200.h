@@ -81,10 +81,10 @@ typedef struct tf_params {
     int32_t use_graphs;       /* capture the Krylov iteration in a CUDA graph (1) or not    */
     int32_t persistent;       /* whole solve in one cooperative persistent kernel (1) or    */
                               /* graph-replayed chunks of iteration kernels (0)             */
-    int32_t smoother_nodes;   /* block-Jacobi block of a single tissue's persistent solve:  */
-                              /* 0 = a prism column of 2 or 3 nodes when the mesh numbers    */
-                              /* every column's nodes consecutively, else one node; 1 = one */
-                              /* node (3x3); 2-4 = that many consecutive nodes              */
+    int32_t smoother_nodes;   /* block-Jacobi block of the persistent solve: 0 = a prism    */
+                              /* column of 2 or 3 nodes when the mesh numbers every column's */
+                              /* nodes consecutively (in a batch: every tissue), else one   */
+                              /* node; 1 = one node (3x3); 2-4 = that many consecutive nodes */
 } tf_params;
 
 typedef struct tf_step_stats {

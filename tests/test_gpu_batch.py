@@ -40,6 +40,7 @@ def test_batch_matches_single_tissue_runs(precond):
             its_single.append(its)
     with BatchSolver(ts, krylov_rtol=1e-14, precond=pc) as b:
         assert b.preconditioner()[0] == pc
+        assert b.smoother_block() == 2  # every tissue has two node surfaces: two-node columns
         x = b.join([t.x for t in ts])
         its_batch = [[] for _ in ts]
         for _ in range(n_steps):
@@ -110,3 +111,23 @@ def test_sharded_batch_matches_one_batch():
     assert sorted(merged) == list(range(len(ts)))
     for i, t in enumerate(ts):
         assert np.abs(merged[i] - whole[i]).max() <= 1e-9 * t.size
+
+
+def test_batch_node_blocks_match_column_blocks():
+    """The batch with 3x3 node blocks and with two-node column blocks: the same positions within
+    1e-9 of each tissue's size and the same Newton iteration counts."""
+    ts = _tissues()[:4]
+    out = {}
+    for sn in (1, 0):
+        with BatchSolver(ts, krylov_rtol=1e-14, smoother_nodes=sn) as b:
+            assert b.smoother_block() == (1 if sn == 1 else 2)
+            x = b.join([t.x for t in ts])
+            its = []
+            for _ in range(2):
+                x, rc, _ = b.runOneStep(x, ts[0].dt)
+                assert rc == capi.TF_OK
+                its.append(b.tissue_stats()["newton_iters"].tolist())
+            out[sn] = (b.split(x), its)
+    assert out[0][1] == out[1][1]
+    for t, a, c in zip(ts, out[1][0], out[0][0]):
+        assert np.abs(a - c).max() <= 1e-9 * t.size

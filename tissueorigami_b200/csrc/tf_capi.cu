@@ -721,7 +721,7 @@ BatchPlan make_plan(tf_ctx* c) {
     p.ncta = dptr<int32_t>(c->plan_ncta_d);
     p.row0 = dptr<int32_t>(c->plan_row0_d);
     p.active = dptr<int32_t>(c->active_d);
-    p.group = c->T == 1 ? c->smooth_G : 1;
+    p.group = c->smooth_G;
     p.queue = dptr<int32_t>(c->plan_queue_d);
     p.n_queue = (int32_t)c->plan_queue.size();
     p.queue_head = dptr<int32_t>(c->queue_head_d);
@@ -1060,12 +1060,18 @@ int build_batch_coarse(tf_ctx* ctx) {
         int na = std::max(1, (int)std::lround((double)nt / kBatchAggNodes));
         na = std::min(na, std::max(1, nt / 8));
         na = std::min(na, kMaxCoarse / 6);
-        for (int k = 0; k < nt; ++k) agg_nodes[n0 + k] = n0 + k;
-        std::vector<int32_t> cuts;
-        bisect_nodes(X, agg_nodes.data() + n0, nt, na, cuts);
+        // bisect the tissue's smoother groups (whole prism columns with G > 1, so that a column
+        // stays in one aggregate, consecutive in its sorted node list), each by its first node
+        const int G = ctx->smooth_G, ng = nt / G;
+        na = std::min(na, ng);
+        std::vector<int32_t> reps(ng), cuts;
+        for (int k = 0; k < ng; ++k) reps[k] = n0 + k * G;
+        bisect_nodes(X, reps.data(), ng, na, cuts);
         for (int k = 0; k < na; ++k) {
-            std::sort(agg_nodes.begin() + n0 + cuts[k], agg_nodes.begin() + n0 + cuts[k + 1]);
-            agg_ptr.push_back(n0 + cuts[k + 1]);
+            std::sort(reps.begin() + cuts[k], reps.begin() + cuts[k + 1]);
+            for (int q = cuts[k]; q < cuts[k + 1]; ++q)
+                for (int j = 0; j < G; ++j) agg_nodes[n0 + q * G + j] = reps[q] + j;
+            agg_ptr.push_back(n0 + cuts[k + 1] * G);
             agg_tissue.push_back(t);
         }
         tagg0[t + 1] = tagg0[t] + na;
@@ -1696,11 +1702,17 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         if (sn < 0 || sn > 4) return TF_ERR_ARGUMENT;
         if (sn >= 2 && N % sn != 0) return TF_ERR_ARGUMENT;
         ctx->smooth_G = 1;
-        if (ctx->T == 1 && use_persistent(ctx)) {
+        bool even = true;  // every tissue holds whole groups (a batch's tissues share G)
+        for (int t = 0; t < ctx->T && sn >= 2; ++t)
+            even = even && (ctx->tissue_node0[t + 1] - ctx->tissue_node0[t]) % sn == 0;
+        if (!even) return TF_ERR_ARGUMENT;
+        if (use_persistent(ctx)) {
             // auto: columns of two or three nodes (the wing disc's three-node columns cut the
             // iterations by 16 %; the large slab's four-node columns cut none and cost 16 % more
             // time per step, so they keep node blocks unless asked for)
-            const int cs = sn == 0 ? column_size(ctx) : 1;
+            int cs = sn == 0 ? column_size(ctx) : 1;
+            for (int t = 0; t < ctx->T; ++t)
+                if ((ctx->tissue_node0[t + 1] - ctx->tissue_node0[t]) % cs != 0) cs = 1;
             ctx->smooth_G = sn >= 2 ? sn : (cs <= 3 ? cs : 1);
         }
         if (ctx->smooth_G > 1) TF_CK(dalloc(ctx->dinv, sizeof(double) * 9 * (size_t)ctx->smooth_G * N));
@@ -2023,7 +2035,7 @@ int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int3
 
 int tf_get_smoother_block(tf_ctx* ctx, int32_t* nodes) {
     if (!ctx || !nodes) return TF_ERR_ARGUMENT;
-    *nodes = ctx->T == 1 && use_persistent(ctx) ? ctx->smooth_G : 1;
+    *nodes = use_persistent(ctx) ? ctx->smooth_G : 1;
     return TF_OK;
 }
 

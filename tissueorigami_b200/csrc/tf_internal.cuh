@@ -112,8 +112,9 @@ struct BatchPlan {
     const int32_t* ncta;         // [T]
     const int32_t* row0;         // [T+1]
     const int32_t* active;       // [T]
-    // smoother block of a single tissue: G consecutive nodes (a prism column when the mesh numbers
-    // a column's nodes consecutively). G = 1: the node's 3x3 inverse in dinv [N][9]; G > 1: the
+    // smoother block of the persistent solve: G consecutive nodes (a prism column when the mesh
+    // numbers a column's nodes consecutively; a batch's tissues share G, and their aggregates'
+    // node lists hold whole groups). G = 1: the node's 3x3 inverse in dinv [N][9]; G > 1: the
     // inverse of the 3G x 3G diagonal sub-block of group g in FP32, column-major at
     // (float*)dinv + g (3G)^2, computed before the launch and applied one DoF per lane; row
     // ranges and aggregates hold whole groups.

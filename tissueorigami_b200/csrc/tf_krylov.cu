@@ -635,10 +635,38 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
     double* vin = PH == 0 ? w.p : w.s;
     double* out = PH == 0 ? w.phat : w.shat;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int G = plan.group;
     for (int a = a0 + warp; a < a1; a += nw) {
         const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int k = k0 + lane; k < k1; k += 32) {
+        if (G > 1) {
+            // the aggregate's list holds whole smoother groups, each group's nodes consecutive:
+            // one DoF per lane, as in the single-tissue phase
+            const int n3 = 3 * G, gpw = 32 / n3, gl = lane / n3, rr = lane - gl * n3;
+            const int ng = (k1 - k0) / G;
+            for (int q = 0; q < ng; q += gpw) {
+                const bool valid = gl < gpw && q + gl < ng;
+                const int g = plan.agg_nodes[k0 + (valid ? q + gl : q) * G] / G;
+                const double u = group_dof_update_apply<PH>(w, g, rr, n3, valid, alpha, beta, omega, vin, out);
+                if (valid) {
+                    const int n = g * G + rr / 3, i = rr % 3;
+                    const double ui = ((plan.node_mask[n] >> i) & 1) ? u : 0.0;
+                    const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+                    acc[i] += ui;
+                    if (i == 0) {
+                        acc[4] += dz * ui;
+                        acc[5] -= dy * ui;
+                    } else if (i == 1) {
+                        acc[3] -= dz * ui;
+                        acc[5] += dx * ui;
+                    } else {
+                        acc[3] += dy * ui;
+                        acc[4] -= dx * ui;
+                    }
+                }
+            }
+        }
+        for (int k = k0 + lane; G == 1 && k < k1; k += 32) {
             const int n = plan.agg_nodes[k];
             double u[3];
 #pragma unroll
