@@ -89,7 +89,8 @@ struct tf_ctx {
     std::vector<int32_t> t_iters, t_status, t_krylov;
     std::vector<int32_t> last_krylov;  // first-round BiCGStab iterations of each tissue, last step
 
-    // two-level preconditioner (precond == TF_PRECOND_TWO_LEVEL, single tissue, persistent solve)
+    // two-level preconditioner (precond == TF_PRECOND_TWO_LEVEL, persistent solve; the fields
+    // below serve a single tissue, the bc_* ones further down a batch)
     std::vector<uint8_t> h_fixmask;
     bool coarse_dirty = true;
     int coarse_m = 0, n_coarse = 0, n_agg = 0, coarse_lwork = 0, n_coarse_empty = 0;
