@@ -331,7 +331,18 @@ def run_b200(args) -> None:
         bytes_solve = (kry * per_iter + solve_launches * per_setup) / solve_launches
         r_solve = roof("bicgstab_persistent", bytes_solve, solve_ms / solve_launches)
         r_solve["bicgstab_iterations_per_launch"] = kry / solve_launches
-        dominant, other = r_solve, {"element_assemble": r_el, "bsr3_spmv_standalone": r_sp}
+        # the element kernel's own bound is FP64, not HBM: the closed-form tangent costs ~15.2 k
+        # flops per prism (counted from the kernel: ~640 per Gauss point for F, Fe, J, their
+        # inverses and the spatial gradients, 648 for the nodal forces, ~85 per tangent block and
+        # Gauss point for 21 blocks) against ~1.4 kB of algorithmic bytes
+        flops_asm = 15200.0 * E
+        fp64_peak = 37.0  # TFLOP/s: NVIDIA's nominal B200 FP64 figure, not measured here
+        ach_fp64 = flops_asm / (ms_el * 1e-3) / 1e12
+        r_el_fp64 = {"kernel": "element_assemble", "bound": "fp64", "achieved": ach_fp64, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": ach_fp64 / fp64_peak, "peak_source": "nominal (not measured)",
+                     "algorithmic_flops": flops_asm, "ms_per_launch": ms_el}
+        dominant, other = r_solve, {"element_assemble": r_el, "element_assemble_fp64": r_el_fp64,
+                                    "bsr3_spmv_standalone": r_sp}
     else:
         dominant, other = (r_sp, r_el) if share_spmv >= share_el else (r_el, r_sp)
 
