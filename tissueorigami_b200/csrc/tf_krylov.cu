@@ -24,7 +24,6 @@ namespace {
 constexpr int kVecThreads = 256;
 constexpr int kSpmvThreads = 256;
 constexpr int kGroup = 8;  // lanes per block row in the SpMV
-constexpr int kPersistThreadsMax = 768;  // persistent solve: 3 x 256 or 1 x 768 threads per SM
 
 __device__ __forceinline__ bool running(const KrylovScalars* sc) {
     return *reinterpret_cast<const volatile int32_t*>(&sc->status) == KS_RUNNING;
@@ -954,8 +953,13 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     return true;
 }
 
-__global__ void __launch_bounds__(kPersistThreadsMax, 1) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
-                                                                      int max_iter) {
+// Two builds of the persistent solve: one 768-thread CTA per SM (single tissues with the
+// two-level preconditioner, large tissues; up to 80 registers) and four 256-thread CTAs per SM
+// (batches, small block-Jacobi tissues; registers capped at 64 so that 32 warps per SM hide the
+// latency of the memory-bound batched solve).
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
+                                                                        int max_iter) {
 
     __shared__ double smem[32 * 2];
     __shared__ double sb[2];
@@ -1337,22 +1341,27 @@ cudaError_t launch_set_identity(double* m, int n, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+namespace {
+void (*persist_kernel(int threads))(KrylovWork, BatchPlan, double, int) {
+    return threads == 768 ? k_bicgstab_batched<768, 1> : k_bicgstab_batched<256, 4>;
+}
+}  // namespace
+
 int persistent_max_grid(int device, int threads) {
     int sms = 0, occ = 0;
     if (threads != 256 && threads != 768) return 0;
+    const auto kern = persist_kernel(threads);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaFuncSetAttribute(k_bicgstab_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemBytes) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemBytes) != cudaSuccess)
         return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bicgstab_batched, threads, 0) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0) != cudaSuccess) return 0;
     if (threads == 768) {  // the two-level solve adds its coarse row block: still one CTA per SM
         int occ_c = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_bicgstab_batched, threads, kCoarseSmemBytes) !=
-                cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, kern, threads, kCoarseSmemBytes) != cudaSuccess ||
             occ_c < 1)
             return 0;
     }
-    const int want = kPersistThreadsMax / threads;  // the kernel is built for 768 threads per SM
+    const int want = threads == 768 ? 1 : 4;  // the CTAs per SM each build is compiled for
     return sms * (occ < want ? occ : want);
 }
 
@@ -1363,8 +1372,9 @@ cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, 
     void* args[] = {&wc, &pc, &rtol, &max_iter};
     const size_t smem = plan.agg_per_cta > 0 ? sizeof(float) * 6 * plan.agg_per_cta * (size_t)plan.n_coarse : 0;
     if (smem > (size_t)kCoarseSmemBytes) return cudaErrorInvalidValue;
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_bicgstab_batched), dim3(plan.n_cta), dim3(threads),
-                                       args, smem, s);
+    if (threads != 256 && threads != 768) return cudaErrorInvalidValue;
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(persist_kernel(threads)), dim3(plan.n_cta),
+                                       dim3(threads), args, smem, s);
 }
 
 cudaError_t launch_newton_update_batched(const KrylovWork& w, const BatchPlan& plan, double* uk,
