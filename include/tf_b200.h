@@ -85,6 +85,10 @@ typedef struct tf_params {
                               /* column of 2 or 3 nodes when the mesh numbers every column's */
                               /* nodes consecutively (in a batch: every tissue), else one   */
                               /* node; 1 = one node (3x3); 2-4 = that many consecutive nodes */
+    int32_t krylov_refine;    /* tf_solve only: passes of iterative refinement after the      */
+                              /* Krylov solve (FP64 residual g - J du, a second solve for the */
+                              /* correction); 0 = none. The Newton loop needs none: each     */
+                              /* Newton iteration corrects the previous one's solve error    */
 } tf_params;
 
 typedef struct tf_step_stats {
@@ -104,8 +108,9 @@ typedef struct tf_step_stats {
 } tf_step_stats;
 
 /* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), BiCGStab
- * rtol 1e-12 with cap 20000, block-Jacobi, autotuned scatter, device 0, graphs on,
- * persistent solve on. */
+ * rtol 1e-12 with cap 20000, the two-level preconditioner (TF_PRECOND_TWO_LEVEL), autotuned
+ * scatter, device 0, graphs on, persistent solve on, smoother block chosen from the mesh, no
+ * refinement. */
 void tf_default_params(tf_params* p);
 
 /* Library version string. */
@@ -186,16 +191,20 @@ int tf_assemble(tf_ctx* ctx, const double* uk, const double* un, double dt, doub
 
 /* Replaces NewtonRaphsonSolver::solveForDeltaU / solveWithPardiso
  * (NewtonRaphsonSolver.cpp:461-763) including equateSlaveDisplacementsToMasters: solves
- * J du = g with preconditioned BiCGStab on the context's pattern. bsr_vals [nnzb*9],
- * g and du [n_nodes*3]. iters / rel_res may be NULL. */
+ * J du = g with preconditioned BiCGStab on the context's pattern, followed by
+ * params.krylov_refine passes of iterative refinement (Pardiso refines once, iparm[7] = 1).
+ * bsr_vals [nnzb*9], g and du [n_nodes*3]. iters (BiCGStab iterations of every pass) and
+ * rel_res (||g - J du|| / ||g|| of the result; with refinement the true residual) may be NULL. */
 int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, int32_t* iters,
              double* rel_res);
 
 /* Direct alternative to tf_solve, timed beside it: the same J du = g factorised and solved on
- * the GPU by cuSOLVER's sparse Cholesky (QR when Cholesky meets a non-positive pivot), the way
- * the reference refactorises every system with Pardiso (NewtonRaphsonSolver.cpp:498-763).
- * ms_factor_solve receives the device time of factorisation + solve, method 1 (Cholesky) or 2
- * (QR); either may be NULL. Returns TF_KRYLOV_BREAKDOWN when the matrix is singular. */
+ * the GPU by cuSOLVER's sparse Cholesky (QR when Cholesky meets a non-positive pivot and the
+ * system has at most 30,000 unknowns), the way the reference refactorises every system with
+ * Pardiso (NewtonRaphsonSolver.cpp:498-763). ms_factor_solve receives the device time of
+ * factorisation + solve, method 1 (Cholesky) or 2 (QR); either may be NULL. Returns
+ * TF_KRYLOV_BREAKDOWN when the matrix is singular and TF_ERR_UNSUPPORTED when it is not positive
+ * definite and larger than the QR limit. */
 int tf_solve_direct(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du,
                     double* ms_factor_solve, int32_t* method);
 
@@ -262,6 +271,11 @@ int tf_adjoint_forward(tf_ctx* ctx, const double* x0, int32_t n_steps, double dt
 int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drates, double* dL_dx0,
                         tf_step_stats* stats);
 
+/* Measurement hook (no reference counterpart): FP64 FMA throughput of `device` in TFLOP/s (an FMA
+ * counted as two flops), from one CUDA-event-timed launch of independent FMA chains that fill
+ * every SM. The element kernel's own ceiling: its closed-form tangent is compute-bound. */
+int tf_measure_fp64(int32_t device, double* tflops);
+
 /* Text of the last error recorded on the context (no reference counterpart); with ctx = NULL,
  * the reason the calling thread's last tf_create / tf_batch_create failed. */
 const char* tf_last_error(tf_ctx* ctx);
@@ -270,17 +284,23 @@ const char* tf_last_error(tf_ctx* ctx);
  * J du = g) for callers that cannot allocate GPU memory: hosts that give all device memory to
  * their own allocator or to a pool fixed at start-up, and therefore cannot let a library call
  * cudaMalloc / cudaFree. Every pointer is a DEVICE pointer the caller owns: the BSR3 pattern
- * (rowptr [n_nodes+1], colidx [nnzb], every row holding its diagonal block), the values
- * vals [nnzb*9], the right-hand side g and the solution du [n_nodes*3]. The work vectors live
- * in one fixed __device__ array inside the library (about 4.5 MB, held by every GPU that
- * loads the library until the process exits), so n_nodes may not exceed
- * TF_NOALLOC_MAX_NODES; larger systems return TF_ERR_TOO_LARGE before any GPU work. The first
- * call on a device looks up that array's address with cudaGetSymbolAddress (that device must
- * be current) and should come before any stream capture on it. Calls share the array: ones
- * that overlap on the GPU race, so serialise them. stream is a cudaStream_t passed as a
- * pointer (NULL: the legacy default stream); the call returns after the solve has finished.
- * The call makes no cudaMalloc, cudaFree or other allocating call. Returns the status codes
- * of tf_solve; iters / rel_res may be NULL. */
+ * (rowptr [n_nodes+1], colidx [nnzb] with the column indices of each row sorted ascending and
+ * every row holding its diagonal block), the values vals [nnzb*9], the right-hand side g and
+ * the solution du [n_nodes*3]. The work vectors live in one fixed __device__ array inside the
+ * library (about 4.5 MB, held by every GPU where the library's kernels are loaded until the
+ * process exits), so n_nodes may not exceed TF_NOALLOC_MAX_NODES; larger systems return
+ * TF_ERR_TOO_LARGE before any GPU work. Every call looks up that array's address on the
+ * current device with cudaGetSymbolAddress, which allocates nothing. Under CUDA's default lazy
+ * module loading the array is reserved when the library's kernels first load on a device,
+ * inside the first call there: a host whose pool takes all device memory makes one call of
+ * this library on each device before the pool claims it (a reservation that fails returns
+ * TF_ERR_OUT_OF_MEMORY). The call synchronises its stream every 32 iterations to poll
+ * convergence, so it cannot be called while that stream is captured into a CUDA graph. Calls
+ * share the array: ones that overlap on the GPU race, so serialise them. stream is a
+ * cudaStream_t passed as a pointer (NULL: the legacy default stream); the call returns after
+ * the solve has finished. The call makes no cudaMalloc, cudaFree or other allocating call.
+ * Returns the status codes of tf_solve (TF_ERR_ARGUMENT when a row has no diagonal block);
+ * iters / rel_res may be NULL. */
 int tf_solve_bsr_noalloc(int32_t n_nodes, const int32_t* d_rowptr, const int32_t* d_colidx,
                          const double* d_vals, const double* d_g, double* d_du, double rtol,
                          int32_t max_iters, void* stream, int32_t* iters, double* rel_res);

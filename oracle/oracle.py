@@ -52,6 +52,8 @@ def lib():
         L.tfo_assemble_bsr.restype = c_int
         L.tfo_grow.argtypes = [c_int, _I, _D, _D, _D, _D, c_double, _D, _D, _D, _I]
         L.tfo_viscosity_surfaces.argtypes = [c_int, c_int, _I, _D, _U, _U, _D]
+        L.tfo_detect_packing.argtypes = [c_int, c_int, _I, _D, _I, _U, _U, c_int, _I, _D]
+        L.tfo_detect_packing.restype = c_int
         _lib = L
     return _lib
 
@@ -189,6 +191,19 @@ def viscosity_surfaces(t, x):
     return vs
 
 
+def detect_packing(t, x):
+    """Node-node packing candidates at positions x (Simulation::detectPacingNodes): returns
+    (pairs[P,2] int32 in the reference's visiting order, packingThreshold)."""
+    args = (t.n_nodes, t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(x, np.float64)),
+            _i(_c(t.node_placement, np.int32)), _u(_c(t.exposed, np.uint8)), _u(_c(t.peripodial, np.uint8)))
+    thr = ctypes.c_double(0.0)
+    n = lib().tfo_detect_packing(*args, 0, None, ctypes.byref(thr))
+    pairs = np.zeros((max(n, 1), 2), np.int32)
+    if n:
+        lib().tfo_detect_packing(*args, n, _i(pairs), None)
+    return pairs[:n], thr.value
+
+
 def bsr_to_scipy(rowptr, colidx, vals, n_nodes):
     import scipy.sparse as sp
 
@@ -211,11 +226,60 @@ def simulate_dense(t, n_steps=None, max_iter=20, tol=None, threads=0):
     return x, fg, iters, traces
 
 
-def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0):
-    """Simulation::updateStepNR with sparse assembly of J = K^T and SuperLU (scipy) as the
-    direct solve standing in for Pardiso. No slave-master pairs. Returns (x, iterations, norms)."""
+def nested_dissection(t, rowptr, colidx, leaf=128):
+    """Fill-reducing node order for the direct solve: recursive coordinate bisection of the
+    reference positions (split at the median of the longer in-plane side), the nodes of the left
+    half that couple to the right half forming the separator, ordered last. Returns the DoF
+    permutation (3 DoFs of a node kept together)."""
+    import scipy.sparse as sp
+
+    N = t.n_nodes
+    A = sp.csr_matrix((np.ones(colidx.shape[0]), colidx, rowptr), shape=(N, N))
+    X = np.asarray(t.x)
+    order = []
+
+    def rec(nodes):
+        if nodes.shape[0] <= leaf:
+            order.append(nodes)
+            return
+        P = X[nodes, :2]
+        ax = int(np.argmax(P.max(axis=0) - P.min(axis=0)))
+        left = P[:, ax] < np.median(P[:, ax])
+        if left.all() or not left.any():
+            order.append(nodes)
+            return
+        L, R = nodes[left], nodes[~left]
+        in_r = np.zeros(N, bool)
+        in_r[R] = True
+        sep = np.asarray(A[L].multiply(in_r[None, :]).sum(axis=1)).ravel() > 0
+        rec(L[~sep])
+        rec(R)
+        order.append(L[sep])
+
+    rec(np.arange(N))
+    nodes = np.concatenate(order)
+    return (3 * nodes[:, None] + np.arange(3)[None, :]).ravel()
+
+
+def sparse_direct_solve(J, g, perm=None):
+    """Direct solve of J du = g by SuperLU (the Pardiso stand-in of the sparse path); with a
+    fill-reducing DoF permutation the factorisation keeps the natural order of the permuted
+    matrix and prefers diagonal pivots (the matrix is structurally symmetric)."""
     import scipy.sparse.linalg as sla
 
+    if perm is None:
+        return sla.spsolve(J.tocsc(), g)
+    Jp = J.tocsr()[perm][:, perm].tocsc()
+    lu = sla.splu(Jp, permc_spec="NATURAL", options=dict(SymmetricMode=True))
+    du = np.empty_like(g)
+    du[perm] = lu.solve(g[perm])
+    return du
+
+
+def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0, perm=None):
+    """Simulation::updateStepNR with sparse assembly of J = K^T and SuperLU (scipy) as the
+    direct solve standing in for Pardiso. No slave-master pairs. Returns (x, iterations, norms).
+    perm: optional fill-reducing DoF order for the factorisation (nested_dissection)."""
     rowptr, colidx = block_pattern(t)
     un = np.array(x_n, dtype=np.float64, copy=True).reshape(-1, 3)
     uk = un.copy()
@@ -225,8 +289,8 @@ def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter
     tol = float(tol if tol is not None else t.newton_tol)
     while not converged:
         vals, g = assemble_bsr(t, uk, un, visc_surface, inv_fg, rowptr, colidx, dt=dt, threads=threads)
-        J = bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
-        du = sla.spsolve(J, g)
+        J = bsr_to_scipy(rowptr, colidx, vals, t.n_nodes)
+        du = sparse_direct_solve(J, g, perm)
         d = float(np.sqrt(np.sum(du * du)))
         norms.append(d)
         converged = not (d > tol)
@@ -237,15 +301,22 @@ def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter
     return uk, it, np.array(norms)
 
 
-def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0):
-    """n time steps with the growth prologue and the sparse Newton step."""
+def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0, reorder=False, positions=None):
+    """n time steps with the growth prologue and the sparse Newton step. reorder: factorise in
+    nested-dissection order (large meshes). positions: optional list that receives the positions
+    at the start of every step and after the last."""
     x = np.array(t.x, dtype=np.float64, copy=True)
     fg = np.array(t.fg, dtype=np.float64, copy=True)
     iters, traces = [], []
+    perm = nested_dissection(t, *block_pattern(t)) if reorder else None
     for _ in range(n_steps if n_steps is not None else t.n_steps):
+        if positions is not None:
+            positions.append(x.copy())
         fg, inv, _, _ = grow(t, x, fg)
         vs = viscosity_surfaces(t, x)
-        x, it, norms = newton_step_sparse(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads)
+        x, it, norms = newton_step_sparse(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads, perm=perm)
         iters.append(it)
         traces.append(norms)
+    if positions is not None:
+        positions.append(x.copy())
     return x, fg, iters, traces

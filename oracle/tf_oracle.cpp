@@ -861,4 +861,162 @@ void tfo_viscosity_surfaces(int n_nodes, int n_elems, const int32_t* conn, const
     }
 }
 
+int tfo_detect_packing(int n_nodes, int n_elems, const int32_t* conn, const double* x,
+                       const int32_t* node_placement, const uint8_t* exposed, const uint8_t* peripodial,
+                       int max_pairs, int32_t* pairs, double* packing_threshold) {
+    // Simulation::calculateBoundingBox (Simulation.cpp:8388-8425): extent of every node (no node
+    // of these tissues belongs only to explicit-ECM elements; no y-symmetry extension)
+    double bb0[2] = {100000.0, 100000.0}, bb1[2] = {-100000.0, -100000.0};
+    for (int n = 0; n < n_nodes; ++n)
+        for (int d = 0; d < 2; ++d) {
+            const double p = x[(size_t)n * 3 + d];
+            if (p < bb0[d])
+                bb0[d] = p;
+            else if (p > bb1[d])
+                bb1[d] = p;
+        }
+    const double bbs[2] = {bb1[0] - bb0[0], bb1[1] - bb0[1]};
+    // Simulation::getAverageSideLength (Simulation.cpp:3197-3262) with Prism::getApicalSideLengthAverage /
+    // getBasalSideLengthAverage (Prism.cpp:1329-1395): columnar elements only; the 10 x 5 grid
+    // takes, per element, the apical average, or the basal one for basal / whole-tissue elements
+    auto side_avg = [&](const int32_t* c, int o) {
+        const int pr[3][2] = {{o, o + 1}, {o, o + 2}, {o + 1, o + 2}};
+        double dsum = 0.0;
+        int counter = 0;
+        for (int i = 0; i < 3; ++i) {
+            double d2 = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                const double dd = x[(size_t)c[pr[i][0]] * 3 + k] - x[(size_t)c[pr[i][1]] * 3 + k];
+                d2 += dd * dd;
+            }
+            if (d2 > 0) {
+                dsum += std::pow(d2, 0.5);
+                counter++;
+            }
+        }
+        return counter > 0 ? dsum / counter : 0.0;
+    };
+    double grid[10][5] = {{0}}, gcount[10][5] = {{0}};
+    double dsum_col = 0.0;
+    int col_counter = 0;
+    for (int e = 0; e < n_elems; ++e) {
+        if (peripodial && peripodial[e]) continue;  // tissueType 1: the peripodial average is unused here
+        const int32_t* c = conn + (size_t)e * 6;
+        // element tissuePlacement from its exposed surfaces (ShapeBase::setTissuePlacement):
+        // basal (0) when only the basal face is exposed, whole tissue when both are
+        const bool basal_like = (exposed[e] & 2) != 0;
+        double cur = side_avg(c, 3);
+        if (cur > 0) {
+            dsum_col += cur;
+            col_counter++;
+        }
+        if (basal_like) {
+            cur = side_avg(c, 0);
+            if (cur > 0) {
+                dsum_col += cur;
+                col_counter++;
+            }
+        }
+        // ShapeBase::calculateRelativePosInBoundingBox (ShapeBase.cpp:2091-2095): centre relative to the box
+        double cx = 0.0, cy = 0.0;
+        for (int a = 0; a < 6; ++a) {
+            cx += x[(size_t)c[a] * 3 + 0];
+            cy += x[(size_t)c[a] * 3 + 1];
+        }
+        cx /= 6.0;
+        cy /= 6.0;
+        int relX = (int)std::floor((cx - bb0[0]) / bbs[0]);
+        int relY = (int)std::floor(((cy - bb0[1]) / bbs[1]) / 2.0);
+        relX = std::min(9, std::max(0, relX));
+        relY = std::min(4, std::max(0, relY));
+        grid[relX][relY] += cur;
+        gcount[relX][relY]++;
+    }
+    double gridSq[10][5];
+    for (int i = 0; i < 10; ++i)
+        for (int j = 0; j < 5; ++j) {
+            if (gcount[i][j] > 0) grid[i][j] /= gcount[i][j];
+            grid[i][j] *= 0.4;  // Simulation.cpp:8009-8014
+            gridSq[i][j] = grid[i][j] * grid[i][j];
+        }
+    const double col_avg = col_counter > 0 ? dsum_col / col_counter : 0.0;
+    if (packing_threshold) *packing_threshold = 0.4 * col_avg;  // Simulation.cpp:8015
+
+    // Node::checkIfNodeHasPacking (Node.cpp:128-146): apical or basal nodes (none is ablated or
+    // owned by a lateral element here); Node::immediateNeigs = the nodes sharing an element
+    // (ShapeBase::fillNodeNeighbourhood, ShapeBase.cpp:3259-3277)
+    // node -> element lists; two nodes are neighbours when one element holds both (checked only
+    // for the few pairs that are close enough)
+    std::vector<int64_t> eptr((size_t)n_nodes + 1, 0);
+    for (size_t k = 0; k < (size_t)n_elems * 6; ++k) eptr[conn[k] + 1]++;
+    for (int n = 0; n < n_nodes; ++n) eptr[n + 1] += eptr[n];
+    std::vector<int32_t> elist(eptr[n_nodes]);
+    {
+        std::vector<int64_t> fill(eptr.begin(), eptr.end() - 1);
+        for (int e = 0; e < n_elems; ++e)
+            for (int a = 0; a < 6; ++a) elist[fill[conn[(size_t)e * 6 + a]]++] = e;
+    }
+    auto neighbours = [&](int i, int j) {
+        for (int64_t k = eptr[i]; k < eptr[i + 1]; ++k) {
+            const int32_t* c = conn + (size_t)elist[k] * 6;
+            for (int a = 0; a < 6; ++a)
+                if (c[a] == j) return true;
+        }
+        return false;
+    };
+    auto eligible = [&](int n) { return node_placement[n] == 0 || node_placement[n] == 1; };
+    // detectPacingNodes (Simulation.cpp:8036-8070) visits every node pair i < j; the pairs it
+    // keeps are those of one placement, not neighbours, closer than the threshold of the master's
+    // grid cell floor((pos - box min) / box size). The same pairs are found here through a cell
+    // list of the largest threshold, then sorted into the reference's (i, j) visiting order.
+    double tmax = 0.0;
+    for (int i = 0; i < 10; ++i)
+        for (int j = 0; j < 5; ++j) tmax = std::max(tmax, grid[i][j]);
+    std::vector<std::pair<int32_t, int32_t>> found;
+    if (tmax > 0.0) {
+        double lo[3] = {1e300, 1e300, 1e300};
+        for (int n = 0; n < n_nodes; ++n)
+            for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], x[(size_t)n * 3 + d]);
+        auto cell = [&](int n, int d) { return (int64_t)std::floor((x[(size_t)n * 3 + d] - lo[d]) / tmax); };
+        auto key = [](int64_t a, int64_t b, int64_t c) { return (a * 73856093) ^ (b * 19349663) ^ (c * 83492791); };
+        std::vector<std::pair<int64_t, int32_t>> cells;
+        for (int n = 0; n < n_nodes; ++n)
+            if (eligible(n)) cells.push_back({key(cell(n, 0), cell(n, 1), cell(n, 2)), n});
+        std::sort(cells.begin(), cells.end());
+        for (int i = 0; i < n_nodes; ++i) {
+            if (!eligible(i)) continue;
+            int gx = (int)std::floor((x[(size_t)i * 3 + 0] - bb0[0]) / bbs[0]);
+            int gy = (int)std::floor((x[(size_t)i * 3 + 1] - bb0[1]) / bbs[1]);
+            if (gx < 0 || gx > 9 || gy < 0 || gy > 4) continue;  // outside the reference's grid: never met here
+            const double t2 = gridSq[gx][gy];
+            const int64_t c0 = cell(i, 0), c1 = cell(i, 1), c2 = cell(i, 2);
+            for (int64_t a = c0 - 1; a <= c0 + 1; ++a)
+                for (int64_t b = c1 - 1; b <= c1 + 1; ++b)
+                    for (int64_t c = c2 - 1; c <= c2 + 1; ++c) {
+                        const int64_t k = key(a, b, c);
+                        auto it = std::lower_bound(cells.begin(), cells.end(), std::make_pair(k, (int32_t)-1));
+                        for (; it != cells.end() && it->first == k; ++it) {
+                            const int j = it->second;
+                            if (j <= i || node_placement[j] != node_placement[i]) continue;
+                            if (cell(j, 0) != a || cell(j, 1) != b || cell(j, 2) != c) continue;  // hash clash
+                            double d2 = 0.0;
+                            for (int d = 0; d < 3; ++d) {
+                                const double dd = x[(size_t)i * 3 + d] - x[(size_t)j * 3 + d];
+                                d2 += dd * dd;
+                            }
+                            if (d2 < t2 && !neighbours(i, j)) found.push_back({i, j});
+                        }
+                    }
+        }
+        std::sort(found.begin(), found.end());
+    }
+    const int np = (int)found.size();
+    if (pairs)
+        for (int p = 0; p < np && p < max_pairs; ++p) {
+            pairs[2 * p] = found[p].first;
+            pairs[2 * p + 1] = found[p].second;
+        }
+    return np;
+}
+
 }  // extern "C"

@@ -116,6 +116,19 @@ void tfo_viscosity_surfaces(int n_nodes, int n_elems, const int32_t* conn, const
                             const uint8_t* exposed, const uint8_t* peripodial,
                             double* visc_surface);
 
+/* Node-node packing candidates of one time step (Simulation::detectPacingNodes,
+ * Simulation.cpp:7997-8153, with getAverageSideLength :3197-3262 and
+ * Node::checkIfNodeHasPacking, Node.cpp:128-146): apical/basal nodes of the same placement that
+ * share no element and lie closer than 0.4 x the average side length of the threshold grid
+ * cell of the first node. node_placement[N] (0 basal, 1 apical, 2 midline), exposed[E] as in
+ * tfo_viscosity_surfaces. Returns the number of pairs and writes up to max_pairs of them,
+ * (i, j) with i < j in the reference's visiting order, to pairs[2*max_pairs] (may be NULL);
+ * packing_threshold (may be NULL) receives Simulation::packingThreshold = 0.4 x the columnar
+ * average side length. */
+int tfo_detect_packing(int n_nodes, int n_elems, const int32_t* conn, const double* x,
+                       const int32_t* node_placement, const uint8_t* exposed, const uint8_t* peripodial,
+                       int max_pairs, int32_t* pairs, double* packing_threshold);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,45 @@ def test_solve_matches_direct(persistent):
     assert np.all(du[fixed] == 0.0)
 
 
+def _exact_solution(J, g, passes=4):
+    """The FP64-rounded solution of J x = g: SuperLU followed by refinement passes whose residual
+    is summed in extended precision (long double), so the result is limited by rounding only."""
+    J = J.tocsr()
+    lu = sla.splu(J.tocsc())
+    x = lu.solve(g)
+    for _ in range(passes):
+        prod = J.data.astype(np.longdouble) * x.astype(np.longdouble)[J.indices]
+        r = g.astype(np.longdouble) - np.add.reduceat(prod, J.indptr[:-1])
+        x = np.asarray(x.astype(np.longdouble) + lu.solve(np.asarray(r, np.float64)).astype(np.longdouble), np.float64)
+    return x
+
+
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_refined_solve_matches_exact_solution_to_1e12(persistent):
+    """solveForDeltaU to 1e-12 relative. BiCGStab alone stops at ||g - J du|| <= rtol ||g||,
+    which leaves an error up to kappa(J) x rtol in du (kappa_1 ~ 6e4 here, so up to ~1e-8 at
+    rtol 1e-13: the 1e-8 gate of test_solve_matches_direct). One pass of iterative refinement
+    (FP64 residual, a second solve for the correction; Pardiso refines once too) brings du to
+    the rounding level, the accuracy of the direct solve itself: both are compared with the
+    solution refined in extended precision, and with each other, at 1e-12."""
+    t = mesh.small_disc(7, 1500, 1200.0)
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
+    J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes)
+    x_star = _exact_solution(J, g)
+    du_lu = sla.spsolve(J.tocsc(), g)
+    assert np.linalg.norm(du_lu - x_star) / np.linalg.norm(x_star) < 1e-12
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, krylov_refine=2, persistent=persistent) as s:
+        du, rc, iters, rr = s.solveForDeltaU(vals, g)
+    assert rc == capi.TF_OK and rr <= 1e-13
+    assert np.linalg.norm(du - x_star) / np.linalg.norm(x_star) < 1e-12
+    assert np.linalg.norm(du - du_lu) / np.linalg.norm(du_lu) < 1e-12
+    fixed = t.fixed.reshape(-1) != 0
+    assert np.all(du[fixed] == 0.0)
+
+
 def test_newton_step_matches_oracle_small_rectangle():
     t = mesh.small_rectangle()
     fg, inv, _, _ = O.grow(t, t.x, t.fg)

@@ -103,3 +103,83 @@ def test_save_frame_round_trip(tmp_path):
     for (tm, x), (tb, xb, flags, conn) in zip(frames, back):
         assert np.abs(xb - x).max() <= 1e-9 * np.abs(x).max()  # 10 significant digits
         np.testing.assert_array_equal(flags[:, 2], t.at_circumference)
+
+
+def _variant(z, **repl):
+    toks = [str(t) for t in z["modelinput_tokens"]]
+    for key, vals in repl.items():
+        i = toks.index(key)
+        toks[i + 1:i + 1 + len(vals)] = vals
+    return MI.setup(MI.parse(" ".join(toks)), (z["x"], z["place"], z["ttype"], z["circ"], z["conn"], z["xref"]))
+
+
+def _tips(z):
+    basal = np.nonzero((z["place"] == 0) & (z["ttype"] == 0))[0]
+    xs = z["x"][basal, 0]
+    return int(basal[np.argmin(xs)]), int(basal[np.argmax(xs)])
+
+
+def _added(st, base):
+    """The (node, dim) fixes the zero-viscosity rule applied, after checking that every other
+    newly fixed DoF is a bound slave above one of them (binding fixes the slaves of a fixed master,
+    Simulation.cpp:1344-1436, and runs after the rule)."""
+    new = {(int(n), int(d)) for n, d in zip(*np.nonzero(st.tissue.fixed != base.tissue.fixed))}
+    applied = set(st.zero_viscosity_fixes)
+    masters = {(int(m) // 3, int(m) % 3) for _, m in base.tissue.slave_master}
+    slave_of = {(int(s_) // 3, int(s_) % 3): (int(m) // 3, int(m) % 3) for s_, m in base.tissue.slave_master}
+    for nd in new - applied:
+        assert nd in slave_of and slave_of[nd] in applied and slave_of[nd] in masters, nd
+    return sorted(a for a in applied if not base.tissue.fixed[a])
+
+
+def test_zero_external_viscosity_fixes_the_tips_with_y_symmetry():
+    """checkForZeroExternalViscosity (Simulation.cpp:4126-4237): with no drag anywhere and y-symmetry
+    the ventral tip is fixed in x, y and z and the dorsal tip in z."""
+    st0, z = _load()
+    st = _variant(z, **{"DiscProperApicalExternalViscosity:": ["0.0"], "DiscProperBasalExternalViscosity:": ["0.0"]})
+    assert not st.tissue.ext_visc.any()
+    dorsal, ventral = _tips(z)
+    expect = sorted({(ventral, 0), (ventral, 1), (ventral, 2), (dorsal, 2)} - {(n, d) for n, d in zip(*np.nonzero(st0.tissue.fixed))})
+    assert _added(st, st0) == expect
+
+
+def test_zero_external_viscosity_fixes_the_tips_without_symmetry():
+    st0, z = _load()
+    base = _variant(z, **{"symmetricInY(bool):": ["0"]})
+    st = _variant(z, **{"symmetricInY(bool):": ["0"], "DiscProperApicalExternalViscosity:": ["0.0"],
+                       "DiscProperBasalExternalViscosity:": ["0.0"]})
+    dorsal, ventral = _tips(z)
+    third = next(k for k in (1, 2, 3) if k not in (dorsal, ventral))
+    want = {(ventral, 0), (ventral, 1), (ventral, 2), (dorsal, 1), (dorsal, 2), (third, 2)}
+    assert _added(st, base) == sorted(want - {(n, d) for n, d in zip(*np.nonzero(base.tissue.fixed))})
+    # a basal surface fix in z already removes the z rigid motion: no z fixes are added then
+    st_z = _variant(z, **{"symmetricInY(bool):": ["0"], "DiscProperApicalExternalViscosity:": ["0.0"],
+                         "DiscProperBasalExternalViscosity:": ["0.0"], "BasalSurfaceFix(bool-x,y,z):": ["0", "0", "1"]})
+    assert all(d != 2 for _, d in MI.fix_zero_external_viscosity(
+        st_z.tissue.fixed.copy() * 0, st_z.tissue.ext_visc, z["place"], z["ttype"], z["x"],
+        {k: [False, False, k.startswith("BasalSurfaceFix")] for k in (
+            "ApicCircumFix(bool-x,y,z)", "BasalCircumFix(bool-x,y,z)", "LinkerApicCircumFix(bool-x,y,z)",
+            "ApicSurfaceFix(bool-x,y,z)", "BasalSurfaceFix(bool-x,y,z)")}, False))
+
+
+def test_zero_drag_rectangle_is_solvable_only_with_the_tip_fixes():
+    """Without drag in x and y the small rectangle (basal nodes fixed in z) can translate and spin
+    in its plane: the Newton system is singular. The reference's tip fixes make it solvable."""
+    from tissueorigami_b200 import mesh
+
+    t = mesh.small_rectangle(nx=8, ny=5)
+    t.ext_visc[:] = 0.0
+    fixes = {k: [k == "BasalSurfaceFix(bool-x,y,z)" and d == 2 for d in range(3)]
+             for k in ("ApicCircumFix(bool-x,y,z)", "BasalCircumFix(bool-x,y,z)", "LinkerApicCircumFix(bool-x,y,z)",
+                       "ApicSurfaceFix(bool-x,y,z)", "BasalSurfaceFix(bool-x,y,z)")}
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    K, g = O.assemble_dense(t, t.x, t.x, vs, inv)
+    assert np.linalg.matrix_rank(K) < K.shape[0]
+    applied = MI.fix_zero_external_viscosity(t.fixed, t.ext_visc, t.node_placement, np.zeros(t.n_nodes, np.int32), t.x,
+                                             fixes, False)
+    assert sorted(d for _, d in applied) == [0, 1, 1]
+    K, g = O.assemble_dense(t, t.x, t.x, vs, inv)
+    assert np.linalg.matrix_rank(K) == K.shape[0]
+    x, it, norms = O.newton_step_dense(t, t.x, vs, inv)
+    assert np.isfinite(x).all() and norms[-1] <= t.newton_tol

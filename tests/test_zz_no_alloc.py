@@ -68,3 +68,26 @@ def test_noalloc_rejects_systems_beyond_its_scratch():
     L = capi.load()
     rc = L.tf_solve_bsr_noalloc(capi.TF_NOALLOC_MAX_NODES + 1, 16, 16, 16, 16, 16, 1e-12, 10, None, None, None)
     assert rc == capi.TF_ERR_TOO_LARGE
+
+
+def test_noalloc_solve_at_its_maximum_size():
+    """A system of exactly TF_NOALLOC_MAX_NODES block rows (a 128 x 64-node rectangle, two node
+    surfaces, rim clamped) fills every region of the fixed scratch - work vectors, block-Jacobi
+    inverses, diagonal slots and the reduction partials of the widest launch. Two calls in a row
+    on two systems against tf_solve, 1e-8 relative."""
+    L = capi.load()
+    t = mesh.small_rectangle(nx=128, ny=64)
+    t.fixed[t.at_circumference != 0, :] = 1
+    assert t.n_nodes == capi.TF_NOALLOC_MAX_NODES
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    rng = np.random.default_rng(9)
+    x2 = t.x + rng.normal(0.0, 0.01, t.x.shape)
+    systems = [_system(t, t.x, inv), _system(t, x2, inv)]
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, precond=capi.TF_PRECOND_BLOCK_JACOBI) as s:
+        refs = [s.solveForDeltaU(vals, g) for (_, _, vals, g) in systems]
+    for (rowptr, colidx, vals, g), (du_ref, rc_ref, _, _) in zip(systems, refs):
+        assert rc_ref == capi.TF_OK
+        rc, du, iters, rr = _noalloc(L, t.n_nodes, rowptr, colidx, vals, g)
+        assert rc == capi.TF_OK, capi.STATUS_NAMES.get(rc, rc)
+        assert iters > 0 and rr <= 1e-13
+        assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8

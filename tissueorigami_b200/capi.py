@@ -48,7 +48,7 @@ EXPORTS = [
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
-    "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block",
+    "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64",
 ]
 
 
@@ -63,7 +63,7 @@ class Params(ctypes.Structure):
                 ("precond", ctypes.c_int32), ("scatter", ctypes.c_int32),
                 ("elems_per_block", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32),
-                ("smoother_nodes", ctypes.c_int32)]
+                ("smoother_nodes", ctypes.c_int32), ("krylov_refine", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):
@@ -140,6 +140,7 @@ def load(build_if_missing: bool = True):
     L.tf_adjoint_backward.argtypes = [_P, _D, _D, _D, ctypes.POINTER(StepStats)]
     L.tf_solve_direct.argtypes = [_P, _D, _D, _D, _D, _I]
     L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
+    L.tf_measure_fp64.argtypes = [c_int, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:

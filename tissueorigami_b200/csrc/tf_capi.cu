@@ -71,6 +71,7 @@ struct tf_ctx {
     DevBuf rowptr_d, colidx_d, diag_d, vals, colour_list_d;
     DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
     DevBuf fg, rates, angles, exposed, peripodial, rotated, xio, barrier;
+    DevBuf refine_acc, refine_g;  // tf_solve's iterative refinement: accumulated du, saved g
     int persistent_grid_max = 0;  // 0: cooperative launch unavailable
     int persist_threads = 256;    // CTA width of the persistent solve
 
@@ -1536,6 +1537,7 @@ void tf_default_params(tf_params* p) {
     p->use_graphs = 1;
     p->persistent = 1;
     p->smoother_nodes = 0;
+    p->krylov_refine = 0;
 }
 
 const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
@@ -1777,7 +1779,8 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->vals, &ctx->colour_list_d, &ctx->uk, &ctx->un, &ctx->g, &ctx->du, &ctx->r,
                      &ctx->rhat, &ctx->p, &ctx->v, &ctx->s, &ctx->t, &ctx->phat, &ctx->shat, &ctx->dinv,
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
-                     &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier};
+                     &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier,
+                     &ctx->refine_acc, &ctx->refine_g};
     for (DevBuf* b : all) dfree(*b);
     DevBuf* batch[] = {&ctx->plan_queue_d, &ctx->queue_head_d, &ctx->node_tissue_d, &ctx->plan_list_ptr_d,
                        &ctx->plan_list_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d, &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
@@ -1954,7 +1957,49 @@ int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, i
     TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
     rc = krylov_solve(ctx);
     if (rc != TF_OK) return rc;
-    const KrylovScalars sc = *ctx->h_sc;
+    KrylovScalars sc = *ctx->h_sc;
+    int32_t total_iters = sc.iter;
+    double rel = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+    if (ctx->params.krylov_refine > 0 && sc.status == KS_CONVERGED && sc.bb > 0) {
+        // Iterative refinement: r = g - J du in FP64, J d = r solved by the same Krylov solve, du += d.
+        // The solve's relative tolerance bounds the correction's error, so each pass multiplies the
+        // error of du by about kappa(J) x krylov_rtol until the residual reaches rounding level.
+        KrylovWork w = make_work(ctx);
+        TF_CK(dalloc(ctx->refine_acc, bytes));
+        TF_CK(dalloc(ctx->refine_g, bytes));
+        double* acc = dptr<double>(ctx->refine_acc);
+        TF_CK(cudaMemcpyAsync(acc, ctx->du.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->refine_g.p, ctx->g.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        const double bb = sc.bb;
+        for (int k = 0; k < ctx->params.krylov_refine; ++k) {
+            TF_CK(launch_residual(w, acc, dptr<double>(ctx->refine_g), dptr<double>(ctx->g), ctx->stream));
+            ctx->launches += 1;
+            TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+            TF_CK(cudaStreamSynchronize(ctx->stream));
+            const double r2 = ctx->h_sc->du2;
+            rel = std::sqrt(r2 / bb);
+            if (!(r2 > 0.0)) break;  // exact (or non-finite: reported by the next solve's status)
+            rc = krylov_solve(ctx);
+            if (rc != TF_OK) break;
+            const KrylovScalars sk = *ctx->h_sc;
+            total_iters += sk.iter;
+            if (sk.status != KS_CONVERGED) {
+                sc.status = sk.status;
+                break;
+            }
+            TF_CK(launch_axpy(3 * ctx->N, 1.0, dptr<double>(ctx->du), acc, ctx->stream));
+            ctx->launches += 1;
+        }
+        // the refined du, g restored, and the true residual of the result
+        TF_CK(cudaMemcpyAsync(ctx->du.p, acc, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        TF_CK(launch_residual(w, acc, dptr<double>(ctx->refine_g), dptr<double>(ctx->g), ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->g.p, ctx->refine_g.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        TF_CK(cudaMemcpyAsync(ctx->h_sc, ctx->sc.p, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        TF_CK(cudaStreamSynchronize(ctx->stream));
+        ctx->launches += 1;
+        rel = std::sqrt(ctx->h_sc->du2 / bb);
+        if (rc != TF_OK) return rc;
+    }
     if (!ctx->slave.empty()) {
         KrylovWork w = make_work(ctx);
         // equate slaves only (no position update): reuse the update kernel on a scratch vector
@@ -1964,8 +2009,8 @@ int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, i
     }
     TF_CK(cudaMemcpyAsync(du, ctx->du.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     TF_CK(cudaStreamSynchronize(ctx->stream));
-    if (iters) *iters = sc.iter;
-    if (rel_res) *rel_res = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+    if (iters) *iters = total_iters;
+    if (rel_res) *rel_res = rel;
     return krylov_status_to_tf(sc.status);
 }
 
@@ -2142,6 +2187,11 @@ int tf_solve_direct(tf_ctx* ctx, const double* bsr_vals, const double* g, double
                                       &ms, &m);
     if (drc == -3) return set_error(ctx, TF_ERR_OUT_OF_MEMORY, "direct solve: CSR buffers");
     if (drc < 0) return set_error(ctx, TF_ERR_CUDA, "direct solve: cuSOLVER failure");
+    if (ms_factor_solve) *ms_factor_solve = ms;
+    if (method) *method = m;
+    if (drc == 4)
+        return set_error(ctx, TF_ERR_UNSUPPORTED,
+                         "direct solve: J is not positive definite (Cholesky failed) and too large for the QR fallback");
     TF_CK(cudaMemcpyAsync(du, ctx->du.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     TF_CK(cudaStreamSynchronize(ctx->stream));
     if (ms_factor_solve) *ms_factor_solve = ms;

@@ -4,7 +4,11 @@
 // NewtonRaphsonSolver.cpp:498-763). The library's own solve is BiCGStab; this file offers the
 // direct alternative on the GPU for comparison and cross-checks: the BSR3 matrix is expanded to
 // scalar CSR by a kernel and handed to cuSOLVER's sparse Cholesky (J is symmetric on the
-// elastic path), falling back to sparse QR when Cholesky reports a non-positive pivot.
+// elastic path). J is positive definite at rest, but growth against clamped boundaries puts
+// elements in compression, whose geometric stiffness can make J indefinite; Cholesky then meets
+// a non-positive pivot. Sparse QR handles that case but costs ~20x more (80 s on the 180k-unknown
+// wing-disc system), so it runs only up to kQrMaxRows unknowns; larger indefinite systems report
+// "not positive definite".
 #include <cuda_runtime.h>
 #include <cusolverSp.h>
 #include <cusparse.h>
@@ -13,6 +17,8 @@
 
 namespace tfb {
 namespace {
+
+constexpr int kQrMaxRows = 30000;  // largest system the QR fallback takes
 
 // Scalar CSR of a BSR3 matrix: row 3A+i holds, for every block k of block row A (sorted), the
 // columns 3*colidx[k] + j, j = 0..2.
@@ -68,14 +74,20 @@ int direct_solve_bsr3(int32_t n_nodes, int64_t nnzb, const int32_t* rowptr, cons
         const int reorder = 3;  // METIS nested dissection
         cusolverStatus_t st = cusolverSpDcsrlsvchol(h, n, (int)nnz, d, cval, crow, ccol, b, 0.0, reorder, x, &singular);
         *method = 1;
+        bool not_spd = false;
         if (st != CUSOLVER_STATUS_SUCCESS || singular >= 0) {
-            st = cusolverSpDcsrlsvqr(h, n, (int)nnz, d, cval, crow, ccol, b, 0.0, reorder, x, &singular);
-            *method = 2;
+            if (n <= kQrMaxRows) {
+                st = cusolverSpDcsrlsvqr(h, n, (int)nnz, d, cval, crow, ccol, b, 0.0, reorder, x, &singular);
+                *method = 2;
+            } else {
+                not_spd = true;
+            }
         }
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
         cudaEventElapsedTime(ms, e0, e1);
-        if (st != CUSOLVER_STATUS_SUCCESS) rc = -2;
+        if (not_spd) rc = 4;
+        else if (st != CUSOLVER_STATUS_SUCCESS) rc = -2;
         else if (singular >= 0) rc = 3;
     }
     if (e0) cudaEventDestroy(e0);

@@ -192,8 +192,8 @@ cudaError_t launch_set_inv_fg(ElemRecord* elems, int32_t n_elems, const double* 
 cudaError_t launch_mask_fixed(int32_t n_nodes, const uint8_t* fixmask, double* v, cudaStream_t s);
 
 // --- direct solve (tf_direct.cu) -----------------------------------------------------------
-// 0 ok, 3 singular, < 0 CUDA / cuSOLVER failure; ms = factorise + solve time; method 1 = Cholesky,
-// 2 = QR.
+// 0 ok, 3 singular, 4 not positive definite and too large for the QR fallback, < 0 CUDA / cuSOLVER
+// failure; ms = factorise + solve time; method 1 = Cholesky, 2 = QR.
 int direct_solve_bsr3(int32_t n_nodes, int64_t nnzb, const int32_t* rowptr, const int32_t* colidx, const double* vals,
                       const double* b, double* x, cudaStream_t s, float* ms, int* method);
 
@@ -235,6 +235,9 @@ cudaError_t launch_block_jacobi_setup(const KrylovWork& w, cudaStream_t s);
 cudaError_t launch_krylov_init(const KrylovWork& w, double rtol, int max_iter, cudaStream_t s);
 cudaError_t launch_bicgstab_iteration(const KrylovWork& w, cudaStream_t s);
 cudaError_t launch_spmv(const KrylovWork& w, const double* xin, double* yout, cudaStream_t s);
+// rout = b - J x and ||rout||^2 into w.sc->du2 (w.partials holds spmv_grid(N) doubles)
+cudaError_t launch_residual(const KrylovWork& w, const double* xin, const double* b, double* rout, cudaStream_t s);
+cudaError_t launch_axpy(int n, double a, const double* x, double* y, cudaStream_t s);  // y += a x
 cudaError_t launch_newton_update(const KrylovWork& w, double* uk, const int32_t* slaves,
                                  const int32_t* masters, int32_t n_pairs, cudaStream_t s);
 int spmv_grid(int n_nodes);

@@ -278,6 +278,35 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv(KrylovWork w, const doubl
     }
 }
 
+// True residual r = b - J x with ||r||^2 summed in fixed order into sc->du2 (the iterative
+// refinement of tf_solve reads it; the Newton loop does not use this kernel).
+__global__ void __launch_bounds__(kSpmvThreads) k_residual(KrylovWork w, const double* __restrict__ xin,
+                                                           const double* __restrict__ b, double* __restrict__ rout) {
+    const int gl = threadIdx.x & (kGroup - 1);
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    if (row < w.n_nodes) row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+#pragma unroll
+    for (int off = kGroup / 2; off > 0; off >>= 1) {
+        y0 += __shfl_xor_sync(0xffffffffu, y0, off);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, off);
+        y2 += __shfl_xor_sync(0xffffffffu, y2, off);
+    }
+    double v[1] = {0.0}, tot[1];
+    if (row < w.n_nodes && gl == 0) {
+        const double r0 = b[row * 3] - y0, r1 = b[row * 3 + 1] - y1, r2 = b[row * 3 + 2] - y2;
+        rout[row * 3] = r0;
+        rout[row * 3 + 1] = r1;
+        rout[row * 3 + 2] = r2;
+        v[0] = r0 * r0 + r1 * r1 + r2 * r2;
+    }
+    if (grid_sum<1>(v, w.partials, &w.sc->ticket[4], tot) && threadIdx.x == 0) w.sc->du2 = tot[0];
+}
+
+__global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
+}
+
 // Slot of the diagonal block of every block row (binary search of the sorted column list).
 __global__ void k_find_diag(const int32_t* rowptr, const int32_t* colidx, int32_t n, int32_t* diag,
                             int32_t* dflags) {
@@ -1424,6 +1453,16 @@ cudaError_t launch_bicgstab_iteration(const KrylovWork& w, cudaStream_t s) {
 
 cudaError_t launch_spmv(const KrylovWork& w, const double* xin, double* yout, cudaStream_t s) {
     k_spmv<0><<<spmv_grid(w.n_nodes), kSpmvThreads, 0, s>>>(w, xin, yout, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual(const KrylovWork& w, const double* xin, const double* b, double* rout, cudaStream_t s) {
+    k_residual<<<spmv_grid(w.n_nodes), kSpmvThreads, 0, s>>>(w, xin, b, rout);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(int n, double a, const double* x, double* y, cudaStream_t s) {
+    k_axpy<<<vec_grid(n / 3 + 1), kVecThreads, 0, s>>>(n, a, x, y);
     return cudaGetLastError();
 }
 

@@ -13,9 +13,17 @@
 // Limits and rules:
 //   - at most kNoAllocMaxNodes block rows (3 * kNoAllocMaxNodes unknowns); larger systems are
 //     rejected with TF_ERR_TOO_LARGE before any GPU work;
-//   - the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that first call
-//     before any stream capture on the device;
+//   - every call looks up the array's device address on the current device with
+//     cudaGetSymbolAddress (which allocates nothing), so a device reset or a new primary context
+//     never leaves a stale address behind. Under CUDA's lazy module loading the array is reserved
+//     when the library's kernels first load on a device, which is inside the first call there:
+//     a host whose pool takes all device memory must make one call (or any other call of this
+//     library) before its pool claims the memory; a failed reservation returns
+//     TF_ERR_OUT_OF_MEMORY;
+//   - the column indices of each block row must be sorted ascending (the diagonal block is
+//     found by binary search);
+//   - the call synchronises its stream after every 32 iterations to poll convergence, so it
+//     cannot be called while that stream is being captured into a CUDA graph;
 //   - every call on a device shares the one array, which keeps the previous call's contents:
 //     the call clears the parts that must start at zero (scalars, tickets, flags) itself, and
 //     calls that overlap on the GPU (two streams, two host threads) race on it.
@@ -25,7 +33,6 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "../../include/tf_b200.h"
 #include "tf_internal.cuh"
@@ -47,20 +54,14 @@ static_assert(sizeof(KrylovScalars) % 8 == 0, "scalar block must be a whole numb
 // The scratch: 8 work vectors | Dinv | diag slots | partials | scalars + flags.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-double* g_scratch_addr[kMaxDevices] = {nullptr};
-std::mutex g_setup_mutex;
-
-// Device address of the scratch array on the current device (looked up once per device).
-cudaError_t scratch_address(int dev, double** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (err != cudaSuccess) return err;
-        g_scratch_addr[dev] = static_cast<double*>(p);
-    }
-    *out = g_scratch_addr[dev];
+// Device address of the scratch array in the current device's context. Looked up on every call:
+// the lookup allocates nothing, and an address cached across calls would go stale once the
+// context is destroyed and made again (cudaDeviceReset), when the module reloads elsewhere.
+cudaError_t scratch_address(double** out) {
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess) return err;
+    *out = static_cast<double*>(p);
     return cudaSuccess;
 }
 
@@ -81,12 +82,11 @@ extern "C" int tf_solve_bsr_noalloc(int32_t n_nodes, const int32_t* d_rowptr, co
     if (n_nodes > kNoAllocMaxNodes) return TF_ERR_TOO_LARGE;
     if (n_nodes <= 0 || !d_rowptr || !d_colidx || !d_vals || !d_g || !d_du || max_iters <= 0 || !(rtol >= 0))
         return TF_ERR_ARGUMENT;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TF_ERR_CUDA;
     double* base = nullptr;
-    if (scratch_address(dev, &base) != cudaSuccess) {
+    const cudaError_t serr = scratch_address(&base);
+    if (serr != cudaSuccess) {
         cudaGetLastError();
-        return TF_ERR_CUDA;
+        return serr == cudaErrorMemoryAllocation ? TF_ERR_OUT_OF_MEMORY : TF_ERR_CUDA;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 

@@ -18,7 +18,9 @@ so the reference's own inputs run unchanged:
 * Young's modulus by placement (Prism::setElasticProperties, Prism.cpp:464-510), Lame parameters
   lambda = E v / (1 + v) / (1 - 2 v), mu = E / 2 / (1 + v); internal viscosity by placement
   (ShapeBase::setViscosity, ShapeBase.cpp:1089-1101);
-* external viscosity per node (Node::setExternalViscosity, Node.cpp:63-110);
+* external viscosity per node (Node::setExternalViscosity, Node.cpp:63-110), then the fixes the
+  reference adds in a direction where no node has drag (checkForZeroExternalViscosity,
+  Simulation.cpp:4126-4237, with the tips of assignTips, Simulation.cpp:8165-8182);
 * circumference x, y binding to the basal node of each column, with a fixed master fixing its
   slaves instead (Simulation::bindCircumferenceXY, Simulation.cpp:1344-1436);
 * exposed surfaces by element placement (Prism::assignExposedSurfaceAreaIndices,
@@ -104,6 +106,7 @@ class ReferenceSetup:
     ecm: np.ndarray
     actin: np.ndarray
     not_modelled: List[str]
+    zero_viscosity_fixes: List[Tuple[int, int]] = dataclasses.field(default_factory=list)
 
     def growth_at(self, t: float) -> Tuple[np.ndarray, np.ndarray]:
         """Per-element growth rates and angles applied by the step that starts at time t."""
@@ -162,6 +165,66 @@ def _element_placement(conn, node_place):
         elif (p == APICAL_BULK).any():
             place[e] = APICAL_BULK
     return place, spans
+
+
+def assign_tips(node_place, node_type, x) -> Tuple[int, int]:
+    """Simulation::assignTips (Simulation.cpp:8165-8182): the dorsal / ventral tips are the basal
+    columnar nodes of smallest / largest x (the first such node on ties); 0 and 1 when there are
+    none (the Simulation constructor's values, Simulation.cpp:132-133). Returns (dorsal, ventral)."""
+    dorsal, ventral = 0, 1
+    lo, hi = 10000.0, -10000.0
+    for i in np.nonzero((node_place == BASAL) & (node_type == 0))[0]:
+        if x[i, 0] < lo:
+            dorsal, lo = int(i), x[i, 0]
+        if x[i, 0] > hi:
+            ventral, hi = int(i), x[i, 0]
+    return dorsal, ventral
+
+
+def fix_zero_external_viscosity(fixed, ext_visc, node_place, node_type, x, fixes, symmetric_y: bool):
+    """Simulation::checkForZeroExternalViscosity (Simulation.cpp:4126-4237), in place on fixed[N,3].
+
+    A direction in which no node feels external drag leaves the tissue free to translate (and
+    rotate) rigidly, so the Newton system is singular unless something else fixes it. Unless the
+    apical, basal or linker-apical circumference fixing (CircumferentialNodeFix[0..2]; the
+    whole-circumference option [4] is not consulted) or the apical / basal surface fixing already
+    fixes that direction, the reference fixes the ventral tip in it, the dorsal tip in y and z,
+    and a third node (node 1, else 2, else 3) in z; with y-symmetry the ventral tip in x (if
+    needed) and y, both tips in z. Returns the (node, dim) fixes it applied."""
+    zero = [not (ext_visc[:, d] > 0).any() for d in range(3)]
+    applied = []
+    if not any(zero):
+        return applied
+    circ = [fixes["ApicCircumFix(bool-x,y,z)"], fixes["BasalCircumFix(bool-x,y,z)"],
+            fixes["LinkerApicCircumFix(bool-x,y,z)"]]
+    apical, basal = fixes["ApicSurfaceFix(bool-x,y,z)"], fixes["BasalSurfaceFix(bool-x,y,z)"]
+    sufficient = [(not zero[d]) or any(c[d] for c in circ) or basal[d] or apical[d] for d in range(3)]
+    dorsal, ventral = assign_tips(node_place, node_type, x)
+
+    def fix(n, d):
+        fixed[n, d] = 1
+        applied.append((int(n), d))
+
+    if not symmetric_y:
+        for d in range(3):
+            if not sufficient[d]:
+                fix(ventral, d)
+        if not sufficient[1]:
+            fix(dorsal, 1)
+        if not sufficient[2]:
+            fix(dorsal, 2)
+            for third in (1, 2, 3):
+                if dorsal != third and ventral != third:
+                    fix(third, 2)
+                    break
+    else:
+        if not sufficient[0]:
+            fix(ventral, 0)
+        fix(ventral, 1)
+        if not sufficient[2]:
+            fix(ventral, 2)
+            fix(dorsal, 2)
+    return applied
 
 
 def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSetup:
@@ -275,6 +338,8 @@ def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSet
     if extend:
         ev[rest & ~circ & np.isin(node_place, [MID, LATERAL, APICAL_BULK])] = min(v_ap, v_ba)
     ext_visc = np.repeat(ev[:, None], 3, axis=1)
+    zero_visc_fixes = fix_zero_external_viscosity(fixed, ext_visc, node_place, np.asarray(node_type), x, fixes,
+                                                  m.flag("symmetricInY(bool)"))
 
     # circumference binding: x, y of every node above a basal circumference node to that node
     pairs = []
@@ -336,7 +401,7 @@ def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSet
     tissue = Tissue("modelinput", conn, np.asarray(xref, np.float64), x, lam, mu, eta, fixed, ext_visc, exposed,
                     np.zeros(E, np.uint8), np.zeros((E, 3)), np.zeros(E), node_place, circ.astype(np.int32),
                     slave_master=slave_master, dt=float(dt), n_steps=int(round(length / dt)), newton_tol=1e-8)
-    return ReferenceSetup(tissue, growth, place, ecm, actin, not_modelled)
+    return ReferenceSetup(tissue, growth, place, ecm, actin, not_modelled, zero_visc_fixes)
 
 
 def load(modelinput_path: str, mesh_path: Optional[str] = None) -> ReferenceSetup:
