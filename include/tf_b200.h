@@ -219,6 +219,43 @@ int tf_set_growth(tf_ctx* ctx, const double* fg, const double* rates, const doub
 /* Read back the device growth state: fg and inv_fg [n_elems*9] (either may be NULL). */
 int tf_get_growth(tf_ctx* ctx, double* fg, double* inv_fg);
 
+/* One grid-based growth function (growth type 3, GridBasedGrowthFunction,
+ * GrowthFunctionTypes.h:269-548), with the values the reference holds after reading its input
+ * (ModelInputObject::readGrowthType3, ModelInputObject.cpp:684-866). */
+typedef struct tf_grid_growth {
+    double t0, t1;        /* active in steps that start at t with t0 <= t < t1 (InitialTime,    */
+                          /* FinalTime; read into float by the reference)                       */
+    int32_t nx, ny;       /* grid points (nGridX, nGridY), each >= 2                             */
+    const double* rates;  /* [nx*ny*3] growth rate in 1/s of grid point (i, j), axis k at       */
+                          /* (i*ny + j)*3 + k (GrowthMatrix: the file's per-hour values / 3600) */
+    const double* angles; /* [nx*ny] orientation of grid point (i, j) in degrees, at i*ny + j    */
+    double z_min, z_max;  /* zRange: applies where initialRelativePositionInZ is in the range    */
+    int32_t flags;        /* bit0 ApplyToColumnarLayer, bit1 ApplyToPeripodialMembrane,          */
+                          /* bit2 ApplyToBasalECM, bit3 ApplyToLateralECM                       */
+    int32_t reserved;
+} tf_grid_growth;
+
+/* Replaces the grid-based branch of Simulation::calculateGrowth (calculateGrowthGridBased,
+ * Simulation.cpp:9038-9085, with ShapeBase::calculateFgFromGridCorners, ShapeBase.cpp:513-658, and
+ * convertRelativePosToGridIndex, :834-860) for grids pinned on the initial mesh
+ * (GridGrowthsPinnedOnInitialMesh). In every time step the functions active at the context's
+ * simulation time (tf_set_time; each tf_time_step advances it by dt) give each element an
+ * increment - nearest grid corner (interpolation 0) or bilinear rates and orientation
+ * (interpolation 1) - composed in list order after the uniform increment of tf_set_growth.
+ * Per element: rel_pos [n_elems*2] the pinned position relative to the tissue's bounding box
+ * (ShapeBase::initialRelativePosInBoundingBox), rel_z [n_elems] initialRelativePositionInZ
+ * (0 apical, 1 basal), elem_flags [n_elems] bit0 ECM-mimicking, bit1 actin-mimicking (no growth
+ * in height), bit2 basal placement, bit3 ECM at the circumference, bits 4-5 tissue type
+ * (0 columnar, 1 peripodial). n_funcs = 0 removes the grid functions. At most 8 may be active
+ * in one step (TF_ERR_UNSUPPORTED). */
+int tf_set_grid_growth(tf_ctx* ctx, int32_t n_funcs, const tf_grid_growth* funcs, int32_t interpolation,
+                       const double* rel_pos, const double* rel_z, const int32_t* elem_flags);
+
+/* Simulation::currSimTimeSec: the time at the start of the next step (starts at 0); it selects the
+ * grid growth functions of a step. tf_time_step and tf_time_step_device add dt to it. */
+int tf_set_time(tf_ctx* ctx, double t);
+int tf_get_time(tf_ctx* ctx, double* t);
+
 /* One full time step of the path, replacing the part of Simulation::runOneStep that feeds
  * and runs the Newton step (Simulation.cpp:6008-6112): CalculateGrowthRotationByF,
  * calculateGrowth (uniform-type rates), growShapeByFg, updateNodeViscositySurfaces, then

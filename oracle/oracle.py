@@ -50,7 +50,9 @@ def lib():
         L.tfo_block_pattern.restype = c_int
         L.tfo_assemble_bsr.argtypes = [c_int, c_int, _I, _D, _D, _D, _D, _D, _D, _D, c_double, _U, _D, _D, _I, _I, _D, _D, c_int]
         L.tfo_assemble_bsr.restype = c_int
-        L.tfo_grow.argtypes = [c_int, _I, _D, _D, _D, _D, c_double, _D, _D, _D, _I]
+        L.tfo_grow.argtypes = [c_int, _I, _D, _D, _D, _D, c_double, _D, _D, _D, _I, _D]
+        L.tfo_grid_growth_increments.argtypes = [c_int, c_int, _I, _D, _D, _D, _D, _I, c_int, _D, _D, _I, c_double,
+                                                 c_double, _D, _D]
         L.tfo_viscosity_surfaces.argtypes = [c_int, c_int, _I, _D, _U, _U, _D]
         L.tfo_detect_packing.argtypes = [c_int, c_int, _I, _D, _I, _U, _U, c_int, _I, _D]
         L.tfo_detect_packing.restype = c_int
@@ -172,16 +174,40 @@ def assemble_bsr(t, uk, un, visc_surface, inv_fg, rowptr, colidx, dt=None, threa
     return vals, g
 
 
-def grow(t, x, fg, dt=None):
-    """One step of the growth prologue. Returns (fg_new[E,9], inv_fg[E,9], det_fg[E], rotated[E])."""
+def grow(t, x, fg, dt=None, grid_inc=None):
+    """One step of the growth prologue. grid_inc[E,9]: optional increments of grid-based growth
+    functions (grid_growth_increments), applied after the uniform one.
+    Returns (fg_new[E,9], inv_fg[E,9], det_fg[E], rotated[E])."""
     fg = np.array(fg, dtype=np.float64, copy=True).reshape(-1, 9)
     inv = np.zeros_like(fg)
     det = np.zeros(t.n_elems)
     rot = np.zeros(t.n_elems, np.int32)
+    gi = None if grid_inc is None else _c(grid_inc, np.float64).reshape(-1, 9)
     lib().tfo_grow(t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(t.xref, np.float64)), _d(_c(x, np.float64)),
                    _d(_c(t.rates, np.float64)), _d(_c(t.angles, np.float64)), float(dt if dt is not None else t.dt),
-                   _d(fg), _d(inv), _d(det), _i(rot))
+                   _d(fg), _d(inv), _d(det), _i(rot), _d(gi))
     return fg, inv, det, rot
+
+
+def grid_growth_increments(funcs, rel_pos, rel_z, eflags, interpolation, t_now, dt, per_function=False):
+    """Composed increments [E,9] of the grid-based growth functions active at t_now. funcs: list of
+    dicts with nx, ny, rates[nx,ny,3] (1/s), angles_deg[nx,ny], t0, t1, zmin, zmax, flags.
+    per_function: also return (applied[F,E] bool, increment[F,E,9]) of each function on its own."""
+    E = rel_z.shape[0]
+    dims = np.array([[f["nx"], f["ny"]] for f in funcs], np.int32).reshape(-1)
+    rates = np.concatenate([np.asarray(f["rates"], np.float64).reshape(-1) for f in funcs])
+    angs = np.concatenate([np.asarray(f["angles_deg"], np.float64).reshape(-1) for f in funcs])
+    win = np.array([[f["t0"], f["t1"]] for f in funcs], np.float64).reshape(-1)
+    zr = np.array([[f["zmin"], f["zmax"]] for f in funcs], np.float64).reshape(-1)
+    fl = np.array([f["flags"] for f in funcs], np.int32)
+    inc = np.zeros((E, 9))
+    pf = np.zeros((len(funcs), E, 10)) if per_function else None
+    lib().tfo_grid_growth_increments(E, len(funcs), _i(dims), _d(rates), _d(angs), _d(win), _d(zr), _i(fl),
+                                     int(interpolation), _d(_c(rel_pos, np.float64)), _d(_c(rel_z, np.float64)),
+                                     _i(_c(eflags, np.int32)), float(t_now), float(dt), _d(inc), _d(pf))
+    if per_function:
+        return inc, pf[:, :, 0] != 0, pf[:, :, 1:]
+    return inc
 
 
 def viscosity_surfaces(t, x):

@@ -736,7 +736,7 @@ int tfo_assemble_bsr(int n_nodes, int n_elems, const int32_t* conn, const double
 
 void tfo_grow(int n_elems, const int32_t* conn, const double* xref, const double* x,
               const double* rates, const double* angles, double dt, double* fg, double* inv_fg,
-              double* det_fg, int32_t* rotated) {
+              double* det_fg, int32_t* rotated, const double* grid_inc) {
     const GaussRule& R = rule();
     for (int e = 0; e < n_elems; ++e) {
         double x18[18];
@@ -800,6 +800,12 @@ void tfo_grow(int n_elems, const int32_t* conn, const double* xref, const double
         // updateGrowthIncrement on a fresh identity (cleanUpGrowthRates, Sim.cpp:8678-8683)
         const M3 I3 = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
         matmul3(inc, I3, growthInc);
+        if (grid_inc) {  // the grid-based functions of the step, applied after the uniform one
+            M3 gi;
+            std::memcpy(gi, grid_inc + (size_t)e * 9, sizeof(M3));
+            matmul3(gi, growthInc, tmp);
+            std::memcpy(growthInc, tmp, sizeof(M3));
+        }
         // growShapeByFg (ShapeBase.cpp:1452-1506)
         if (rot) {
             matmul3_tn(GrowthStrainsRotMat, growthInc, tmp);
@@ -858,6 +864,205 @@ void tfo_viscosity_surfaces(int n_nodes, int n_elems, const int32_t* conn, const
             const double A = area(c, ba[0], ba[1], ba[2]);
             for (int i = 0; i < 3; ++i) visc_surface[c[ba[i]]] += A / 3;
         }
+    }
+}
+
+void tfo_grid_growth_increments(int n_elems, int n_funcs, const int32_t* dims, const double* rates,
+                                const double* angles_deg, const double* windows, const double* zrange,
+                                const int32_t* fflags, int interpolation, const double* rel_pos,
+                                const double* rel_z, const int32_t* eflags, double t, double dt, double* inc,
+                                double* per_func) {
+    // GridBasedGrowthFunction (GrowthFunctionTypes.h:269-548): per function, the corner tables of
+    // every grid cell with the angles brought next to each other (preCalculateAnglesForCompatibleAveraging)
+    struct Cell {
+        double g[4][3], a[4];
+        bool elim[4];
+    };
+    std::vector<std::vector<Cell>> cells(n_funcs);
+    size_t off = 0;
+    for (int f = 0; f < n_funcs; ++f) {
+        const int nx = dims[2 * f], ny = dims[2 * f + 1];
+        const double* G = rates + 3 * off;
+        const double* A = angles_deg + off;
+        off += (size_t)nx * ny;
+        auto gm = [&](int i, int j, int k) { return G[((size_t)i * ny + j) * 3 + k]; };
+        auto ang = [&](int i, int j) { return A[(size_t)i * ny + j] * M_PI / 180.0; };
+        auto ar_over = [&](int i, int j) {  // aspect ratio x / y against the 1.1 threshold
+            double AR = gm(i, j, 0) / gm(i, j, 1);
+            if (AR < 0) AR *= -1.0;
+            if (AR < 1.0) AR = 1 / AR;
+            return !(AR < 1.1);
+        };
+        cells[f].assign((size_t)(nx - 1) * (ny - 1), Cell());
+        for (int IX = 0; IX < nx - 1; ++IX)
+            for (int IY = 0; IY < ny - 1; ++IY) {
+                Cell& c = cells[f][(size_t)IX * (ny - 1) + IY];
+                const int ci[4][2] = {{IX, IY}, {IX + 1, IY}, {IX, IY + 1}, {IX + 1, IY + 1}};
+                double angles[4] = {0, 0, 0, 0};
+                bool elim[4] = {false, false, false, false};
+                for (int q = 0; q < 4; ++q) {
+                    for (int k = 0; k < 3; ++k) c.g[q][k] = gm(ci[q][0], ci[q][1], k);
+                    if (ar_over(ci[q][0], ci[q][1]))
+                        angles[q] = ang(ci[q][0], ci[q][1]);
+                    else
+                        elim[q] = true;
+                }
+                for (int q = 0; q < 4; ++q) {
+                    while (angles[q] < 0) angles[q] += M_PI;
+                    while (angles[q] > M_PI) angles[q] -= M_PI;
+                }
+                // the base angle: the first corner that was not eliminated; adjustment starts there
+                bool selected = false;
+                int sel = 3;
+                double tet = 0;
+                for (int q = 0; q < 4; ++q) {
+                    if (!elim[q] && !selected) {
+                        tet = angles[q];
+                        selected = true;
+                    }
+                    if (selected) {
+                        sel = q;
+                        break;
+                    }
+                }
+                bool flip[4] = {false, false, false, false};
+                for (int q = sel; q < 4; ++q) {
+                    const double d = angles[q] - tet;
+                    if (d > 0) {
+                        if (d >= M_PI / 4.0 && d < 3.0 * M_PI / 4.0) {
+                            angles[q] -= M_PI / 2.0;
+                            flip[q] = true;
+                        } else if (d >= 3.0 * M_PI / 4.0 && d < 5.0 * M_PI / 4.0) {
+                            angles[q] -= M_PI;
+                        } else if (d >= 5.0 * M_PI / 4.0 && d < 7.0 * M_PI / 4.0) {
+                            angles[q] -= 6.0 * M_PI / 4.0;
+                            flip[q] = true;
+                        } else if (d >= 7.0 * M_PI / 4.0) {
+                            angles[q] -= 2.0 * M_PI;
+                        }
+                    } else if (d < 0) {
+                        if (d <= -M_PI / 4.0 && d > -3.0 * M_PI / 4.0) {
+                            angles[q] += M_PI / 2.0;
+                            flip[q] = true;
+                        } else if (d <= -3.0 * M_PI / 4.0 && d > -5.0 * M_PI / 4.0) {
+                            angles[q] += M_PI;
+                        } else if (d <= -5.0 * M_PI / 4.0 && d > -7.0 * M_PI / 4.0) {
+                            angles[q] += 6.0 * M_PI / 4.0;
+                            flip[q] = true;
+                        } else if (d <= -7.0 * M_PI / 4.0) {
+                            angles[q] += 2.0 * M_PI;
+                        }
+                    }
+                }
+                for (int q = 0; q < 4; ++q) {
+                    if (flip[q]) std::swap(c.g[q][0], c.g[q][1]);
+                    c.a[q] = angles[q];
+                    c.elim[q] = elim[q];
+                }
+            }
+    }
+    const M3 I3 = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int e = 0; e < n_elems; ++e) {
+        M3 growthInc;
+        std::memcpy(growthInc, I3, sizeof(M3));
+        const int ef = eflags[e];
+        const bool ecm = ef & 1, actin = ef & 2, basal = ef & 4, ecm_circ = ef & 8;
+        const int ttype = (ef >> 4) & 3;
+        for (int f = 0; f < n_funcs; ++f) {
+            // Simulation::calculateGrowthGridBased (Simulation.cpp:9038-9085): active on [t0, t1)
+            if (!(t >= windows[2 * f] && t < windows[2 * f + 1])) continue;
+            const int nx = dims[2 * f], ny = dims[2 * f + 1];
+            // ShapeBase::convertRelativePosToGridIndex (ShapeBase.cpp:834-860)
+            double rp0 = rel_pos[2 * e] * (float)(nx - 1), rp1 = rel_pos[2 * e + 1] * (float)(ny - 1);
+            int IX = (int)std::floor(rp0), IY = (int)std::floor(rp1);
+            double FX = rp0 - IX, FY = rp1 - IY;
+            if (IX >= nx - 1) {
+                IX = nx - 2;
+                FX = 1.0;
+            } else if (IX < 0) {
+                IX = 0;
+                FX = 0.0;
+            }
+            if (IY >= ny - 1) {
+                IY = ny - 2;
+                FY = 1.0;
+            } else if (IY < 0) {
+                IY = 0;
+                FY = 0.0;
+            }
+            const Cell& c = cells[f][(size_t)IX * (ny - 1) + IY];
+            // ShapeBase::calculateFgFromGridCorners (ShapeBase.cpp:513-658) into a fresh identity
+            bool applied = false;
+            auto corner_increment = [&](int source, M3 out) {
+                std::memcpy(out, I3, sizeof(M3));
+                // isGrowthRateApplicable (ShapeBase.cpp:297-334); columnar and peripodial elements
+                // only (linker elements, with their transition weights, are not built here)
+                if (rel_z[e] < zrange[2 * f] || rel_z[e] > zrange[2 * f + 1]) return;
+                const double weight = 1.0;
+                if (!((source == 0 && ttype == 0) || (source == 1 && ttype == 1))) return;
+                applied = true;
+                double growth[3] = {0.0, 0.0, 0.0};
+                double angle = 0;
+                if (interpolation == 0) {
+                    const int q = FX > 0.5 ? (FY > 0.5 ? 3 : 1) : (FY > 0.5 ? 2 : 0);
+                    for (int k = 0; k < 3; ++k) growth[k] = c.g[q][k];
+                } else {
+                    double elimFrac = 0.0;
+                    if (c.elim[0]) elimFrac += (1.0 - FX) * (1.0 - FY);
+                    if (c.elim[1]) elimFrac += FX * (1.0 - FY);
+                    if (c.elim[2]) elimFrac += (1.0 - FX) * FY;
+                    if (c.elim[3]) elimFrac += FX * FY;
+                    angle = c.a[0] * (1.0 - FX) * (1.0 - FY) + c.a[1] * FX * (1.0 - FY) + c.a[2] * (1.0 - FX) * FY +
+                            c.a[3] * FX * FY;
+                    if (elimFrac > 0) {
+                        if (elimFrac >= 0.9999999)
+                            angle = 0.0;
+                        else
+                            angle /= (1.0 - elimFrac);
+                    }
+                    for (int k = 0; k < 3; ++k) {
+                        growth[k] = c.g[0][k] * (1.0 - FX) * (1.0 - FY) + c.g[1][k] * FX * (1.0 - FY) +
+                                    c.g[2][k] * (1.0 - FX) * FY + c.g[3][k] * FX * FY;
+                        growth[k] *= weight;
+                    }
+                }
+                if (actin) growth[2] = 0;  // actin-mimicking elements do not grow in height
+                for (int k = 0; k < 3; ++k) out[k][k] = std::exp(growth[k] * dt);
+                if (angle != 0.0) {
+                    const double cs = std::cos(angle), sn = std::sin(angle);
+                    const M3 R = {{cs, -1.0 * sn, 0.0}, {sn, cs, 0.0}, {0.0, 0.0, 1.0}};
+                    M3 tmp;
+                    matmul3(R, out, tmp);
+                    matmul3_nt(tmp, R, out);
+                }
+            };
+            const int fl = fflags[f];
+            M3 col, per, tmp;
+            std::memcpy(col, I3, sizeof(M3));
+            std::memcpy(per, I3, sizeof(M3));
+            if (fl & 12) {  // apply to basal / lateral ECM
+                if ((fl & 4) && ecm && basal) corner_increment(0, col);
+                if ((fl & 8) && ecm_circ && !basal) corner_increment(0, col);
+            }
+            if (!ecm) {
+                if (fl & 1) corner_increment(0, col);
+                if (fl & 2) corner_increment(1, per);
+            }
+            if (per_func) {  // this function's own increment (1 + 9 doubles: applied flag, matrix)
+                double* o = per_func + ((size_t)f * n_elems + e) * 10;
+                o[0] = applied ? 1.0 : 0.0;
+                std::memcpy(o + 1, ttype == 1 ? per : col, sizeof(M3));
+            }
+            // ShapeBase::updateGrowthIncrement (ShapeBase.cpp:764-787)
+            if (ttype == 0) {
+                matmul3(col, growthInc, tmp);
+                std::memcpy(growthInc, tmp, sizeof(M3));
+            } else if (ttype == 1) {
+                matmul3(per, growthInc, tmp);
+                std::memcpy(growthInc, tmp, sizeof(M3));
+            }
+        }
+        std::memcpy(inc + (size_t)e * 9, growthInc, sizeof(M3));
     }
 }
 

@@ -107,7 +107,28 @@ int tfo_assemble_bsr(int n_nodes, int n_elems, const int32_t* conn, const double
  * rotated[E] (may be NULL) receives the rotatedGrowth flag. */
 void tfo_grow(int n_elems, const int32_t* conn, const double* xref, const double* x,
               const double* rates, const double* angles, double dt, double* fg, double* inv_fg,
-              double* det_fg, int32_t* rotated);
+              double* det_fg, int32_t* rotated, const double* grid_inc);
+
+/* Growth increments of the grid-based growth functions (type 3) active at time t
+ * (Simulation::calculateGrowthGridBased, Simulation.cpp:9038-9085; GridBasedGrowthFunction,
+ * GrowthFunctionTypes.h:269-548; ShapeBase::calculateFgFromGridCorners, ShapeBase.cpp:513-658;
+ * convertRelativePosToGridIndex :834-860; updateGrowthIncrement :764-787), composed in function
+ * order into inc[E*9] (identity where none applies). Per function f: dims[2f..] = (nGridX, nGridY),
+ * rates (1/s) and angles_deg (degrees, as read from the grid file) at grid point (i, j) at
+ * offset i*nGridY + j of the function's block (blocks concatenated), windows[2f..] = [t0, t1),
+ * zrange[2f..] = (zMin, zMax), fflags[f] bit0 columnar, bit1 peripodial, bit2 basal ECM, bit3
+ * lateral ECM. interpolation 0 = nearest corner, 1 = bilinear. Per element: rel_pos[E*2] the
+ * (pinned) relative position in the bounding box, rel_z[E] initialRelativePositionInZ,
+ * eflags[E] bit0 ECM-mimicking, bit1 actin-mimicking, bit2 basal placement, bit3 ECM at the
+ * circumference, bits 4-5 tissue type (0 columnar, 1 peripodial). tfo_grow applies inc after
+ * the uniform increment. per_func[F*E*10] (may be NULL) receives, per function and element,
+ * 1 when calculateFgFromGridCorners passed its applicability test (the reference then prints the
+ * increment's diagonal) and that function's own increment (9 doubles). */
+void tfo_grid_growth_increments(int n_elems, int n_funcs, const int32_t* dims, const double* rates,
+                                const double* angles_deg, const double* windows, const double* zrange,
+                                const int32_t* fflags, int interpolation, const double* rel_pos,
+                                const double* rel_z, const int32_t* eflags, double t, double dt, double* inc,
+                                double* per_func);
 
 /* Node viscosity surfaces (Simulation::updateNodeViscositySurfaces, Sim.cpp:7598-7620):
  * exposed[E] bit0 = exposed apical surface, bit1 = exposed basal surface,

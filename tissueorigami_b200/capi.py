@@ -49,6 +49,7 @@ EXPORTS = [
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
     "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64",
+    "tf_set_grid_growth", "tf_set_time", "tf_get_time",
 ]
 
 
@@ -64,6 +65,13 @@ class Params(ctypes.Structure):
                 ("elems_per_block", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32),
                 ("smoother_nodes", ctypes.c_int32), ("krylov_refine", ctypes.c_int32)]
+
+
+class GridGrowth(ctypes.Structure):
+    _fields_ = [("t0", ctypes.c_double), ("t1", ctypes.c_double), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+                ("rates", ctypes.POINTER(ctypes.c_double)), ("angles", ctypes.POINTER(ctypes.c_double)),
+                ("z_min", ctypes.c_double), ("z_max", ctypes.c_double), ("flags", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class StepStats(ctypes.Structure):
@@ -141,6 +149,9 @@ def load(build_if_missing: bool = True):
     L.tf_solve_direct.argtypes = [_P, _D, _D, _D, _D, _I]
     L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
     L.tf_measure_fp64.argtypes = [c_int, _D]
+    L.tf_set_grid_growth.argtypes = [_P, c_int, ctypes.POINTER(GridGrowth), c_int, _D, _D, _I]
+    L.tf_set_time.argtypes = [_P, c_double]
+    L.tf_get_time.argtypes = [_P, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:

@@ -72,6 +72,18 @@ struct tf_ctx {
     DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
     DevBuf fg, rates, angles, exposed, peripodial, rotated, xio, barrier;
     DevBuf refine_acc, refine_g;  // tf_solve's iterative refinement: accumulated du, saved g
+
+    // grid-based growth functions (tf_set_grid_growth) and the simulation clock that selects the
+    // ones active in a step (currSimTimeSec of the reference)
+    struct GridFuncHost {
+        double t0, t1, zmin, zmax;
+        int32_t nx, ny, flags;
+        DevBuf cells;
+    };
+    std::vector<GridFuncHost> grid_funcs;
+    int32_t grid_interp = 0;
+    DevBuf grid_rel_pos, grid_rel_z, grid_eflags, grid_inc;
+    double sim_time = 0.0;
     int persistent_grid_max = 0;  // 0: cooperative launch unavailable
     int persist_threads = 256;    // CTA width of the persistent solve
 
@@ -1486,9 +1498,35 @@ int call_end(tf_ctx* ctx, tf_step_stats* st) {
     return TF_OK;
 }
 
+// The growth prologue of a step at the context's simulation time: the grid-based functions active
+// then (InitialTime <= t < FinalTime, Simulation.cpp:9041) give a per-element increment, applied
+// after the uniform one; then the growth update and the exposed areas.
 int prologue(tf_ctx* ctx, double dt) {
+    const double* grid_inc = nullptr;
+    GridStep gs;
+    std::memset(&gs, 0, sizeof(gs));
+    gs.interpolation = ctx->grid_interp;
+    gs.dt = dt;
+    for (const auto& gf : ctx->grid_funcs) {
+        if (!(ctx->sim_time >= gf.t0 && ctx->sim_time < gf.t1)) continue;
+        if (gs.n >= kMaxGridFuncs) return set_error(ctx, TF_ERR_UNSUPPORTED, "more than 8 grid growth functions in a step");
+        GridFunc& f = gs.f[gs.n++];
+        f.cells = static_cast<const GridCell*>(gf.cells.p);
+        f.nx = gf.nx;
+        f.ny = gf.ny;
+        f.zmin = gf.zmin;
+        f.zmax = gf.zmax;
+        f.flags = gf.flags;
+    }
+    if (gs.n > 0) {
+        TF_CK(launch_grid_increment(ctx->E, gs, dptr<double>(ctx->grid_rel_pos), dptr<double>(ctx->grid_rel_z),
+                                    dptr<int32_t>(ctx->grid_eflags), dptr<double>(ctx->grid_inc), ctx->stream));
+        grid_inc = dptr<double>(ctx->grid_inc);
+        ctx->launches += 1;
+    }
     TF_CK(launch_grow(dptr<ElemRecord>(ctx->elems), ctx->E, dptr<double>(ctx->un), dptr<double>(ctx->fg),
-                      dptr<double>(ctx->rates), dptr<double>(ctx->angles), dt, dptr<int32_t>(ctx->rotated), ctx->stream));
+                      dptr<double>(ctx->rates), dptr<double>(ctx->angles), dt, dptr<int32_t>(ctx->rotated), grid_inc,
+                      ctx->stream));
     TF_CK(launch_viscosity_surface(dptr<ElemRecord>(ctx->elems), ctx->E, ctx->N, dptr<double>(ctx->un),
                                    dptr<uint8_t>(ctx->exposed), dptr<uint8_t>(ctx->peripodial),
                                    dptr<double>(ctx->visc_surface), ctx->stream));
@@ -1780,8 +1818,10 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->rhat, &ctx->p, &ctx->v, &ctx->s, &ctx->t, &ctx->phat, &ctx->shat, &ctx->dinv,
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
                      &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier,
-                     &ctx->refine_acc, &ctx->refine_g};
+                     &ctx->refine_acc, &ctx->refine_g, &ctx->grid_rel_pos, &ctx->grid_rel_z,
+                     &ctx->grid_eflags, &ctx->grid_inc};
     for (DevBuf* b : all) dfree(*b);
+    for (auto& gf : ctx->grid_funcs) dfree(gf.cells);
     DevBuf* batch[] = {&ctx->plan_queue_d, &ctx->queue_head_d, &ctx->node_tissue_d, &ctx->plan_list_ptr_d,
                        &ctx->plan_list_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d, &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
     for (DevBuf* b : batch) dfree(*b);
@@ -1901,6 +1941,7 @@ static int step_entry(tf_ctx* ctx, const double* x_n, double dt, double* x_out, 
     }
     rc = newton_core(ctx, dt, st);
     if (rc < 0) return rc;
+    if (grow) ctx->sim_time += dt;  // runOneStep ends with currSimTimeSec += dt
     TF_CK(cudaMemcpyAsync(x_out, ctx->uk.p, bytes, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
     const int rc2 = call_end(ctx, st);
     return rc2 != TF_OK ? rc2 : rc;
@@ -2060,6 +2101,140 @@ int tf_get_growth(tf_ctx* ctx, double* fg, double* inv_fg) {
         TF_CK(cudaMemcpy(rec.data(), ctx->elems.p, sizeof(ElemRecord) * (size_t)ctx->E, cudaMemcpyDeviceToHost));
         for (int e = 0; e < ctx->E; ++e) std::memcpy(inv_fg + (size_t)e * 9, rec[e].inv_fg, sizeof(double) * 9);
     }
+    return TF_OK;
+}
+
+// GridBasedGrowthFunction's constructor (GrowthFunctionTypes.h:287-345) and
+// preCalculateAnglesForCompatibleAveraging (:368-531): per cell, the four corners' growth and
+// angles, angles of corners whose x / y growth ratio is below 1.1 left out, the others brought
+// into [0, pi] and then within 45 degrees of the first kept corner, with x / y growth swapped
+// where that took a 90-degree turn.
+static void grid_cells(const tf_grid_growth& f, std::vector<GridCell>& cells) {
+    const int nx = f.nx, ny = f.ny;
+    auto gm = [&](int i, int j, int k) { return f.rates[((size_t)i * ny + j) * 3 + k]; };
+    auto over = [&](int i, int j) {
+        double AR = gm(i, j, 0) / gm(i, j, 1);
+        if (AR < 0) AR *= -1.0;
+        if (AR < 1.0) AR = 1 / AR;
+        return !(AR < 1.1);
+    };
+    cells.assign((size_t)(nx - 1) * (ny - 1), GridCell());
+    for (int IX = 0; IX < nx - 1; ++IX)
+        for (int IY = 0; IY < ny - 1; ++IY) {
+            GridCell& c = cells[(size_t)IX * (ny - 1) + IY];
+            std::memset(&c, 0, sizeof(c));
+            const int ci[4][2] = {{IX, IY}, {IX + 1, IY}, {IX, IY + 1}, {IX + 1, IY + 1}};
+            double a[4] = {0, 0, 0, 0};
+            bool elim[4] = {false, false, false, false};
+            for (int q = 0; q < 4; ++q) {
+                for (int k = 0; k < 3; ++k) c.g[q][k] = gm(ci[q][0], ci[q][1], k);
+                if (over(ci[q][0], ci[q][1]))
+                    a[q] = f.angles[(size_t)ci[q][0] * ny + ci[q][1]] * M_PI / 180.0;
+                else
+                    elim[q] = true;
+            }
+            for (int q = 0; q < 4; ++q) {
+                while (a[q] < 0) a[q] += M_PI;
+                while (a[q] > M_PI) a[q] -= M_PI;
+            }
+            int sel = 3;
+            double tet = 0;
+            for (int q = 0; q < 4; ++q)
+                if (!elim[q]) {
+                    tet = a[q];
+                    sel = q;
+                    break;
+                }
+            for (int q = sel; q < 4; ++q) {
+                const double d = a[q] - tet;
+                bool flip = false;
+                if (d > 0) {
+                    if (d >= M_PI / 4.0 && d < 3.0 * M_PI / 4.0) {
+                        a[q] -= M_PI / 2.0;
+                        flip = true;
+                    } else if (d >= 3.0 * M_PI / 4.0 && d < 5.0 * M_PI / 4.0) {
+                        a[q] -= M_PI;
+                    } else if (d >= 5.0 * M_PI / 4.0 && d < 7.0 * M_PI / 4.0) {
+                        a[q] -= 6.0 * M_PI / 4.0;
+                        flip = true;
+                    } else if (d >= 7.0 * M_PI / 4.0) {
+                        a[q] -= 2.0 * M_PI;
+                    }
+                } else if (d < 0) {
+                    if (d <= -M_PI / 4.0 && d > -3.0 * M_PI / 4.0) {
+                        a[q] += M_PI / 2.0;
+                        flip = true;
+                    } else if (d <= -3.0 * M_PI / 4.0 && d > -5.0 * M_PI / 4.0) {
+                        a[q] += M_PI;
+                    } else if (d <= -5.0 * M_PI / 4.0 && d > -7.0 * M_PI / 4.0) {
+                        a[q] += 6.0 * M_PI / 4.0;
+                        flip = true;
+                    } else if (d <= -7.0 * M_PI / 4.0) {
+                        a[q] += 2.0 * M_PI;
+                    }
+                }
+                if (flip) std::swap(c.g[q][0], c.g[q][1]);
+            }
+            for (int q = 0; q < 4; ++q) {
+                c.a[q] = a[q];
+                if (elim[q]) c.elim |= 1 << q;
+            }
+        }
+}
+
+int tf_set_grid_growth(tf_ctx* ctx, int32_t n_funcs, const tf_grid_growth* funcs, int32_t interpolation,
+                       const double* rel_pos, const double* rel_z, const int32_t* elem_flags) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (n_funcs < 0 || (n_funcs > 0 && (!funcs || !rel_pos || !rel_z || !elem_flags)) ||
+        (interpolation != 0 && interpolation != 1))
+        return TF_ERR_ARGUMENT;
+    for (int f = 0; f < n_funcs; ++f)
+        if (funcs[f].nx < 2 || funcs[f].ny < 2 || !funcs[f].rates || !funcs[f].angles) return TF_ERR_ARGUMENT;
+    for (auto& gf : ctx->grid_funcs) dfree(gf.cells);
+    ctx->grid_funcs.clear();
+    ctx->grid_interp = interpolation;
+    if (n_funcs == 0) return TF_OK;
+    const size_t E = (size_t)ctx->E;
+    TF_CK(dalloc(ctx->grid_rel_pos, sizeof(double) * 2 * E));
+    TF_CK(dalloc(ctx->grid_rel_z, sizeof(double) * E));
+    TF_CK(dalloc(ctx->grid_eflags, sizeof(int32_t) * E));
+    TF_CK(dalloc(ctx->grid_inc, sizeof(double) * 9 * E));
+    TF_CK(cudaMemcpy(ctx->grid_rel_pos.p, rel_pos, sizeof(double) * 2 * E, cudaMemcpyHostToDevice));
+    TF_CK(cudaMemcpy(ctx->grid_rel_z.p, rel_z, sizeof(double) * E, cudaMemcpyHostToDevice));
+    TF_CK(cudaMemcpy(ctx->grid_eflags.p, elem_flags, sizeof(int32_t) * E, cudaMemcpyHostToDevice));
+    std::vector<GridCell> cells;
+    for (int f = 0; f < n_funcs; ++f) {
+        tf_ctx::GridFuncHost h;
+        h.t0 = funcs[f].t0;
+        h.t1 = funcs[f].t1;
+        h.zmin = funcs[f].z_min;
+        h.zmax = funcs[f].z_max;
+        h.nx = funcs[f].nx;
+        h.ny = funcs[f].ny;
+        h.flags = funcs[f].flags;
+        grid_cells(funcs[f], cells);
+        ctx->grid_funcs.push_back(h);
+        TF_CK(dalloc(ctx->grid_funcs.back().cells, sizeof(GridCell) * cells.size()));
+        TF_CK(cudaMemcpy(ctx->grid_funcs.back().cells.p, cells.data(), sizeof(GridCell) * cells.size(),
+                         cudaMemcpyHostToDevice));
+    }
+    return TF_OK;
+}
+
+int tf_set_time(tf_ctx* ctx, double t) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!std::isfinite(t)) return TF_ERR_ARGUMENT;
+    ctx->sim_time = t;
+    return TF_OK;
+}
+
+int tf_get_time(tf_ctx* ctx, double* t) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!t) return TF_ERR_ARGUMENT;
+    *t = ctx->sim_time;
     return TF_OK;
 }
 

@@ -364,7 +364,8 @@ __global__ void k_node_terms(NodeArgs a) {
 // Per-element growth step (ShapeBase.cpp:1914-2041 rotation extraction, 471-505 increment,
 // 1452-1506 growShapeByFg) from the positions at the start of the step.
 __global__ void k_grow(ElemRecord* elems, int32_t n_elems, const double* x, double* fg,
-                       const double* rates, const double* angles, double dt, int32_t* rotated) {
+                       const double* rates, const double* angles, double dt, int32_t* rotated,
+                       const double* grid_inc) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_elems) return;
     ElemRecord& R = elems[e];
@@ -435,6 +436,18 @@ __global__ void k_grow(ElemRecord* elems, int32_t n_elems, const double* x, doub
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) gi[i][j] = tmp[i][0] * Ra[j][0] + tmp[i][1] * Ra[j][1] + tmp[i][2] * Ra[j][2];
+    if (grid_inc) {  // updateGrowthIncrement of the step's grid functions: growthInc = G growthInc
+        double G[3][3], prod[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) G[i][j] = grid_inc[(size_t)e * 9 + i * 3 + j];
+        mm3(G, gi, prod);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) gi[i][j] = prod[i][j];
+    }
     if (rot) {
         double GtI[3][3];
 #pragma unroll
@@ -457,6 +470,92 @@ __global__ void k_grow(ElemRecord* elems, int32_t n_elems, const double* x, doub
             fg[(size_t)e * 9 + i * 3 + j] = Fn[i][j];
             R.inv_fg[i * 3 + j] = inv[i][j];
         }
+}
+
+// Growth increments of the step's grid-based functions, one element per thread
+// (Simulation::calculateGrowthGridBased, Simulation.cpp:9038-9085; ShapeBase::calculateFgFromGridCorners,
+// ShapeBase.cpp:513-658; convertRelativePosToGridIndex :834-860; isGrowthRateApplicable :297-334;
+// updateGrowthIncrement :764-787). eflags: bit0 ECM-mimicking, bit1 actin-mimicking, bit2 basal
+// placement, bit3 ECM at the circumference, bits 4-5 tissue type (0 columnar, 1 peripodial).
+__global__ void k_grid_increment(int32_t n_elems, GridStep gs, const double* __restrict__ rel_pos,
+                                 const double* __restrict__ rel_z, const int32_t* __restrict__ eflags,
+                                 double* __restrict__ inc) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_elems) return;
+    const int ef = eflags[e];
+    const bool ecm = ef & 1, actin = ef & 2, basal = ef & 4, ecm_circ = ef & 8;
+    const int ttype = (ef >> 4) & 3;
+    const double rx = rel_pos[2 * e], ry = rel_pos[2 * e + 1], rz = rel_z[e];
+    double acc[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int f = 0; f < gs.n; ++f) {
+        const GridFunc& F = gs.f[f];
+        const double px = rx * (double)(float)(F.nx - 1), py = ry * (double)(float)(F.ny - 1);
+        int ix = (int)floor(px), iy = (int)floor(py);
+        double fx = px - ix, fy = py - iy;
+        if (ix >= F.nx - 1) {
+            ix = F.nx - 2;
+            fx = 1.0;
+        } else if (ix < 0) {
+            ix = 0;
+            fx = 0.0;
+        }
+        if (iy >= F.ny - 1) {
+            iy = F.ny - 2;
+            fy = 1.0;
+        } else if (iy < 0) {
+            iy = 0;
+            fy = 0.0;
+        }
+        const GridCell& c = F.cells[(size_t)ix * (F.ny - 1) + iy];
+        // which increment the element takes from this function: the columnar one (also through
+        // the ECM options) or the peripodial one; -1: neither (identity)
+        int source = -1;
+        if (((F.flags & 4) && ecm && basal) || ((F.flags & 8) && ecm_circ && !basal)) source = 0;
+        if (!ecm) {
+            if ((F.flags & 1) && ttype == 0) source = 0;
+            if ((F.flags & 2) && ttype == 1) source = 1;
+        }
+        if (source < 0 || (source == 0 && ttype != 0) || (source == 1 && ttype != 1)) continue;
+        if (rz < F.zmin || rz > F.zmax) continue;  // outside the function's z range: identity
+        double g[3] = {0.0, 0.0, 0.0}, angle = 0.0;
+        if (gs.interpolation == 0) {
+            const int q = fx > 0.5 ? (fy > 0.5 ? 3 : 1) : (fy > 0.5 ? 2 : 0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) g[k] = c.g[q][k];
+        } else {
+            const double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
+            double elim = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if ((c.elim >> q) & 1) elim += w[q];
+            angle = c.a[0] * w[0] + c.a[1] * w[1] + c.a[2] * w[2] + c.a[3] * w[3];
+            if (elim > 0) angle = elim >= 0.9999999 ? 0.0 : angle / (1.0 - elim);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) g[k] = c.g[0][k] * w[0] + c.g[1][k] * w[1] + c.g[2][k] * w[2] + c.g[3][k] * w[3];
+        }
+        if (actin) g[2] = 0.0;  // actin-mimicking elements do not grow in height
+        double D[3][3] = {{exp(g[0] * gs.dt), 0, 0}, {0, exp(g[1] * gs.dt), 0}, {0, 0, exp(g[2] * gs.dt)}};
+        if (angle != 0.0) {
+            const double cs = cos(angle), sn = sin(angle);
+            const double R[3][3] = {{cs, -1.0 * sn, 0.0}, {sn, cs, 0.0}, {0.0, 0.0, 1.0}};
+            double T[3][3];
+            mm3(R, D, T);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) D[i][j] = T[i][0] * R[j][0] + T[i][1] * R[j][1] + T[i][2] * R[j][2];
+        }
+        double P[3][3];
+        mm3(D, acc, P);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[i][j] = P[i][j];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) inc[(size_t)e * 9 + i * 3 + j] = acc[i][j];
 }
 
 // Exposed-triangle area (Prism::calculateApicalArea / calculateBasalArea, Prism.cpp:1485-1556)
@@ -577,11 +676,19 @@ cudaError_t launch_node_terms(const NodeArgs& a, cudaStream_t s) {
 
 cudaError_t launch_grow(ElemRecord* elems, int32_t n_elems, const double* x, double* fg,
                         const double* rates, const double* angles, double dt, int32_t* rotated,
-                        cudaStream_t s) {
+                        const double* grid_inc, cudaStream_t s) {
     cudaError_t err = upload_gauss_table();
     if (err != cudaSuccess) return err;
     if (n_elems <= 0) return cudaSuccess;
-    k_grow<<<(n_elems + 127) / 128, 128, 0, s>>>(elems, n_elems, x, fg, rates, angles, dt, rotated);
+    k_grow<<<(n_elems + 127) / 128, 128, 0, s>>>(elems, n_elems, x, fg, rates, angles, dt, rotated, grid_inc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid_increment(int32_t n_elems, const GridStep& gs, const double* rel_pos, const double* rel_z,
+                                  const int32_t* eflags, double* inc, cudaStream_t s) {
+    if (n_elems <= 0) return cudaSuccess;
+    if (gs.n < 0 || gs.n > kMaxGridFuncs) return cudaErrorInvalidValue;
+    k_grid_increment<<<(n_elems + 127) / 128, 128, 0, s>>>(n_elems, gs, rel_pos, rel_z, eflags, inc);
     return cudaGetLastError();
 }
 

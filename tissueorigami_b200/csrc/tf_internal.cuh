@@ -172,9 +172,44 @@ cudaError_t launch_element_assemble(const AssembleArgs& a, int teams, bool visc,
 cudaError_t launch_node_terms(const NodeArgs& a, cudaStream_t s);
 
 // --- growth prologue (tf_element.cu) ------------------------------------------------------
+// grid_inc [E][9] (may be NULL): the increments of the step's grid-based growth functions, applied
+// after the uniform increment (the reference composes its growth functions in list order)
 cudaError_t launch_grow(ElemRecord* elems, int32_t n_elems, const double* x, double* fg,
                         const double* rates, const double* angles, double dt, int32_t* rotated,
-                        cudaStream_t s);
+                        const double* grid_inc, cudaStream_t s);
+
+// One cell of a grid-based growth function (GridBasedGrowthFunction, GrowthFunctionTypes.h:269-548):
+// the growth rates (1/s) and orientation angles (radians) of its four corners (0: (i, j), 1: (i+1, j),
+// 2: (i, j+1), 3: (i+1, j+1)) after the reference's compatible-averaging pass, which brings the
+// angles within 45 degrees of the first corner with an aspect ratio over 1.1 and swaps x / y
+// growth where it turned an angle by 90 degrees; elim bit q: corner q's angle left out of the
+// average.
+struct GridCell {
+    double g[4][3];
+    double a[4];
+    int32_t elim;
+    int32_t pad;
+};
+
+constexpr int kMaxGridFuncs = 8;  // grid-based growth functions active in one step
+struct GridFunc {
+    const GridCell* cells;  // [(nx-1)*(ny-1)], cell (i, j) at i*(ny-1) + j
+    int32_t nx, ny;
+    double zmin, zmax;      // range of initialRelativePositionInZ the function applies to
+    int32_t flags;          // bit0 columnar, bit1 peripodial, bit2 basal ECM, bit3 lateral ECM
+    int32_t pad;
+};
+struct GridStep {
+    int32_t n;              // active functions, in the reference's list order
+    int32_t interpolation;  // 0 nearest corner, 1 bilinear
+    double dt;
+    GridFunc f[kMaxGridFuncs];
+};
+// inc [E][9] = the product of the active functions' increments (ShapeBase::calculateFgFromGridCorners,
+// updateGrowthIncrement); rel_pos [E][2] pinned relative positions, rel_z [E], eflags [E] as in
+// tf_set_grid_growth.
+cudaError_t launch_grid_increment(int32_t n_elems, const GridStep& gs, const double* rel_pos, const double* rel_z,
+                                  const int32_t* eflags, double* inc, cudaStream_t s);
 cudaError_t launch_viscosity_surface(const ElemRecord* elems, int32_t n_elems, int32_t n_nodes,
                                      const double* x, const uint8_t* exposed,
                                      const uint8_t* peripodial, double* visc_surface,

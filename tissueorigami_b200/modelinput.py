@@ -107,6 +107,9 @@ class ReferenceSetup:
     actin: np.ndarray
     not_modelled: List[str]
     zero_viscosity_fixes: List[Tuple[int, int]] = dataclasses.field(default_factory=list)
+    grid_growth: List[dict] = dataclasses.field(default_factory=list)
+    grid_interpolation: int = 0
+    grid_state: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None  # rel_pos, rel_z, eflags
 
     def growth_at(self, t: float) -> Tuple[np.ndarray, np.ndarray]:
         """Per-element growth rates and angles applied by the step that starts at time t."""
@@ -131,6 +134,9 @@ class ReferenceSetup:
         own = solver is None
         s = solver or NewtonRaphsonSolver.from_tissue(t, **params)
         try:
+            if self.grid_growth:
+                s.set_grid_growth(self.grid_growth, self.grid_interpolation, *self.grid_state)
+            s.set_time(0.0)
             x = np.array(t.x, dtype=np.float64, copy=True)
             xs, stats = [], []
             for k in range(n_steps if n_steps is not None else t.n_steps):
@@ -227,8 +233,105 @@ def fix_zero_external_viscosity(fixed, ext_visc, node_place, node_type, x, fixes
     return applied
 
 
-def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSetup:
-    """Apply the reference's set-up rules to parsed ``modelinput`` entries and ``read_mesh`` arrays."""
+def growth_blocks(entries: Sequence[Tuple[str, List[str]]]) -> List[Tuple[int, List[Tuple[str, List[str]]]]]:
+    """The growth functions of a model input in their order (ModelInputObject::readGrowthOptions):
+    (type, entries up to the next function or section) for every GrowthFunctionType entry."""
+    out: List[Tuple[int, List[Tuple[str, List[str]]]]] = []
+    for k, v in entries:
+        if k == "GrowthFunctionType(int-seeDocumentation)":
+            out.append((int(float(v[0])), []))
+        elif out and v:
+            out[-1][1].append((k, v))
+        elif out and not v:  # a section header ends the growth options
+            break
+    return out
+
+
+def read_growth_grid(text: str):
+    """A grid growth file as ModelInputObject::readGrowthType3 (ModelInputObject.cpp:782-833) reads
+    it: nGridX nGridY, then the rates of every grid point (row j from nGridY-1 down to 0, i from 0,
+    three axes) read into float, then the angles in degrees in the same order read into double;
+    the rates are held per second (per-hour value x 1/3600). Returns (rates[nx, ny, 3], angles[nx, ny])."""
+    tok = text.split()
+    nx, ny = int(tok[0]), int(tok[1])
+    pos = 2
+    rates = np.zeros((nx, ny, 3))
+    for j in range(ny - 1, -1, -1):
+        for i in range(nx):
+            for k in range(3):
+                rates[i, j, k] = float(np.float32(tok[pos]))
+                pos += 1
+    angles = np.zeros((nx, ny))
+    for j in range(ny - 1, -1, -1):
+        for i in range(nx):
+            angles[i, j] = float(tok[pos])
+            pos += 1
+    return rates * (1.0 / 3600.0), angles
+
+
+def grid_element_state(x, conn, node_place, node_type, place, spans, ecm, actin):
+    """Per-element inputs of the grid growth functions on the initial mesh:
+
+    * rel_pos [E,2]: the element centre (mean of its six nodes, ShapeBase::getCentre) relative to the
+      x, y bounding box of the nodes not owned by ECM elements only (calculateBoundingBox,
+      Simulation.cpp:8388-8425; calculateRelativePosInBoundingBox, ShapeBase.cpp:2091-2095), with
+      the apical element's value copied down its column as updateRelativePositionsToApicalPositioning
+      does (Simulation.cpp:6147-6167: the column list runs basal to apical and the copy covers its
+      first L-2 entries);
+    * rel_z [E]: initialRelativePositionInZ = 1 - (centre z - minimum node z) / tissue height,
+      clipped to [0, 1] (ShapeBase::setInitialZPosition, ShapeBase.cpp:813-828), the height summed
+      along the first basal columnar node's column (calculateTissueHeight, Simulation.cpp:3275-3330);
+    * eflags [E]: bit0 ECM-mimicking, bit1 actin-mimicking, bit2 basal placement; tissue type 0."""
+    x = np.asarray(x, np.float64)
+    conn = np.asarray(conn)
+    E = conn.shape[0]
+    cen = np.zeros((E, 3))
+    for a in range(6):  # summed in node order, then divided, as getCentre does
+        cen += x[conn[:, a]]
+    cen /= 6
+    owned = np.zeros(x.shape[0], bool)
+    owned[conn[~ecm].ravel()] = True
+    keep = owned if ecm.any() else np.ones(x.shape[0], bool)
+    lo = x[keep, :2].min(axis=0)
+    size = x[keep, :2].max(axis=0) - lo
+    rel = np.zeros((E, 2))
+    rel[:, 0] = (cen[:, 0] - lo[0]) / size[0]
+    rel[:, 1] = (cen[:, 1] - lo[1]) / size[1]
+    # columns: the element above e is the one whose basal nodes are e's apical nodes
+    by_basal = {tuple(sorted(c[:3])): e for e, c in enumerate(conn)}
+    height, layers = 0.0, 0
+    first = next((n for n in range(x.shape[0]) if node_place[n] == BASAL and node_type[n] == 0), None)
+    if first is not None:
+        cur = first
+        while node_place[cur] != APICAL:
+            owner = next((e for e in range(E) if cur in conn[e, :3]), None)
+            if owner is None:
+                break
+            height += float(np.linalg.norm(x[conn[owner, 0]] - x[conn[owner, 3]]))
+            layers += 1
+            cur = int(conn[owner, 3 + list(conn[owner, :3]).index(cur)])
+    for e in range(E):
+        if place[e] != APICAL:
+            continue
+        stack = [e]
+        while True:  # walk down to the basal element of the column
+            below = next((b for b, c in enumerate(conn) if tuple(sorted(c[3:])) == tuple(sorted(conn[stack[-1], :3]))), None)
+            if below is None:
+                break
+            stack.append(below)
+        stack = stack[::-1]  # basal first, as elementsIdsOnSameColumn
+        for b in stack[:max(layers - 2, 0)]:
+            rel[b] = rel[e]
+    del by_basal
+    zmin = x[:, 2].min()
+    rel_z = np.clip(1.0 - (cen[:, 2] - zmin) / height, 0.0, 1.0) if height > 0 else np.zeros(E)
+    eflags = ecm.astype(np.int32) | (actin.astype(np.int32) << 1) | ((np.asarray(place) == BASAL).astype(np.int32) << 2)
+    return rel, rel_z, eflags
+
+
+def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays, grid_files=None) -> ReferenceSetup:
+    """Apply the reference's set-up rules to parsed ``modelinput`` entries and ``read_mesh`` arrays.
+    grid_files: the text of every grid growth file, keyed by its Filename entry."""
     m = _Entries(entries)
     x, node_place, node_type, circ, conn, xref = mesh_arrays
     x = np.asarray(x, np.float64)
@@ -267,10 +370,21 @@ def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSet
     ell = m.get("bindEllipses(bool,nFunctions)")
     if ell and int(float(ell[0])):
         unsupported.append("ellipse binding")
-    n_growth = int(m.num("NumberofGrowthFunctions(int)", 0))
-    types = [int(float(m.get("GrowthFunctionType(int-seeDocumentation)", ["0"], i)[0])) for i in range(n_growth)]
-    if any(t != 1 for t in types):
-        unsupported.append(f"growth function types {sorted(set(t for t in types if t != 1))} (only uniform, 1)")
+    blocks = growth_blocks(entries)
+    types = [b[0] for b in blocks]
+    if any(t not in (1, 3) for t in types):
+        unsupported.append(f"growth function types {sorted(set(t for t in types if t not in (1, 3)))} "
+                           "(only uniform, 1, and grid-based, 3)")
+    if 3 in types:
+        if not m.flag("GridGrowthsPinnedOnInitialMesh(bool)"):
+            unsupported.append("grid growth read on the current mesh (GridGrowthsPinnedOnInitialMesh 0)")
+        pins = m.get("PinningUpdateTimes(number-times(sec))", ["0"])
+        if any(float(v) > 0 for v in pins[1:1 + int(float(pins[0]))]):
+            unsupported.append("grid growth re-pinned during the run (PinningUpdateTimes after 0)")
+        if 1 in types[types.index(3):]:
+            unsupported.append("a uniform growth function listed after a grid-based one")
+    if m.num("noTimeseriesInputs(size_t)", 0):
+        unsupported.append("Young's modulus time series")
     if m.flag("AddLateralECM(bool)"):
         unsupported.append("lateral ECM")
     if unsupported:
@@ -370,15 +484,29 @@ def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSet
     exposed[(place == BASAL) | ((place == MID) & spans)] |= 2
 
     # growth: uniform functions, parameters held in single precision as the reference reads them
-    growth = []
-    for i in range(n_growth):
-        t0 = float(np.float32(m.num("InitialTime(sec)", index=i)))
-        t1 = float(np.float32(m.num("FinalTime(sec)", index=i)))
-        col = m.flag("ApplyToColumnarLayer(bool)", index=i)
-        basal_ecm = m.flag("ApplyToBasalECM(bool)", index=i)
-        per_hour = m.num("MaxValue(fractionPerHour-DV,AP,AB)", n=3, index=i)
+    # (resolved per element here); grid-based functions as the reference holds them, evaluated on
+    # the device every step from the elements' pinned positions
+    growth, grid = [], []
+    for gtype, g in blocks:
+        gm = _Entries(g)
+        t0 = float(np.float32(gm.num("InitialTime(sec)")))
+        t1 = float(np.float32(gm.num("FinalTime(sec)")))
+        if gtype == 3:
+            name = gm.get("Filename(full-path)")[0]
+            if grid_files is None or name not in grid_files:
+                raise ValueError(f"grid growth file {name} not given")
+            rates_g, angles_g = read_growth_grid(grid_files[name])
+            zr = gm.num("zRange", n=2)
+            flags = (int(gm.flag("ApplyToColumnarLayer(bool)")) | int(gm.flag("ApplyToPeripodialMembrane(bool)")) << 1
+                     | int(gm.flag("ApplyToBasalECM(bool)")) << 2 | int(gm.flag("ApplyToLateralECM(bool)")) << 3)
+            grid.append({"t0": t0, "t1": t1, "rates": rates_g, "angles_deg": angles_g, "zmin": zr[0], "zmax": zr[1],
+                         "flags": flags, "nx": rates_g.shape[0], "ny": rates_g.shape[1], "file": name})
+            continue
+        col = gm.flag("ApplyToColumnarLayer(bool)")
+        basal_ecm = gm.flag("ApplyToBasalECM(bool)")
+        per_hour = gm.num("MaxValue(fractionPerHour-DV,AP,AB)", n=3)
         rate = [float(np.float32(np.float32(v) * (1.0 / 3600.0))) for v in per_hour]
-        angle = float(np.float32(np.float32(m.num("Angle(degrees)", index=i)) * (np.pi / 180.0)))
+        angle = float(np.float32(np.float32(gm.num("Angle(degrees)")) * (np.pi / 180.0)))
         on = np.zeros(E, bool)
         if col:
             on |= ~ecm if explicit_ecm else np.ones(E, bool)
@@ -388,6 +516,10 @@ def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSet
         rates = np.zeros((E, 3))
         rates[on] = rate
         growth.append(UniformGrowth(t0, t1, rates, np.full(E, angle)))
+    grid_state = None
+    if grid:
+        grid_state = grid_element_state(x, conn, node_place, np.asarray(node_type), place, spans, ecm if explicit_ecm else
+                                        np.zeros(E, bool), actin)
 
     dt = m.num("TimeStep(sec)")
     length = m.num("SimulationLength(sec)", dt)
@@ -401,7 +533,8 @@ def setup(entries: Sequence[Tuple[str, List[str]]], mesh_arrays) -> ReferenceSet
     tissue = Tissue("modelinput", conn, np.asarray(xref, np.float64), x, lam, mu, eta, fixed, ext_visc, exposed,
                     np.zeros(E, np.uint8), np.zeros((E, 3)), np.zeros(E), node_place, circ.astype(np.int32),
                     slave_master=slave_master, dt=float(dt), n_steps=int(round(length / dt)), newton_tol=1e-8)
-    return ReferenceSetup(tissue, growth, place, ecm, actin, not_modelled, zero_visc_fixes)
+    interp = int(m.num("GridGrowthsInterpolationType(0=step,1=linear)", 0))
+    return ReferenceSetup(tissue, growth, place, ecm, actin, not_modelled, zero_visc_fixes, grid, interp, grid_state)
 
 
 def load(modelinput_path: str, mesh_path: Optional[str] = None) -> ReferenceSetup:
@@ -414,4 +547,11 @@ def load(modelinput_path: str, mesh_path: Optional[str] = None) -> ReferenceSetu
         if name is None:
             raise ValueError("no MeshFile in the model input")
         mesh_path = name if os.path.isabs(name) else os.path.join(os.path.dirname(os.path.abspath(modelinput_path)), name)
-    return setup(entries, read_mesh(mesh_path))
+    folder = os.path.dirname(os.path.abspath(modelinput_path))
+    grid_files = {}
+    for gtype, g in growth_blocks(entries):
+        if gtype == 3:
+            name = _Entries(g).get("Filename(full-path)")[0]
+            with open(name if os.path.isabs(name) else os.path.join(folder, name)) as fh:
+                grid_files[name] = fh.read()
+    return setup(entries, read_mesh(mesh_path), grid_files)

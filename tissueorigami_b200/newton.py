@@ -98,6 +98,33 @@ class NewtonRaphsonSolver:
             capi.uptr(np.ascontiguousarray(peripodial, dtype=np.uint8)) if peripodial is not None else None),
             "tf_set_growth", self._h)
 
+    def set_grid_growth(self, funcs, interpolation: int, rel_pos, rel_z, elem_flags):
+        """Grid-based growth functions (tf_set_grid_growth): funcs is a list of dicts with t0, t1,
+        rates[nx,ny,3] (1/s), angles_deg[nx,ny], zmin, zmax, flags; per element the pinned relative
+        position [E,2], initialRelativePositionInZ [E] and flags [E] (modelinput.grid_element_state)."""
+        keep = []
+        arr = (capi.GridGrowth * max(len(funcs), 1))()
+        for i, f in enumerate(funcs):
+            r = _f64(f["rates"]).reshape(-1)
+            a = _f64(f["angles_deg"]).reshape(-1)
+            nx, ny = int(f["rates"].shape[0]), int(f["rates"].shape[1])
+            keep += [r, a]
+            arr[i] = capi.GridGrowth(float(f["t0"]), float(f["t1"]), nx, ny, capi.dptr(r), capi.dptr(a),
+                                     float(f["zmin"]), float(f["zmax"]), int(f["flags"]), 0)
+        rp, rz = _f64(rel_pos).reshape(-1), _f64(rel_z)
+        ef = np.ascontiguousarray(elem_flags, dtype=np.int32)
+        capi.check(self._L.tf_set_grid_growth(self._h, len(funcs), arr, int(interpolation), capi.dptr(rp),
+                                              capi.dptr(rz), capi.iptr(ef)), "tf_set_grid_growth", self._h)
+
+    def set_time(self, t: float):
+        """Simulation time at the start of the next step (Simulation::currSimTimeSec)."""
+        capi.check(self._L.tf_set_time(self._h, float(t)), "tf_set_time", self._h)
+
+    def time(self) -> float:
+        v = ctypes.c_double()
+        capi.check(self._L.tf_get_time(self._h, ctypes.byref(v)), "tf_get_time", self._h)
+        return v.value
+
     def get_growth(self):
         fg = np.zeros((self.n_elems, 9))
         inv = np.zeros((self.n_elems, 9))
