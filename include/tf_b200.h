@@ -162,6 +162,22 @@ int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
  * (Simulation.cpp:7598-7620): per-node exposed area, [n_nodes]. */
 int tf_set_viscosity_surface(tf_ctx* ctx, const double* visc_surface);
 
+/* Replaces the external-force vector NewtonRaphsonSolver::gExt (NewtonRaphsonSolver.h:39) that
+ * addExernalForces adds to the residual (NewtonRaphsonSolver.cpp:449-457): packing, pipette or
+ * random forces the host computes, [n_nodes*3]; added on free DoFs, routed through slave-master
+ * pairs like every force. Kept until replaced; NULL removes it. */
+int tf_set_external_force(tf_ctx* ctx, const double* f);
+
+/* One Newton iteration at the method level of NewtonRaphsonSolver: the sequence
+ * calculateDisplacementMatrix ... calculateBoundKWithSlavesMasterDoF, solveForDeltaU
+ * (NewtonRaphsonSolver.cpp:95-488; Simulation.cpp:6651-6716) on the device, from host positions
+ * uk (iteration k) and un (end of the previous step), [n_nodes*3] each; du [n_nodes*3] receives
+ * deltaU (slaves equal to their masters). The Jacobian never leaves the device. For hosts that keep
+ * the reference's Newton loop (checkConvergenceViaDeltaU, updateUkInIteration) on the host.
+ * iters / rel_res (may be NULL): BiCGStab iterations and final relative residual. */
+int tf_newton_iteration(tf_ctx* ctx, const double* uk, const double* un, double dt, double* du, int32_t* iters,
+                        double* rel_res);
+
 /* Replaces Simulation::updateStepNR (Simulation.cpp:6605-6747) with the surface-based
  * external viscosity of NewtonRaphsonSolver (externalViscosityVolumeBased = false) and no
  * packing or lumen terms: x_n [n_nodes*3] host positions at the end of the previous step,

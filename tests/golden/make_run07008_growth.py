@@ -11,8 +11,8 @@ parameters exactly as the reference holds them (rates and angle are read into si
 floats and scaled in place), the elements that grow (those whose Fg leaves the identity in the
 golden file) and the golden Fg of every element after every step.
 
-Run from the repository root with the reference checked out at REFERENCE_ROOT (default
-/root/reference):  python tests/golden/make_run07008_growth.py
+Run from the repository root with the reference's checkout given:
+    REFERENCE_ROOT=<path to the reference> python tests/golden/make_run07008_growth.py
 """
 import os
 import sys
@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from tissueorigami_b200 import mesh  # noqa: E402
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
 RUN = os.path.join(REF, "tests", "sim_no_pardiso_reg", "run07008")
 
 
@@ -46,6 +46,8 @@ def _growth_block(path):
 
 
 def main():
+    if not REF:
+        raise SystemExit("set REFERENCE_ROOT to the reference checkout")
     x, place, ttype, circ, conn, xref = mesh.read_mesh(os.path.join(RUN, "smallWingDisc.mesh"))
     dt, length, t0, t1, rates, angle = _growth_block(os.path.join(RUN, "modelinput07008"))
     E = conn.shape[0]

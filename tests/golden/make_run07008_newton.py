@@ -32,7 +32,7 @@ The fixture keeps the step-1 inputs and the recorded step-1 results:
   * the model input file's tokens (for the test of tissueorigami_b200.modelinput) and the first
     Save_Frame block verbatim (for the test of the Save_Frame writer).
 
-Run from the repository root with the reference at REFERENCE_ROOT (default /root/reference):
+Run from the repository root with the reference's checkout given in REFERENCE_ROOT:
     python tests/golden/make_run07008_newton.py
 (after tests/golden/make_run07008_growth.py, whose fixture supplies the growth parameters).
 """
@@ -46,7 +46,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from tissueorigami_b200 import mesh  # noqa: E402
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
 INP = os.path.join(REF, "tests", "sim_no_pardiso_reg", "run07008")
 OUT = os.path.join(REF, "tests", "sim_pardiso_reg", "run07008", "expected_out")
 
@@ -83,6 +83,8 @@ def _du_traces(path):
 
 
 def main():
+    if not REF:
+        raise SystemExit("set REFERENCE_ROOT to the reference checkout")
     x, place, ttype, circ, conn, xref = mesh.read_mesh(os.path.join(INP, "smallWingDisc.mesh"))
     N, E = x.shape[0], conn.shape[0]
     pp = np.fromfile(os.path.join(OUT, "Save_PhysicalProp"), dtype="<f8").reshape(-1, 3 * E + 3 * N)

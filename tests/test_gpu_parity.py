@@ -3,7 +3,9 @@
 Tolerances (written per test):
   * element forces / residual g and Jacobian entries: 1e-12 relative to the largest entry;
   * one linear solve (BiCGStab, rtol 1e-13) against the direct solve of the same system:
-    1e-8 relative in ||du|| (the systems have condition numbers ~1e5);
+    1e-8 relative in ||du|| (the systems have condition numbers ~1e5, so a residual of 1e-13
+    leaves up to ~1e-8 in du); with one pass of iterative refinement: 1e-12 relative against
+    the solution refined in extended precision and against the direct solve;
   * node positions after N implicit steps: 1e-9 of the tissue size (bounding-box diagonal).
 """
 import numpy as np
@@ -405,3 +407,75 @@ def test_two_level_with_slaves_matches_block_jacobi():
     x = out[capi.TF_PRECOND_TWO_LEVEL].reshape(-1)
     for s_, m_ in t.slave_master:
         assert x[s_] - t.x.reshape(-1)[s_] == pytest.approx(x[m_] - t.x.reshape(-1)[m_], abs=1e-12 * t.size)
+
+
+@pytest.mark.parametrize("degrees", [10.0, -25.0, 0.5])
+def test_device_growth_rotation_branch_matches_oracle(degrees):
+    """The growth prologue's rotation test (ShapeBase::CalculateGrowthRotationByF,
+    ShapeBase.cpp:1914-2041): elements turned about z by more than the 0.017 (about 1 degree)
+    threshold get their growth increment rotated back into the reference frame, those turned
+    less do not. The tissue is turned rigidly with every DoF fixed, so the step's mechanics leave
+    it where it is; the device's Fg after the step must equal the oracle's at 1e-12, with the
+    branch taken exactly where the oracle takes it."""
+    t = mesh.small_rectangle(nx=6, ny=4)
+    t.fixed[:] = 1
+    t.rates[:, 0], t.rates[:, 1] = 3e-4, 0.5e-4  # anisotropic, so the rotation changes Fg
+    th = np.deg2rad(degrees)
+    R = np.array([[np.cos(th), -np.sin(th), 0.0], [np.sin(th), np.cos(th), 0.0], [0.0, 0.0, 1.0]])
+    x = t.x @ R.T
+    fg_ref, _, _, rot = O.grow(t, x, t.fg)
+    assert rot.all() == (abs(degrees) > 1.0) and rot.any() == (abs(degrees) > 1.0)
+    with NewtonRaphsonSolver.from_tissue(t) as s:
+        x_out, rc, _ = s.runOneStep(x, t.dt)
+        assert rc == capi.TF_OK
+        fg, _ = s.get_growth()
+    np.testing.assert_array_equal(x_out, x)
+    assert np.abs(fg.reshape(-1, 9) - fg_ref).max() / np.abs(fg_ref).max() <= 1e-12
+
+
+def test_host_newton_loop_over_newton_iteration_matches_device_loop():
+    """The reference's updateStepNR loop kept on the host (checkConvergenceViaDeltaU,
+    updateUkInIteration), each iteration's assembly and solve through tf_newton_iteration: the
+    same positions and iteration count as the device loop of tf_newton_step and the oracle."""
+    t = mesh.small_rectangle()
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    x_ref, it_ref, _ = O.newton_step_dense(t, t.x, vs, inv, tol=t.newton_tol)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14) as s:
+        s.set_inv_fg(inv)
+        s.set_viscosity_surface(vs)
+        x_dev, rc, st = s.updateStepNR(t.x, t.dt)
+        assert rc == capi.TF_OK
+        un = t.x.reshape(-1).copy()
+        uk = un.copy()
+        k, converged = 0, False
+        while not converged:
+            du, rc, _, _ = s.newton_iteration(uk, un, t.dt)
+            assert rc == capi.TF_OK
+            converged = not (np.linalg.norm(du) > t.newton_tol)
+            uk = uk + du
+            k += 1
+            assert k <= 21
+    assert k == st["newton_iters"] == it_ref
+    assert np.abs(uk.reshape(-1, 3) - x_dev).max() <= 1e-12 * t.size
+    assert np.abs(uk.reshape(-1, 3) - x_ref).max() <= 1e-9 * t.size
+
+
+def test_external_force_enters_the_residual_on_free_dofs():
+    """NewtonRaphsonSolver::addExernalForces: gSum += gExt, then the fixed DoFs are zeroed."""
+    t, uk, un, inv = _state(mesh.small_rectangle(nx=7, ny=5))
+    vs = O.viscosity_surfaces(t, uk)
+    f = np.random.default_rng(2).normal(0.0, 50.0, (t.n_nodes, 3))
+    with NewtonRaphsonSolver.from_tissue(t) as s:
+        s.set_inv_fg(inv)
+        s.set_viscosity_surface(vs)
+        g0, J0, _, _, rc0 = s.assemble(uk, un, t.dt)
+        s.set_external_force(f)
+        g1, J1, _, _, rc1 = s.assemble(uk, un, t.dt)
+        s.set_external_force(None)
+        g2, _, _, _, _ = s.assemble(uk, un, t.dt)
+    assert rc0 == rc1 == capi.TF_OK
+    want = np.where(t.fixed.reshape(-1) != 0, 0.0, f.reshape(-1))
+    assert np.abs((g1 - g0) - want).max() <= 1e-12 * np.abs(g0).max()
+    assert _rel(J1, J0) <= 1e-14  # the Jacobian does not see the force (atomic sums may reorder)
+    assert np.abs(g2 - g0).max() <= 1e-12 * np.abs(g0).max()

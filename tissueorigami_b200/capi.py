@@ -49,7 +49,7 @@ EXPORTS = [
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
     "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64",
-    "tf_set_grid_growth", "tf_set_time", "tf_get_time",
+    "tf_set_grid_growth", "tf_set_time", "tf_get_time", "tf_set_external_force", "tf_newton_iteration",
 ]
 
 
@@ -151,6 +151,8 @@ def load(build_if_missing: bool = True):
     L.tf_measure_fp64.argtypes = [c_int, _D]
     L.tf_set_grid_growth.argtypes = [_P, c_int, ctypes.POINTER(GridGrowth), c_int, _D, _D, _I]
     L.tf_set_time.argtypes = [_P, c_double]
+    L.tf_set_external_force.argtypes = [_P, _D]
+    L.tf_newton_iteration.argtypes = [_P, _D, _D, c_double, _D, _I, _D]
     L.tf_get_time.argtypes = [_P, _D]
     L.tf_last_error.argtypes = [_P]
     L.tf_last_error.restype = ctypes.c_char_p

@@ -72,6 +72,8 @@ struct tf_ctx {
     DevBuf uk, un, g, du, r, rhat, p, v, s, t, phat, shat, dinv, partials, sc, dflags;
     DevBuf fg, rates, angles, exposed, peripodial, rotated, xio, barrier;
     DevBuf refine_acc, refine_g;  // tf_solve's iterative refinement: accumulated du, saved g
+    DevBuf ext_force;             // gExt [3N] (tf_set_external_force); used when has_ext_force
+    bool has_ext_force = false;
 
     // grid-based growth functions (tf_set_grid_growth) and the simulation clock that selects the
     // ones active in a step (currSimTimeSec of the reference)
@@ -781,6 +783,7 @@ int assemble_system(tf_ctx* ctx, double dt) {
     na.fixmask = dptr<uint8_t>(ctx->fixmask);
     na.ext_visc = dptr<double>(ctx->ext_visc);
     na.visc_surface = dptr<double>(ctx->visc_surface);
+    na.ext_force = ctx->has_ext_force ? dptr<double>(ctx->ext_force) : nullptr;
     na.dofmap = dptr<int32_t>(ctx->dofmap_d);
     na.diag = dptr<int32_t>(ctx->diag_d);
     na.rowptr = dptr<int32_t>(ctx->rowptr_d);
@@ -1818,7 +1821,7 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->rhat, &ctx->p, &ctx->v, &ctx->s, &ctx->t, &ctx->phat, &ctx->shat, &ctx->dinv,
                      &ctx->partials, &ctx->sc, &ctx->dflags, &ctx->fg, &ctx->rates, &ctx->angles,
                      &ctx->exposed, &ctx->peripodial, &ctx->rotated, &ctx->xio, &ctx->barrier,
-                     &ctx->refine_acc, &ctx->refine_g, &ctx->grid_rel_pos, &ctx->grid_rel_z,
+                     &ctx->refine_acc, &ctx->refine_g, &ctx->ext_force, &ctx->grid_rel_pos, &ctx->grid_rel_z,
                      &ctx->grid_eflags, &ctx->grid_inc};
     for (DevBuf* b : all) dfree(*b);
     for (auto& gf : ctx->grid_funcs) dfree(gf.cells);
@@ -1912,6 +1915,52 @@ int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
     if (changed) return upload_structure(ctx);
     TF_CK(cudaMemcpy(ctx->dofmap_d.p, dm.data(), sizeof(int32_t) * dm.size(), cudaMemcpyHostToDevice));
     return TF_OK;
+}
+
+int tf_set_external_force(tf_ctx* ctx, const double* f) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!f) {
+        ctx->has_ext_force = false;
+        return TF_OK;
+    }
+    TF_CK(dalloc(ctx->ext_force, sizeof(double) * 3 * (size_t)ctx->N));
+    TF_CK(cudaMemcpy(ctx->ext_force.p, f, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyHostToDevice));
+    ctx->has_ext_force = true;
+    return TF_OK;
+}
+
+int tf_newton_iteration(tf_ctx* ctx, const double* uk, const double* un, double dt, double* du, int32_t* iters,
+                        double* rel_res) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    rc = activate_all(ctx);
+    if (rc != TF_OK) return rc;
+    if (!uk || !un || !du || !(dt > 0)) return TF_ERR_ARGUMENT;
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(cudaMemcpyAsync(ctx->uk.p, uk, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->un.p, un, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+    rc = assemble_system(ctx, dt);
+    if (rc != TF_OK) return rc;
+    rc = krylov_solve(ctx);
+    if (rc != TF_OK) return rc;
+    const KrylovScalars sc = *ctx->h_sc;
+    if (!ctx->slave.empty()) {
+        KrylovWork w = make_work(ctx);
+        TF_CK(cudaMemsetAsync(ctx->xio.p, 0, bytes, ctx->stream));  // equate slaves only: scratch positions
+        TF_CK(launch_newton_update(w, dptr<double>(ctx->xio), dptr<int32_t>(ctx->slaves_d), dptr<int32_t>(ctx->masters_d),
+                                   (int32_t)ctx->slave.size(), ctx->stream));
+    }
+    TF_CK(cudaMemcpyAsync(du, ctx->du.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    rc = read_flags(ctx);
+    if (rc != TF_OK) return rc;
+    if (iters) *iters = sc.iter;
+    if (rel_res) *rel_res = sc.bb > 0 ? std::sqrt(sc.rr / sc.bb) : 0.0;
+    if (*ctx->h_flags & DF_PATTERN_MISS) return set_error(ctx, TF_ERR_STATE, "routed entry outside the pattern");
+    if (*ctx->h_flags & DF_NONFINITE) return TF_NONFINITE;
+    if (*ctx->h_flags & DF_INVERTED) return TF_ELEMENT_INVERTED;
+    return krylov_status_to_tf(sc.status);
 }
 
 int tf_set_viscosity_surface(tf_ctx* ctx, const double* visc_surface) {

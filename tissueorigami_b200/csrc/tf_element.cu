@@ -354,6 +354,9 @@ __global__ void k_node_terms(NodeArgs a) {
             const double v = (a.uk[d] - a.un[d]) * inv_dt;
             atomicAdd(dg, surfacePerDt * ev);
             atomicAdd(a.g + md, -((vs * ev) * v));
+            // addExernalForces (NewtonRaphsonSolver.cpp:449-457): gSum += gExt on free DoFs (the
+            // fixed ones are zeroed afterwards by calcutateFixedK), routed like every force
+            if (a.ext_force) atomicAdd(a.g + md, a.ext_force[d]);
         }
         if (md != d) a.vals[(size_t)a.diag[A] * 9 + i * 4] = 1.0;
     }

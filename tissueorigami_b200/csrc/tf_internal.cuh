@@ -89,6 +89,7 @@ struct NodeArgs {
     const uint8_t* fixmask;
     const double* ext_visc;      // [3N]
     const double* visc_surface;  // [N]
+    const double* ext_force;     // [3N] external forces added to g (gExt of the reference), or NULL
     const int32_t* dofmap;
     const int32_t* diag;         // [N] slot of the diagonal block
     const int32_t* rowptr;

@@ -169,6 +169,21 @@ class NewtonRaphsonSolver:
                                             float(dt), capi.dptr(g), capi.dptr(vals)), "tf_assemble", self._h)
         return g, vals, rowptr, colidx, rc
 
+    def set_external_force(self, f=None):
+        """NewtonRaphsonSolver::gExt: external nodal forces [N,3] added to the residual (None: none)."""
+        capi.check(self._L.tf_set_external_force(self._h, capi.dptr(_f64(f).reshape(-1)) if f is not None else None),
+                   "tf_set_external_force", self._h)
+
+    def newton_iteration(self, uk, un, dt: float):
+        """One Newton iteration's assembly and solve on the device (tf_newton_iteration):
+        returns (deltaU [3N], status, BiCGStab iterations, relative residual)."""
+        du = np.zeros(3 * self.n_nodes)
+        it, rr = ctypes.c_int32(), ctypes.c_double()
+        rc = capi.check(self._L.tf_newton_iteration(self._h, capi.dptr(_f64(uk).reshape(-1)), capi.dptr(_f64(un).reshape(-1)),
+                                                    float(dt), capi.dptr(du), ctypes.byref(it), ctypes.byref(rr)),
+                        "tf_newton_iteration", self._h)
+        return du, rc, it.value, rr.value
+
     def solveForDeltaU(self, vals, g):
         """Solve J du = g on the context's pattern (NewtonRaphsonSolver::solveForDeltaU)."""
         du = np.zeros(3 * self.n_nodes)
