@@ -54,6 +54,12 @@ extern "C" {
                                   /* operator per tissue; needs the persistent solve (a one- */
                                   /* tissue context with persistent = 0 uses block-Jacobi)  */
 
+#define TF_KRYLOV_AUTO 0      /* conjugate gradients when J is symmetric (no internal     */
+                              /* viscosity), else BiCGStab (persistent solve)             */
+#define TF_KRYLOV_BICGSTAB 1  /* BiCGStab                                                 */
+#define TF_KRYLOV_CG 2        /* preconditioned conjugate gradients; a tissue whose J turns */
+                              /* out indefinite is solved again with BiCGStab              */
+
 #define TF_SCATTER_AUTO 0     /* pick by the autotuner's cached choice                   */
 #define TF_SCATTER_ATOMIC 1   /* FP64 atomics into the fixed BSR3 pattern                */
 #define TF_SCATTER_COLOURED 2 /* greedy element colouring, plain read-modify-write       */
@@ -89,6 +95,8 @@ typedef struct tf_params {
                               /* Krylov solve (FP64 residual g - J du, a second solve for the */
                               /* correction); 0 = none. The Newton loop needs none: each     */
                               /* Newton iteration corrects the previous one's solve error    */
+    int32_t krylov_method;    /* TF_KRYLOV_*; the persistent solve only (the graph-replayed */
+                              /* and allocation-free paths run BiCGStab)                    */
 } tf_params;
 
 typedef struct tf_step_stats {
@@ -104,13 +112,14 @@ typedef struct tf_step_stats {
     int64_t gpu_launches;       /* kernels this call launched (graph nodes counted)         */
     double ms_solve_kernel;     /* device time inside the persistent BiCGStab launches      */
     int32_t solve_launches;     /* number of those launches                                 */
-    int32_t reserved;
+    int32_t krylov_method;      /* 1 BiCGStab, 2 conjugate gradients, 3 CG fell back to     */
+                                /* BiCGStab on some solve (the largest over the call)       */
 } tf_step_stats;
 
-/* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), BiCGStab
- * rtol 1e-12 with cap 20000, the two-level preconditioner (TF_PRECOND_TWO_LEVEL), autotuned
- * scatter, device 0, graphs on, persistent solve on, smoother block chosen from the mesh, no
- * refinement. */
+/* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), Krylov rtol
+ * 1e-12 with cap 20000, the two-level preconditioner (TF_PRECOND_TWO_LEVEL), autotuned scatter,
+ * device 0, graphs on, persistent solve on, smoother block chosen from the mesh, no refinement,
+ * TF_KRYLOV_AUTO. */
 void tf_default_params(tf_params* p);
 
 /* Library version string. */
@@ -292,6 +301,11 @@ int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* 
  * aggregates would be too large to help), and how many times the coarse operators have been
  * refactorised. */
 int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes);
+
+/* The Krylov method of the last call's linear solves (no counterpart in the reference, whose
+ * Pardiso solve is direct): 1 BiCGStab, 2 conjugate gradients, 3 conjugate gradients that met a
+ * non-positive curvature on some tissue, solved again by BiCGStab; 0 before any solve. */
+int tf_get_krylov_method(tf_ctx* ctx, int32_t* method);
 
 /* Nodes per block of the block-Jacobi smoother the context uses (1: 3x3 node blocks; G > 1:
  * the 3G x 3G diagonal sub-block of G consecutive nodes, a prism column). No counterpart in the

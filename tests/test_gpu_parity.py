@@ -479,3 +479,72 @@ def test_external_force_enters_the_residual_on_free_dofs():
     assert np.abs((g1 - g0) - want).max() <= 1e-12 * np.abs(g0).max()
     assert _rel(J1, J0) <= 1e-14  # the Jacobian does not see the force (atomic sums may reorder)
     assert np.abs(g2 - g0).max() <= 1e-12 * np.abs(g0).max()
+
+
+def _disc_system():
+    t = mesh.small_disc(7, 1500, 1200.0)
+    fg, inv, _, _ = O.grow(t, t.x, t.fg)
+    vs = O.viscosity_surfaces(t, t.x)
+    rowptr, colidx = O.block_pattern(t)
+    vals, g = O.assemble_bsr(t, t.x, t.x, vs, inv, rowptr, colidx)
+    return t, rowptr, colidx, vals, g
+
+
+@pytest.mark.parametrize("precond", [capi.TF_PRECOND_BLOCK_JACOBI, capi.TF_PRECOND_TWO_LEVEL])
+@pytest.mark.parametrize("smoother", [1, 2])
+def test_conjugate_gradients_match_direct_and_bicgstab(precond, smoother):
+    """The persistent solve by conjugate gradients (the default for a symmetric J: no internal
+    viscosity) against SuperLU (1e-8, as BiCGStab) and against BiCGStab on the same system, for
+    node and column smoother blocks, with and without the coarse correction."""
+    t, rowptr, colidx, vals, g = _disc_system()
+    J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
+    du_ref = sla.spsolve(J, g)
+    out = {}
+    for method in (capi.TF_KRYLOV_CG, capi.TF_KRYLOV_BICGSTAB):
+        with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, precond=precond, smoother_nodes=smoother,
+                                             krylov_method=method) as s:
+            du, rc, iters, rr = s.solveForDeltaU(vals, g)
+            assert rc == capi.TF_OK and rr <= 1e-13
+            assert s.krylov_method() == {capi.TF_KRYLOV_CG: 2, capi.TF_KRYLOV_BICGSTAB: 1}[method]
+        out[method] = du
+        assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
+        assert np.all(du[t.fixed.reshape(-1) != 0] == 0.0)
+    assert np.linalg.norm(out[capi.TF_KRYLOV_CG] - out[capi.TF_KRYLOV_BICGSTAB]) / np.linalg.norm(du_ref) < 1e-8
+
+
+def test_conjugate_gradients_fall_back_to_bicgstab_on_an_indefinite_system():
+    """A symmetric but indefinite system (one node's diagonal block negated): the preconditioned
+    residual of CG has (r, M^-1 r) < 0 when the right-hand side sits on that node, CG stops with a
+    non-positive curvature and the library solves the system again with BiCGStab."""
+    t, rowptr, colidx, vals, g = _disc_system()
+    free = np.nonzero(t.fixed.sum(axis=1) == 0)[0]
+    node = int(free[len(free) // 2])
+    k = int(np.nonzero(colidx[rowptr[node]:rowptr[node + 1]] == node)[0][0]) + rowptr[node]
+    vals = vals.copy()
+    vals[k] = -vals[k]
+    g = np.zeros_like(g)
+    g[3 * node:3 * node + 3] = [1.0, -2.0, 0.5]
+    J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes).tocsc()
+    du_ref = sla.spsolve(J, g)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-13, precond=capi.TF_PRECOND_BLOCK_JACOBI,
+                                         krylov_method=capi.TF_KRYLOV_CG) as s:
+        du, rc, iters, rr = s.solveForDeltaU(vals, g)
+        assert s.krylov_method() == 3
+    assert rc == capi.TF_OK and rr <= 1e-13
+    assert np.linalg.norm(du - du_ref) / np.linalg.norm(du_ref) < 1e-8
+
+
+@pytest.mark.parametrize("method", [capi.TF_KRYLOV_CG, capi.TF_KRYLOV_BICGSTAB])
+def test_ten_time_steps_small_rectangle_either_krylov_method(method):
+    t = mesh.small_rectangle()
+    x_ref, _, it_ref, _ = O.simulate_dense(t, n_steps=10)
+    with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14, krylov_method=method) as s:
+        x = t.x.copy()
+        its = []
+        for _ in range(10):
+            x, rc, st = s.runOneStep(x, t.dt)
+            assert rc == capi.TF_OK
+            assert st["krylov_method"] == {capi.TF_KRYLOV_CG: 2, capi.TF_KRYLOV_BICGSTAB: 1}[method]
+            its.append(st["newton_iters"])
+    assert its == it_ref
+    assert np.abs(x - x_ref).max() <= 1e-9 * t.size

@@ -30,6 +30,9 @@ TF_NOALLOC_MAX_NODES = 16384
 TF_PRECOND_BLOCK_JACOBI = 0
 TF_PRECOND_ILU0 = 1
 TF_PRECOND_TWO_LEVEL = 2
+TF_KRYLOV_AUTO = 0
+TF_KRYLOV_BICGSTAB = 1
+TF_KRYLOV_CG = 2
 TF_SCATTER_AUTO = 0
 TF_SCATTER_ATOMIC = 1
 TF_SCATTER_COLOURED = 2
@@ -50,6 +53,7 @@ EXPORTS = [
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
     "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64",
     "tf_set_grid_growth", "tf_set_time", "tf_get_time", "tf_set_external_force", "tf_newton_iteration",
+    "tf_get_krylov_method",
 ]
 
 
@@ -64,7 +68,8 @@ class Params(ctypes.Structure):
                 ("precond", ctypes.c_int32), ("scatter", ctypes.c_int32),
                 ("elems_per_block", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32),
-                ("smoother_nodes", ctypes.c_int32), ("krylov_refine", ctypes.c_int32)]
+                ("smoother_nodes", ctypes.c_int32), ("krylov_refine", ctypes.c_int32),
+                ("krylov_method", ctypes.c_int32)]
 
 
 class GridGrowth(ctypes.Structure):
@@ -81,7 +86,7 @@ class StepStats(ctypes.Structure):
                 ("ms_assemble", ctypes.c_double), ("ms_solve", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("gpu_launches", ctypes.c_int64),
                 ("ms_solve_kernel", ctypes.c_double), ("solve_launches", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("krylov_method", ctypes.c_int32)]
 
     def as_dict(self):
         n = min(self.newton_iters, 32)
@@ -90,7 +95,7 @@ class StepStats(ctypes.Structure):
                 "du_norm": list(self.du_norm[:n]), "krylov_rel_res": list(self.krylov_rel_res[:n]),
                 "ms_assemble": self.ms_assemble, "ms_solve": self.ms_solve, "ms_total": self.ms_total,
                 "gpu_launches": int(self.gpu_launches), "ms_solve_kernel": self.ms_solve_kernel,
-                "solve_launches": int(self.solve_launches)}
+                "solve_launches": int(self.solve_launches), "krylov_method": int(self.krylov_method)}
 
 
 _lib = None
@@ -152,6 +157,7 @@ def load(build_if_missing: bool = True):
     L.tf_set_grid_growth.argtypes = [_P, c_int, ctypes.POINTER(GridGrowth), c_int, _D, _D, _I]
     L.tf_set_time.argtypes = [_P, c_double]
     L.tf_set_external_force.argtypes = [_P, _D]
+    L.tf_get_krylov_method.argtypes = [_P, _I]
     L.tf_newton_iteration.argtypes = [_P, _D, _D, c_double, _D, _I, _D]
     L.tf_get_time.argtypes = [_P, _D]
     L.tf_last_error.argtypes = [_P]

@@ -142,6 +142,7 @@ struct tf_ctx {
     KrylovScalars* h_sc = nullptr;  // pinned
     int32_t* h_flags = nullptr;     // pinned
 
+    int32_t last_method = 0;  // Krylov method of the current call's solves (KM_*; the largest seen)
     int scatter = TF_SCATTER_ATOMIC;
     int teams = 32;
     bool tuned = false;
@@ -714,8 +715,15 @@ int build_plan_all(tf_ctx* ctx) {
     return build_plan(ctx, rows_weight(ctx), all.data());
 }
 
+// Conjugate gradients for the persistent solve: asked for, or left to the library (TF_KRYLOV_AUTO)
+// and every tissue's Jacobian symmetric (no element has internal viscosity).
+bool use_cg(const tf_ctx* c) {
+    return c->params.krylov_method == TF_KRYLOV_CG || (c->params.krylov_method == TF_KRYLOV_AUTO && !c->has_visc);
+}
+
 BatchPlan make_plan(tf_ctx* c) {
     BatchPlan p;
+    p.cg = use_cg(c) ? 1 : 0;
     p.agg_per_cta = (c->coarse_m > 0 && c->coarse_ok) ? c->coarse_m : 0;
     p.n_coarse = c->n_coarse;
     p.node_d = dptr<double>(c->node_d);
@@ -1177,6 +1185,8 @@ int batch_coarse_setup(tf_ctx* ctx) {
         return set_error(ctx, TF_ERR_CUDA, "cublasDgetrfBatched");
     if (cublasDgetriBatched(ctx->cb, ld, (const double* const*)pa, ld, piv, pc, ld, info, T) != CUBLAS_STATUS_SUCCESS)
         return set_error(ctx, TF_ERR_CUDA, "cublasDgetriBatched");
+    TF_CK(launch_symmetrize(dptr<double>(ctx->coarse_inv), ld, ld, (long long)ld * ld, T, ctx->stream));
+    ctx->launches += 1;
     std::vector<int32_t> h_info(T);
     TF_CK(cudaMemcpyAsync(h_info.data(), info, sizeof(int32_t) * T, cudaMemcpyDeviceToHost, ctx->stream));
     TF_CK(cudaStreamSynchronize(ctx->stream));
@@ -1223,7 +1233,8 @@ int coarse_setup(tf_ctx* ctx) {
     TF_CK(launch_set_identity(inv, nc, ctx->stream));
     if (cusolverDnDgetrs(ctx->dn, CUBLAS_OP_T, nc, nc, A, nc, ipiv, inv, nc, info) != CUSOLVER_STATUS_SUCCESS)
         return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrs");
-    ctx->launches += 1;  // k_set_identity
+    TF_CK(launch_symmetrize(inv, nc, nc, 0, 1, ctx->stream));
+    ctx->launches += 2;  // k_set_identity, k_symmetrize
     ctx->coarse_ok = true;
     return TF_OK;
 }
@@ -1282,7 +1293,47 @@ int krylov_solve(tf_ctx* ctx) {
             TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
             return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
         }
+        if (plan.cg) {
+            // Tissues whose conjugate gradients met a non-positive curvature (J indefinite, e.g.
+            // compressed elements whose geometric stiffness outweighs the rest) are solved again by
+            // BiCGStab in a second launch with only them active; the others keep their CG result.
+            std::vector<int32_t> redo(ctx->T, 0);
+            bool any = false;
+            for (int t = 0; t < ctx->T; ++t)
+                if ((ctx->T == 1 || ctx->h_active[t]) && ctx->h_tsc[t].status == KS_INDEFINITE) redo[t] = any = 1;
+            if (any) {
+                BatchPlan p2 = plan;
+                p2.cg = 0;
+                TF_CK(cudaMemcpyAsync(ctx->active_d.p, redo.data(), sizeof(int32_t) * ctx->T, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+                TF_CK(cudaMemsetAsync(ctx->queue_head_d.p, 0, sizeof(int32_t), ctx->stream));
+                TF_CK(cudaEventRecord(ctx->ev_solve[0], ctx->stream));
+                TF_CK(launch_bicgstab_batched(w, p2, ctx->params.krylov_rtol, ctx->params.krylov_max_iters,
+                                              ctx->persist_threads, ctx->stream));
+                TF_CK(cudaEventRecord(ctx->ev_solve[1], ctx->stream));
+                ctx->launches += 1;
+                TF_CK(cudaMemcpyAsync(ctx->active_d.p, ctx->h_active, sizeof(int32_t) * ctx->T, cudaMemcpyHostToDevice,
+                                      ctx->stream));  // the Newton loop's active tissues again
+                TF_CK(cudaMemcpyAsync(ctx->h_tsc, ctx->tscalars.p, sizeof(KrylovScalars) * ctx->T, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+                TF_CK(cudaMemcpyAsync(ctx->h_flags, ctx->dflags.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+                TF_CK(cudaStreamSynchronize(ctx->stream));
+                float kms = 0.0f;
+                TF_CK(cudaEventElapsedTime(&kms, ctx->ev_solve[0], ctx->ev_solve[1]));
+                ctx->solve_kernel_ms += kms;
+                ctx->solve_kernel_launches += 1;
+                if (*ctx->h_flags & DF_BARRIER_TIMEOUT) {
+                    TF_CK(cudaMemsetAsync(ctx->tbarriers.p, 0, sizeof(GridBarrier) * ctx->T, ctx->stream));
+                    TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+                    return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
+                }
+                for (int t = 0; t < ctx->T; ++t)
+                    if (redo[t]) ctx->h_tsc[t].method = KM_CG_FALLBACK;
+            }
+        }
         *ctx->h_sc = ctx->h_tsc[0];
+        for (int t = 0; t < ctx->T; ++t)
+            if (ctx->T == 1 || ctx->h_active[t]) ctx->last_method = std::max(ctx->last_method, ctx->h_tsc[t].method);
         ctx->last_solve_iters = 0;
         for (int t = 0; t < ctx->T; ++t)
             if (ctx->T == 1 || ctx->h_active[t]) ctx->last_solve_iters = std::max(ctx->last_solve_iters, ctx->h_tsc[t].iter);
@@ -1292,6 +1343,7 @@ int krylov_solve(tf_ctx* ctx) {
         }
         return TF_OK;
     }
+    ctx->last_method = std::max<int32_t>(ctx->last_method, KM_BICGSTAB);  // graph-replayed iterations: BiCGStab
     const bool ilu = ctx->params.precond == TF_PRECOND_ILU0;
     if (ilu) {
         TF_CK(cudaMemcpyAsync(ctx->ilu_lu.p, ctx->vals.p, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyDeviceToDevice,
@@ -1483,6 +1535,7 @@ int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
 int call_begin(tf_ctx* ctx, tf_step_stats* st) {
     std::memset(st, 0, sizeof(*st));
     ctx->launches = 0;
+    ctx->last_method = 0;
     ctx->solve_kernel_ms = 0.0;
     ctx->solve_kernel_launches = 0;
     TF_CK(cudaEventRecord(ctx->ev_call[0], ctx->stream));
@@ -1498,6 +1551,7 @@ int call_end(tf_ctx* ctx, tf_step_stats* st) {
     st->gpu_launches = ctx->launches;
     st->ms_solve_kernel = ctx->solve_kernel_ms;
     st->solve_launches = ctx->solve_kernel_launches;
+    st->krylov_method = ctx->last_method;
     return TF_OK;
 }
 
@@ -1579,6 +1633,7 @@ void tf_default_params(tf_params* p) {
     p->persistent = 1;
     p->smoother_nodes = 0;
     p->krylov_refine = 0;
+    p->krylov_method = TF_KRYLOV_AUTO;
 }
 
 const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
@@ -1941,6 +1996,7 @@ int tf_newton_iteration(tf_ctx* ctx, const double* uk, const double* un, double 
     TF_CK(cudaMemcpyAsync(ctx->uk.p, uk, bytes, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemcpyAsync(ctx->un.p, un, bytes, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+    ctx->last_method = 0;
     rc = assemble_system(ctx, dt);
     if (rc != TF_OK) return rc;
     rc = krylov_solve(ctx);
@@ -2045,6 +2101,7 @@ int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, i
     TF_CK(cudaMemcpyAsync(ctx->vals.p, bsr_vals, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemcpyAsync(ctx->g.p, g, bytes, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
+    ctx->last_method = 0;
     rc = krylov_solve(ctx);
     if (rc != TF_OK) return rc;
     KrylovScalars sc = *ctx->h_sc;
@@ -2300,6 +2357,14 @@ int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int3
     if (precond) *precond = ctx->params.precond;
     if (n_coarse) *n_coarse = (ctx->coarse_m > 0 || ctx->bc_active) ? ctx->n_coarse : 0;
     if (coarse_refreshes) *coarse_refreshes = ctx->coarse_refreshes;
+    return TF_OK;
+}
+
+int tf_get_krylov_method(tf_ctx* ctx, int32_t* method) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!method) return TF_ERR_ARGUMENT;
+    *method = ctx->last_method;
     return TF_OK;
 }
 

@@ -36,9 +36,15 @@ constexpr int kElemWords = sizeof(ElemRecord) / 8;  // 52 doubles
 struct KrylovScalars {
     double rho_prev, rho, alpha, omega;
     double bb, rr, tol2, du2;
-    int32_t iter, max_iter, status, finish;
+    int32_t iter, max_iter, status, method;  // method: the Krylov method that produced the result (KM_*)
     uint32_t ticket[6];
     int32_t pad[2];
+};
+
+enum KrylovMethod : int32_t {
+    KM_BICGSTAB = 1,     // BiCGStab
+    KM_CG = 2,           // preconditioned conjugate gradients (symmetric J)
+    KM_CG_FALLBACK = 3,  // CG met a non-positive curvature; BiCGStab solved the system
 };
 
 enum KrylovStatus : int32_t {
@@ -47,6 +53,7 @@ enum KrylovStatus : int32_t {
     KS_MAXIT = 2,
     KS_BREAKDOWN = 3,
     KS_NONFINITE = 4,
+    KS_INDEFINITE = 5,  // conjugate gradients met (p, J p) <= 0 or (r, M^-1 r) <= 0
 };
 
 // Device-side error / outcome bits written by kernels.
@@ -120,6 +127,9 @@ struct BatchPlan {
     // (float*)dinv + g (3G)^2, computed before the launch and applied one DoF per lane; row
     // ranges and aggregates hold whole groups.
     int32_t group;
+    // conjugate gradients instead of BiCGStab (every tissue's J symmetric: no internal viscosity);
+    // a tissue whose CG ends with KS_INDEFINITE is solved again by a BiCGStab launch
+    int32_t cg;
     // tissues solved by one CTA each (the packing CTAs' tissues), heaviest first: once its group
     // tissue (if any) is solved, every CTA takes the next one (atomic ticket in queue_head, zeroed
     // before each launch), so these tissues are spread over the CTAs as they become free
@@ -307,6 +317,8 @@ struct CoarseAssembly {
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
                                    size_t a_cm_doubles, cudaStream_t s);
 cudaError_t launch_set_identity(double* m, int n, cudaStream_t s);
+// m = (m + m^T) / 2 for count matrices of order n, leading dimension ld, stride doubles apart
+cudaError_t launch_symmetrize(double* m, int n, int ld, long long stride, int count, cudaStream_t s);
 // Rows [r0, r1) of part k of n of the rows [b0, b1), cut at multiples of G from b0 (G = 1: the
 // proportional split b0 + L k / n). The persistent solve's CTA row ranges and a single tissue's
 // two-level aggregates are cut this way, so a smoother group never straddles two of them.

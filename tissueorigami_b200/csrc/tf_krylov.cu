@@ -161,7 +161,7 @@ __global__ void k_krylov_init(KrylovWork w, double rtol, int max_iter) {
         sc->tol2 = rtol * rtol * tot[0];
         sc->iter = 0;
         sc->max_iter = max_iter;
-        sc->finish = 0;
+        sc->method = KM_BICGSTAB;
         sc->status = !isfinite(tot[0]) ? KS_NONFINITE : (tot[0] == 0.0 ? KS_CONVERGED : KS_RUNNING);
     }
 }
@@ -429,7 +429,7 @@ __device__ void write_partials(double (&v)[NDOT], double* buf, int local, double
 }
 
 // y = J x for rows [r0, r1) with kGroup lanes per row; returns this thread's share of the
-// dots (rhat,y) [KIND 1] or (s,y), (y,y) [KIND 2].
+// dots (rhat,y) [KIND 1], (s,y), (y,y) [KIND 2] or (p,y) [KIND 3].
 template <int KIND>
 __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, const double* __restrict__ xin,
                                           double* __restrict__ yout, double& d0, double& d1) {
@@ -451,6 +451,8 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
             yout[row * 3 + 2] = y2;
             if (KIND == 1) {
                 d0 += w.rhat[row * 3] * y0 + w.rhat[row * 3 + 1] * y1 + w.rhat[row * 3 + 2] * y2;
+            } else if (KIND == 3) {
+                d0 += w.p[row * 3] * y0 + w.p[row * 3 + 1] * y1 + w.p[row * 3 + 2] * y2;
             } else {
                 d0 += w.s[row * 3] * y0 + w.s[row * 3 + 1] * y1 + w.s[row * 3 + 2] * y2;
                 d1 += y0 * y0 + y1 * y1 + y2 * y2;
@@ -481,6 +483,17 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
     D[6] = (m[3] * m[7] - m[4] * m[6]) * id;
     D[7] = (m[1] * m[6] - m[0] * m[7]) * id;
     D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+// The vector a phase updates and the one its preconditioner writes: BiCGStab's p / phat (PH 0)
+// and s / shat (PH 1); conjugate gradients' r / z (PH 2: r -= alpha q with q in w.v, z in w.phat).
+template <int PH>
+__device__ __forceinline__ double* phase_in(const KrylovWork& w) {
+    return PH == 0 ? w.p : (PH == 1 ? w.s : w.r);
+}
+template <int PH>
+__device__ __forceinline__ double* phase_out(const KrylovWork& w) {
+    return PH == 0 ? w.phat : (PH == 1 ? w.shat : w.phat);
 }
 
 // Smoother groups of G > 1 nodes are handled one DoF per lane: a warp takes 32 / 3G groups at a
@@ -525,8 +538,8 @@ template <int PH>
 __device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, double alpha,
                               double beta, double omega, GridBarrier* bar, int nct, double* red, double* ys,
                               double* cs, const float* cinv, const double* Ms) {
-    double* vin = PH == 0 ? w.p : w.s;
-    double* out = PH == 0 ? w.phat : w.shat;
+    double* vin = phase_in<PH>(w);
+    double* out = phase_out<PH>(w);
     const int m = plan.agg_per_cta, G = plan.group;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int wpa = nw / m;
@@ -660,8 +673,8 @@ __device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc
 template <int PH>
 __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t, int a0, int a1, double alpha,
                               double beta, double omega, GridBarrier* bar, int nct, double* cs) {
-    double* vin = PH == 0 ? w.p : w.s;
-    double* out = PH == 0 ? w.phat : w.shat;
+    double* vin = phase_in<PH>(w);
+    double* out = phase_out<PH>(w);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int G = plan.group;
     for (int a = a0 + warp; a < a1; a += nw) {
@@ -770,6 +783,66 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
     return true;
 }
 
+// The vector update of a phase and the preconditioner applied to it, on the rows this CTA
+// preconditions (its contiguous range [r0, r1), or the node lists of its aggregates [ba0, ba1)
+// for a batch tissue with the two-level preconditioner): PH 0 p = r + beta (p - omega v),
+// phat = M^-1 p; PH 1 s = r - alpha v, shat = M^-1 s (BiCGStab); PH 2 r = r - alpha q (q in v),
+// z = M^-1 r (z in phat; conjugate gradients). Returns false when a group barrier timed out.
+template <int PH>
+__device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int r0, int r1, int ba0,
+                                    int ba1, double alpha, double beta, double omega, GridBarrier* bar, int nct,
+                                    double* red, double* ys, double* cs, const float* cinv_s, const double* Ms) {
+    if (plan.agg_per_cta > 0)
+        return precond_phase<PH>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms);
+    if (plan.batch_coarse) return precond_batch<PH>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs);
+    double* vin = phase_in<PH>(w);
+    double* out = phase_out<PH>(w);
+    if (plan.group > 1) {
+        const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
+        const int g1 = r1 / plan.group;
+        for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
+            const bool valid = gl < gpw && gc + gl < g1;
+            group_dof_update_apply<PH>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, beta, omega, vin, out);
+        }
+        return true;
+    }
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            vin[d] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+        }
+        apply_dinv(w.dinv, n, vin, out);
+    }
+    return true;
+}
+
+// (r, z) and (r, r) over the rows this CTA preconditions (z in phat), after update_precondition<2>.
+__device__ __forceinline__ void precond_rows_dots(const KrylovWork& w, const BatchPlan& plan, int r0, int r1, int ba0,
+                                                  int ba1, double& rz, double& rr) {
+    __syncthreads();  // z of these rows may have been written by another warp of the CTA
+    if (plan.batch_coarse) {
+        const int k0 = plan.agg_ptr[ba0], k1 = plan.agg_ptr[ba1];
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+            const int n = plan.agg_nodes[k];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double r = w.r[n * 3 + i];
+                rz += r * w.phat[n * 3 + i];
+                rr += r * r;
+            }
+        }
+        return;
+    }
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double r = w.r[n * 3 + i];
+            rz += r * w.phat[n * 3 + i];
+            rr += r * r;
+        }
+}
+
 // BiCGStab restart after a breakdown: rhat = r, p = v = 0, rho = (r, r); at most kMaxRestarts
 // per solve. Returns false when the restarts are used up (the caller reports a breakdown).
 constexpr int kMaxRestarts = 8;
@@ -856,28 +929,9 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     while (status == KS_RUNNING) {
         // A: p = r + beta (p - omega v); phat = M^-1 p
         const double beta = (rho / rho_prev) * (alpha / omega);
-        if (plan.agg_per_cta > 0) {
-            if (!precond_phase<0>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
-        } else if (plan.batch_coarse) {
-            if (!precond_batch<0>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs)) return false;
-        } else if (plan.group > 1) {
-            const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
-            const int g1 = r1 / plan.group;
-            for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
-                const bool valid = gl < gpw && gc + gl < g1;
-                group_dof_update_apply<0>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, beta, omega, w.p,
-                                          w.phat);
-            }
-        } else {
-            for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const int d = n * 3 + i;
-                    w.p[d] = w.r[d] + beta * (w.p[d] - omega * w.v[d]);
-                }
-                apply_dinv(w.dinv, n, w.p, w.phat);
-            }
-        }
+        if (!update_precondition<0>(w, plan, t, lc, r0, r1, ba0, ba1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s,
+                                    Ms))
+            return false;
         if (!group_barrier(bar, nct, w.dflags)) return false;
         // B: v = J phat; (rhat, v)
         double d0 = 0.0, d1 = 0.0;
@@ -898,28 +952,8 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
         }
         alpha = rho / t1[0];
         // C: s = r - alpha v; shat = M^-1 s
-        if (plan.agg_per_cta > 0) {
-            if (!precond_phase<1>(w, plan, lc, r0, r1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms)) return false;
-        } else if (plan.batch_coarse) {
-            if (!precond_batch<1>(w, plan, t, ba0, ba1, alpha, 0.0, 0.0, bar, nct, cs)) return false;
-        } else if (plan.group > 1) {
-            const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
-            const int g1 = r1 / plan.group;
-            for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
-                const bool valid = gl < gpw && gc + gl < g1;
-                group_dof_update_apply<1>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, 0.0, 0.0, w.s,
-                                          w.shat);
-            }
-        } else {
-            for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const int d = n * 3 + i;
-                    w.s[d] = w.r[d] - alpha * w.v[d];
-                }
-                apply_dinv(w.dinv, n, w.s, w.shat);
-            }
-        }
+        if (!update_precondition<1>(w, plan, t, lc, r0, r1, ba0, ba1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms))
+            return false;
         if (!group_barrier(bar, nct, w.dflags)) return false;
         // D: t = J shat; (t, s), (t, t)
         d0 = 0.0;
@@ -978,6 +1012,151 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
         sc->iter = it;
         sc->max_iter = max_iter;
         sc->status = status;
+        sc->method = KM_BICGSTAB;
+    }
+    return true;
+}
+
+// Preconditioned conjugate gradients on tissue t by this CTA (CTA lc of the tissue's group), for a
+// symmetric J - no internal viscosity: the elastic tangent, the diagonal drag and the fixed /
+// slave-master elimination are all symmetric - with the symmetric preconditioner of solve_tissue
+// (block-Jacobi inverses, the column smoother's inverses stored symmetrised, the coarse inverse
+// symmetrised). One SpMV per iteration and three group barriers (four with the two-level coarse
+// correction):  p = z + beta p  |  q = J p, (p, q)  |  x += alpha p, r -= alpha q, z = M^-1 r,
+// (r, z), (r, r). Same stopping rule as BiCGStab (||r||^2 <= rtol^2 ||b||^2). When (p, J p) <= 0
+// or (r, z) <= 0 before convergence (J or M not positive definite) the tissue's status is
+// KS_INDEFINITE and the host solves it again with BiCGStab. Returns false when a group barrier
+// timed out.
+__device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int pbase, double rtol,
+                                int max_iter, double* smem, double* sb, double* red, double* ys, double* Ms, double* cs,
+                                float* cinv_s, bool& indefinite) {
+    indefinite = false;
+    if (!plan.active[t]) return true;
+    const int nct = plan.ncta[t];
+    const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
+    int r0, r1;
+    group_split(tr0, tr1, lc, nct, plan.group, r0, r1);
+    int ba0 = 0, ba1 = 0;
+    if (plan.batch_coarse) {
+        const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
+        ba0 = g0 + (int)((long long)na * lc / nct);
+        ba1 = g0 + (int)((long long)na * (lc + 1) / nct);
+    }
+    GridBarrier* bar = plan.barriers + t;
+    double* part[2] = {w.partials + 4 * pbase, w.partials + 4 * pbase + 2 * nct};
+    int pb = 0;
+    if (plan.agg_per_cta > 0) {
+        const size_t cnt = (size_t)6 * plan.agg_per_cta * plan.n_coarse;
+        const double* src = plan.coarse_inv + (size_t)6 * lc * plan.agg_per_cta * plan.n_coarse;
+        for (size_t i = threadIdx.x; i < cnt; i += blockDim.x) cinv_s[i] = (float)src[i];
+        for (int i = threadIdx.x; i < 36 * plan.agg_per_cta; i += blockDim.x)
+            Ms[i] = plan.agg_m[(size_t)lc * plan.agg_per_cta * 36 + i];
+    }
+    // set-up: block-Jacobi inverses, x = 0, r = b, p = q = 0, ||b||^2
+    double v1[1] = {0.0};
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        if (plan.group == 1) block_jacobi_row(w, n);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            const double b = w.b[d];
+            w.x[d] = 0.0;
+            w.r[d] = b;
+            w.p[d] = 0.0;
+            w.v[d] = 0.0;
+            v1[0] += b * b;
+        }
+    }
+    write_partials<1>(v1, part[pb], lc, smem);
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    double t1[1], t2[2];
+    sum_partials<1>(part[pb], nct, t1, smem, sb);
+    pb ^= 1;
+    const double bb = t1[0];
+    const double tol2 = rtol * rtol * bb;
+    double rr = bb, rz = 0.0, alpha = 0.0, beta = 0.0;
+    int it = 0;
+    int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
+    if (status == KS_RUNNING) {  // z = M^-1 r, (r, z)
+        if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, 0.0, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms))
+            return false;
+        double d0 = 0.0, d1 = 0.0;
+        precond_rows_dots(w, plan, r0, r1, ba0, ba1, d0, d1);
+        double v2[2] = {d0, d1};
+        write_partials<2>(v2, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+        sum_partials<2>(part[pb], nct, t2, smem, sb);
+        pb ^= 1;
+        rz = t2[0];
+        if (!isfinite(rz)) status = KS_NONFINITE;
+        else if (!(rz > 0.0)) indefinite = true;
+    }
+    while (status == KS_RUNNING && !indefinite) {
+        // p = z + beta p on the contiguous rows (z of every row is final after the last barrier)
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.p[d] = w.phat[d] + beta * w.p[d];
+            }
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+        // q = J p, (p, q)
+        double d0 = 0.0, d1 = 0.0;
+        spmv_rows<3>(w, r0, r1, w.p, w.v, d0, d1);
+        v1[0] = d0;
+        write_partials<1>(v1, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+        sum_partials<1>(part[pb], nct, t1, smem, sb);
+        pb ^= 1;
+        const double pq = t1[0];
+        if (!isfinite(pq)) { status = KS_NONFINITE; break; }
+        if (!(pq > 0.0)) { indefinite = true; break; }
+        alpha = rz / pq;
+        // x += alpha p; r -= alpha q; z = M^-1 r; (r, z), (r, r)
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.x[d] += alpha * w.p[d];
+            }
+        if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms))
+            return false;
+        d0 = 0.0;
+        d1 = 0.0;
+        precond_rows_dots(w, plan, r0, r1, ba0, ba1, d0, d1);
+        double v2[2] = {d0, d1};
+        write_partials<2>(v2, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+        sum_partials<2>(part[pb], nct, t2, smem, sb);
+        pb ^= 1;
+        const double rz_new = t2[0];
+        rr = t2[1];
+        ++it;
+        if (!isfinite(rz_new) || !isfinite(rr))
+            status = KS_NONFINITE;
+        else if (rr <= tol2)
+            status = KS_CONVERGED;
+        else if (it >= max_iter)
+            status = KS_MAXIT;
+        else if (!(rz_new > 0.0))
+            indefinite = true;
+        beta = rz_new / rz;
+        rz = rz_new;
+    }
+    if (indefinite) status = KS_INDEFINITE;  // the host solves the tissue again with BiCGStab
+    if (lc == 0 && threadIdx.x == 0) {
+        KrylovScalars* sc = plan.scalars + t;
+        sc->bb = bb;
+        sc->rr = rr;
+        sc->rho = rz;
+        sc->rho_prev = 0.0;
+        sc->alpha = alpha;
+        sc->omega = beta;
+        sc->tol2 = tol2;
+        sc->iter = it;
+        sc->max_iter = max_iter;
+        sc->status = status;
+        sc->method = KM_CG;
     }
     return true;
 }
@@ -986,7 +1165,18 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
 // two-level preconditioner, large tissues; up to 80 registers) and four 256-thread CTAs per SM
 // (batches, small block-Jacobi tissues; registers capped at 64 so that 32 warps per SM hide the
 // latency of the memory-bound batched solve).
-template <int THREADS, int MIN_BLOCKS>
+template <int THREADS, int MIN_BLOCKS, bool CG>
+__device__ __forceinline__ bool solve_by(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int pbase,
+                                         double rtol, int max_iter, double* smem, double* sb, double* red, double* ys,
+                                         double* Ms, double* cs, float* cinv_s) {
+    if (CG) {
+        bool indefinite = false;
+        return solve_tissue_cg(w, plan, t, lc, pbase, rtol, max_iter, smem, sb, red, ys, Ms, cs, cinv_s, indefinite);
+    }
+    return solve_tissue(w, plan, t, lc, pbase, rtol, max_iter, smem, sb, red, ys, Ms, cs, cinv_s);
+}
+
+template <int THREADS, int MIN_BLOCKS, bool CG>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
                                                                         int max_iter) {
 
@@ -1003,8 +1193,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(Krylov
     if (j0 < plan.cta_list_ptr[blockIdx.x + 1]) {
         const int t = plan.cta_list[j0];
         if (plan.ncta[t] > 1 &&
-            !solve_tissue(w, plan, t, blockIdx.x - plan.cta0[t], plan.cta0[t], rtol, max_iter, smem, sb, red, ys, Ms,
-                          cs, cinv_s))
+            !solve_by<THREADS, MIN_BLOCKS, CG>(w, plan, t, blockIdx.x - plan.cta0[t], plan.cta0[t], rtol, max_iter, smem,
+                                               sb, red, ys, Ms, cs, cinv_s))
             return;
     }
     // then every CTA takes single-CTA tissues from the queue until it is empty; their partials use
@@ -1015,8 +1205,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(Krylov
         const int q = ticket;
         __syncthreads();
         if (q >= plan.n_queue) break;
-        if (!solve_tissue(w, plan, plan.queue[q], 0, plan.n_cta + blockIdx.x, rtol, max_iter, smem, sb, red, ys, Ms, cs,
-                          cinv_s))
+        if (!solve_by<THREADS, MIN_BLOCKS, CG>(w, plan, plan.queue[q], 0, plan.n_cta + blockIdx.x, rtol, max_iter, smem, sb,
+                                               red, ys, Ms, cs, cinv_s))
             return;
     }
 }
@@ -1291,7 +1481,8 @@ __global__ void __launch_bounds__(128) k_group_jacobi_setup(KrylovWork w, int G)
     if (!ok) atomicOr(w.dflags, DF_SINGULAR_DIAG);
     for (int r = 0; r < n3; ++r)
         for (int c = 0; c < n3; ++c)
-            reinterpret_cast<float*>(w.dinv)[(size_t)g * n3 * n3 + c * n3 + r] = (float)(ok ? B[r][c] : (r == c ? 1.0 : 0.0));
+            reinterpret_cast<float*>(w.dinv)[(size_t)g * n3 * n3 + c * n3 + r] =
+                (float)(ok ? 0.5 * (B[r][c] + B[c][r]) : (r == c ? 1.0 : 0.0));
 }
 
 // One CTA per aggregate a; thread t of a slot s computes entry e = (r, c) of the 6x6 coarse
@@ -1336,6 +1527,22 @@ __global__ void k_coarse_unit(double* a_cm, const int64_t* offsets, int n) {
     if (i < n) a_cm[offsets[i]] = 1.0;
 }
 
+// m = (m + m^T) / 2 for count matrices of order n, leading dimension ld, stride apart: the inverse
+// of the symmetric coarse operator, made exactly symmetric so conjugate gradients see a symmetric
+// preconditioner (the factorisation leaves rounding-level asymmetry).
+__global__ void k_symmetrize(double* m, int n, int ld, long long stride, int count) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per = (long long)n * n;
+    if (i >= per * count) return;
+    const int mat = (int)(i / per);
+    const int r = (int)((i % per) / n), c = (int)(i % n);
+    if (c <= r) return;
+    double* a = m + mat * stride;
+    const double v = 0.5 * (a[(size_t)r * ld + c] + a[(size_t)c * ld + r]);
+    a[(size_t)r * ld + c] = v;
+    a[(size_t)c * ld + r] = v;
+}
+
 __global__ void k_set_identity(double* m, int n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < (size_t)n * n) m[i] = (i % (size_t)(n + 1) == 0) ? 1.0 : 0.0;
@@ -1364,6 +1571,12 @@ cudaError_t launch_group_jacobi_setup(const KrylovWork& w, int G, cudaStream_t s
     return cudaGetLastError();
 }
 
+cudaError_t launch_symmetrize(double* m, int n, int ld, long long stride, int count, cudaStream_t s) {
+    const long long total = (long long)n * n * count;
+    if (total > 0) k_symmetrize<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(m, n, ld, stride, count);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_set_identity(double* m, int n, cudaStream_t s) {
     const size_t total = (size_t)n * n;
     k_set_identity<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(m, n);
@@ -1371,24 +1584,30 @@ cudaError_t launch_set_identity(double* m, int n, cudaStream_t s) {
 }
 
 namespace {
-void (*persist_kernel(int threads))(KrylovWork, BatchPlan, double, int) {
-    return threads == 768 ? k_bicgstab_batched<768, 1> : k_bicgstab_batched<256, 4>;
+void (*persist_kernel(int threads, bool cg))(KrylovWork, BatchPlan, double, int) {
+    if (cg) return threads == 768 ? k_bicgstab_batched<768, 1, true> : k_bicgstab_batched<256, 4, true>;
+    return threads == 768 ? k_bicgstab_batched<768, 1, false> : k_bicgstab_batched<256, 4, false>;
 }
 }  // namespace
 
 int persistent_max_grid(int device, int threads) {
     int sms = 0, occ = 0;
     if (threads != 256 && threads != 768) return 0;
-    const auto kern = persist_kernel(threads);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemBytes) != cudaSuccess)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0) != cudaSuccess) return 0;
-    if (threads == 768) {  // the two-level solve adds its coarse row block: still one CTA per SM
-        int occ_c = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, kern, threads, kCoarseSmemBytes) != cudaSuccess ||
-            occ_c < 1)
+    occ = 1 << 30;
+    for (int cg = 0; cg < 2; ++cg) {  // both methods' builds must fit the same plan
+        const auto kern = persist_kernel(threads, cg != 0);
+        int o = 0;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemBytes) != cudaSuccess)
             return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, threads, 0) != cudaSuccess) return 0;
+        occ = o < occ ? o : occ;
+        if (threads == 768) {  // the two-level solve adds its coarse row block: still one CTA per SM
+            int occ_c = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, kern, threads, kCoarseSmemBytes) != cudaSuccess ||
+                occ_c < 1)
+                return 0;
+        }
     }
     const int want = threads == 768 ? 1 : 4;  // the CTAs per SM each build is compiled for
     return sms * (occ < want ? occ : want);
@@ -1402,7 +1621,7 @@ cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, 
     const size_t smem = plan.agg_per_cta > 0 ? sizeof(float) * 6 * plan.agg_per_cta * (size_t)plan.n_coarse : 0;
     if (smem > (size_t)kCoarseSmemBytes) return cudaErrorInvalidValue;
     if (threads != 256 && threads != 768) return cudaErrorInvalidValue;
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(persist_kernel(threads)), dim3(plan.n_cta),
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(persist_kernel(threads, plan.cg != 0)), dim3(plan.n_cta),
                                        dim3(threads), args, smem, s);
 }
 

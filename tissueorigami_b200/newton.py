@@ -234,6 +234,12 @@ class NewtonRaphsonSolver:
                    "tf_get_preconditioner", self._h)
         return pc.value, nc.value, rf.value
 
+    def krylov_method(self) -> int:
+        """Krylov method of the last call's solves: 1 BiCGStab, 2 CG, 3 CG that fell back to BiCGStab."""
+        m = ctypes.c_int32()
+        capi.check(self._L.tf_get_krylov_method(self._h, ctypes.byref(m)), "tf_get_krylov_method", self._h)
+        return m.value
+
     def smoother_block(self) -> int:
         """Nodes per block of the block-Jacobi smoother (1: 3x3 node blocks; 3: a prism column of
         three nodes, 9x9)."""
