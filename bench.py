@@ -506,6 +506,7 @@ def run_batch(args) -> None:
         dist.barrier()
     clk = clocks.stop()
     pc_info = b.preconditioner() if b is not None else (pc, 0, 0)
+    x_batch = b.split(x.cpu().numpy().reshape(-1, 3)) if b is not None else []
     sb.close()
     t_dev = ms / 1000.0
     if dist:
@@ -518,8 +519,10 @@ def run_batch(args) -> None:
     seq = None
     if world == 1 and not args.no_sequential:
         # sequential baseline: the same tissues one after another, one context each, same steps
-        seq_ms, seq_units = 0.0, 0.0
-        for t in ts:
+        # and the parity check of the batch against them: every tissue's positions after the same
+        # steps, within 1e-9 of the tissue's size
+        seq_ms, seq_units, worst_dev = 0.0, 0.0, 0.0
+        for i, t in enumerate(ts):
             with NewtonRaphsonSolver.from_tissue(t, precond=pc) as s:
                 xx = t.x.copy()
                 for _ in range(args.warmup):
@@ -528,8 +531,10 @@ def run_batch(args) -> None:
                     xx, _, st = s.runOneStep(xx, t.dt)
                     seq_ms += st["ms_total"]
                     seq_units += t.n_elems * st["newton_iters"]
+            worst_dev = max(worst_dev, float(np.abs(x_batch[i] - xx).max()) / t.size)
         seq = {"value": seq_units / (seq_ms / 1000.0), "ms_per_step": seq_ms / args.steps,
-               "tissue_steps_per_s": len(ts) * args.steps / (seq_ms / 1000.0)}
+               "tissue_steps_per_s": len(ts) * args.steps / (seq_ms / 1000.0),
+               "max_position_difference_over_size": worst_dev, "positions_match_1e-9": worst_dev <= 1e-9}
     if rank == 0:
         line = {
             "metric": METRIC, "value": units / t_dev, "unit": UNIT, "n_gpus": world, "steps": args.steps,
