@@ -343,6 +343,13 @@ int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drate
  * every SM. The element kernel's own ceiling: its closed-form tangent is compute-bound. */
 int tf_measure_fp64(int32_t device, double* tflops);
 
+/* Dense inverse utility (no reference counterpart): inverts `count` column-major n x n matrices
+ * `a` of host memory in place on `device` with the Gauss-Jordan kernels that invert the two-level
+ * preconditioner's coarse operators (partial pivoting; one CTA per matrix, or each matrix over a
+ * cooperative grid when `cooperative` != 0). info[t] = 0, or k + 1 when step k of matrix t met a
+ * zero or non-finite pivot (that matrix is then left partly eliminated). */
+int tf_invert_dense(int32_t device, int32_t n, int32_t count, int32_t cooperative, double* a, int32_t* info);
+
 /* Text of the last error recorded on the context (no reference counterpart); with ctx = NULL,
  * the reason the calling thread's last tf_create / tf_batch_create failed. */
 const char* tf_last_error(tf_ctx* ctx);

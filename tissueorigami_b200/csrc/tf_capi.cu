@@ -8,8 +8,6 @@
 // Newton iteration. The linear solve runs as graph-replayed chunks of BiCGStab iterations
 // whose scalars never leave the device.
 #include <cuda_runtime.h>
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <array>
@@ -108,15 +106,14 @@ struct tf_ctx {
     // below serve a single tissue, the bc_* ones further down a batch)
     std::vector<uint8_t> h_fixmask;
     bool coarse_dirty = true;
-    int coarse_m = 0, n_coarse = 0, n_agg = 0, coarse_lwork = 0, n_coarse_empty = 0;
+    int coarse_m = 0, n_coarse = 0, n_agg = 0, n_coarse_empty = 0;
     bool coarse_ok = false;  // the last coarse factorisation succeeded
-    DevBuf pmode_d, coarse_a, coarse_inv, coarse_r, coarse_ipiv, coarse_info, coarse_work;
+    DevBuf pmode_d, coarse_inv, coarse_r, coarse_info, coarse_work;
     DevBuf node_d, node_mask, agg_m;
     int coarse_age = 0, coarse_base_iters = 0;  // solves since the last coarse refresh; iterations of the first
     int last_solve_iters = 0;
     int32_t coarse_refreshes = 0;
     DevBuf ca_agg_slot_ptr, ca_slot_agg, ca_slot_ptr, ca_blk, ca_blk_row, ca_empty;
-    cusolverDnHandle_t dn = nullptr;
     int32_t* h_coarse_info = nullptr;  // pinned
     // two-level preconditioner of a batch: fixed aggregates per tissue, padded per-tissue coarse
     // matrices (leading dimension bc_ld) inverted together by batched LU
@@ -124,9 +121,7 @@ struct tf_ctx {
     int bc_ld = 0;
     int64_t bc_n_unit = 0;
     std::vector<int32_t> bc_tissue_agg0;
-    DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_ptr_a_d, bc_ptr_c_d, bc_info_d,
-        bc_piv_d;
-    cublasHandle_t cb = nullptr;
+    DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_order_d, bc_info_d;
 
     // multicolour block ILU(0) (precond == TF_PRECOND_ILU0)
     std::vector<int32_t> ilu_colour_ptr;
@@ -511,6 +506,12 @@ IluPlan make_ilu(tf_ctx* c) {
     return p;
 }
 
+// Conjugate gradients for the persistent solve: asked for, or left to the library (TF_KRYLOV_AUTO)
+// and every tissue's Jacobian symmetric (no element has internal viscosity).
+bool use_cg(const tf_ctx* c) {
+    return c->params.krylov_method == TF_KRYLOV_CG || (c->params.krylov_method == TF_KRYLOV_AUTO && !c->has_visc);
+}
+
 KrylovWork make_work(tf_ctx* c) {
     KrylovWork w;
     w.n_nodes = c->N;
@@ -713,12 +714,6 @@ std::vector<double> rows_weight(tf_ctx* ctx) {
 int build_plan_all(tf_ctx* ctx) {
     std::vector<int32_t> all(ctx->T, 1);
     return build_plan(ctx, rows_weight(ctx), all.data());
-}
-
-// Conjugate gradients for the persistent solve: asked for, or left to the library (TF_KRYLOV_AUTO)
-// and every tissue's Jacobian symmetric (no element has internal viscosity).
-bool use_cg(const tf_ctx* c) {
-    return c->params.krylov_method == TF_KRYLOV_CG || (c->params.krylov_method == TF_KRYLOV_AUTO && !c->has_visc);
 }
 
 BatchPlan make_plan(tf_ctx* c) {
@@ -992,22 +987,11 @@ int build_coarse(tf_ctx* ctx) {
         const int rc = coarse_space_upload(ctx, agg0, iota, empty);
         if (rc != TF_OK) return rc;
     }
-    TF_CK(dalloc(ctx->coarse_a, sizeof(double) * (size_t)nc * nc));
     TF_CK(dalloc(ctx->coarse_inv, sizeof(double) * (size_t)nc * nc));
     TF_CK(dalloc(ctx->coarse_r, sizeof(double) * (size_t)nc));
-    TF_CK(dalloc(ctx->coarse_ipiv, sizeof(int32_t) * (size_t)nc));
     TF_CK(dalloc(ctx->coarse_info, sizeof(int32_t)));
-    if (!ctx->dn) {
-        if (cusolverDnCreate(&ctx->dn) != CUSOLVER_STATUS_SUCCESS) return set_error(ctx, TF_ERR_CUDA, "cusolverDnCreate");
-        if (cusolverDnSetStream(ctx->dn, ctx->stream) != CUSOLVER_STATUS_SUCCESS)
-            return set_error(ctx, TF_ERR_CUDA, "cusolverDnSetStream");
-    }
-    int lwork = 0;
-    if (cusolverDnDgetrf_bufferSize(ctx->dn, nc, nc, dptr<double>(ctx->coarse_a), nc, &lwork) != CUSOLVER_STATUS_SUCCESS)
-        return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrf_bufferSize");
-    TF_CK(dalloc(ctx->coarse_work, sizeof(double) * (size_t)std::max(lwork, 1)));
+    TF_CK(dalloc(ctx->coarse_work, invert_coop_scratch_bytes(nc)));
     if (!ctx->h_coarse_info) TF_CK(cudaMallocHost(&ctx->h_coarse_info, sizeof(int32_t)));
-    ctx->coarse_lwork = lwork;
     ctx->n_agg = n_agg;
     ctx->n_coarse = nc;
     ctx->n_coarse_empty = (int)empty.size();
@@ -1123,28 +1107,18 @@ int build_batch_coarse(tf_ctx* ctx) {
         if (e == cudaSuccess && bytes) e = cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice);
         return e;
     };
-    TF_CK(dalloc(ctx->coarse_a, sizeof(double) * ld2 * T));
     TF_CK(dalloc(ctx->coarse_inv, sizeof(double) * ld2 * T));
     TF_CK(dalloc(ctx->coarse_r, sizeof(double) * 6 * (size_t)tagg0[T]));
-    TF_CK(dalloc(ctx->bc_piv_d, sizeof(int32_t) * (size_t)ld * T));
     TF_CK(dalloc(ctx->bc_info_d, sizeof(int32_t) * (size_t)T));
-    std::vector<double*> pa(T), pc(T);
-    for (int t = 0; t < T; ++t) {
-        pa[t] = dptr<double>(ctx->coarse_a) + base[t];
-        pc[t] = dptr<double>(ctx->coarse_inv) + base[t];
-    }
-    TF_CK(up(ctx->bc_ptr_a_d, pa.data(), sizeof(double*) * T));
-    TF_CK(up(ctx->bc_ptr_c_d, pc.data(), sizeof(double*) * T));
+    std::vector<int32_t> order(T);  // each tissue's coarse order; the padding beyond it is the identity
+    for (int t = 0; t < T; ++t) order[t] = 6 * (tagg0[t + 1] - tagg0[t]);
+    TF_CK(up(ctx->bc_order_d, order.data(), sizeof(int32_t) * T));
     TF_CK(up(ctx->bc_tissue_agg0_d, tagg0.data(), sizeof(int32_t) * tagg0.size()));
     TF_CK(up(ctx->bc_agg_ptr_d, agg_ptr.data(), sizeof(int32_t) * agg_ptr.size()));
     TF_CK(up(ctx->bc_agg_nodes_d, agg_nodes.data(), sizeof(int32_t) * agg_nodes.size()));
     TF_CK(up(ctx->bc_agg_tissue_d, agg_tissue.data(), sizeof(int32_t) * agg_tissue.size()));
     TF_CK(up(ctx->bc_base_d, base.data(), sizeof(int64_t) * base.size()));
     TF_CK(up(ctx->bc_unit_d, unit.data(), sizeof(int64_t) * unit.size()));
-    if (!ctx->cb) {
-        if (cublasCreate(&ctx->cb) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, TF_ERR_CUDA, "cublasCreate");
-        if (cublasSetStream(ctx->cb, ctx->stream) != CUBLAS_STATUS_SUCCESS) return set_error(ctx, TF_ERR_CUDA, "cublasSetStream");
-    }
     if (!ctx->h_coarse_info) TF_CK(cudaMallocHost(&ctx->h_coarse_info, sizeof(int32_t)));
     ctx->bc_tissue_agg0 = tagg0;
     ctx->bc_ld = ld;
@@ -1174,19 +1148,18 @@ int batch_coarse_setup(tf_ctx* ctx) {
     ca.tissue_base = dptr<int64_t>(ctx->bc_base_d);
     ca.ld = ld;
     ca.empty_offsets = dptr<int64_t>(ctx->bc_unit_d);
-    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), dptr<double>(ctx->coarse_a),
+    // each tissue's operator is written row-major (transposed, in column-major terms), so the
+    // in-place column-major inverse is the row-major inverse the solve reads
+    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), dptr<double>(ctx->coarse_inv),
                                  (size_t)ld * ld * T, ctx->stream));
-    ctx->launches += 1 + (ca.n_empty > 0 ? 1 : 0);  // this library's kernels only (not cuBLAS's)
-    double** pa = dptr<double*>(ctx->bc_ptr_a_d);
-    double** pc = dptr<double*>(ctx->bc_ptr_c_d);
-    int32_t* piv = dptr<int32_t>(ctx->bc_piv_d);
     int32_t* info = dptr<int32_t>(ctx->bc_info_d);
-    if (cublasDgetrfBatched(ctx->cb, ld, pa, ld, piv, info, T) != CUBLAS_STATUS_SUCCESS)
-        return set_error(ctx, TF_ERR_CUDA, "cublasDgetrfBatched");
-    if (cublasDgetriBatched(ctx->cb, ld, (const double* const*)pa, ld, piv, pc, ld, info, T) != CUBLAS_STATUS_SUCCESS)
-        return set_error(ctx, TF_ERR_CUDA, "cublasDgetriBatched");
-    TF_CK(launch_symmetrize(dptr<double>(ctx->coarse_inv), ld, ld, (long long)ld * ld, T, ctx->stream));
-    ctx->launches += 1;
+    TF_CK(launch_invert_batched(dptr<double>(ctx->coarse_inv), dptr<int64_t>(ctx->bc_base_d), dptr<int32_t>(ctx->bc_order_d),
+                                ld, T, info, ctx->stream));
+    ctx->launches += 2 + (ca.n_empty > 0 ? 1 : 0);
+    if (use_cg(ctx)) {  // symmetric J: a symmetric coarse inverse for conjugate gradients
+        TF_CK(launch_symmetrize(dptr<double>(ctx->coarse_inv), ld, ld, (long long)ld * ld, T, ctx->stream));
+        ctx->launches += 1;
+    }
     std::vector<int32_t> h_info(T);
     TF_CK(cudaMemcpyAsync(h_info.data(), info, sizeof(int32_t) * T, cudaMemcpyDeviceToHost, ctx->stream));
     TF_CK(cudaStreamSynchronize(ctx->stream));
@@ -1218,23 +1191,20 @@ int coarse_setup(tf_ctx* ctx) {
     ca.tissue_base = nullptr;
     ca.ld = nc;
     ca.empty_offsets = nullptr;
-    double* A = dptr<double>(ctx->coarse_a);
     double* inv = dptr<double>(ctx->coarse_inv);
-    int32_t* ipiv = dptr<int32_t>(ctx->coarse_ipiv);
     int32_t* info = dptr<int32_t>(ctx->coarse_info);
-    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), A, (size_t)nc * nc, ctx->stream));
-    ctx->launches += 1 + (ca.n_empty > 0 ? 1 : 0);  // this library's kernels only (not cuSOLVER's)
-    if (cusolverDnDgetrf(ctx->dn, nc, nc, A, nc, dptr<double>(ctx->coarse_work), ipiv, info) != CUSOLVER_STATUS_SUCCESS)
-        return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrf");
+    // P^T J P written row-major, inverted in place (column-major terms): the row-major inverse
+    TF_CK(launch_coarse_assemble(make_work(ctx), ca, dptr<double>(ctx->pmode_d), inv, (size_t)nc * nc, ctx->stream));
+    TF_CK(launch_invert_coop(inv, nc, ctx->coarse_work.p, info, ctx->device, ctx->stream));
+    ctx->launches += 3 + (ca.n_empty > 0 ? 1 : 0);
     TF_CK(cudaMemcpyAsync(ctx->h_coarse_info, info, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     TF_CK(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->h_coarse_info < 0) return set_error(ctx, TF_ERR_STATE, "coarse inverse: grid barrier timed out");
     if (*ctx->h_coarse_info != 0) return TF_OK;  // singular: block-Jacobi only
-    // X with A^T X = I is A^-1 in row-major order (the layout the solve reads)
-    TF_CK(launch_set_identity(inv, nc, ctx->stream));
-    if (cusolverDnDgetrs(ctx->dn, CUBLAS_OP_T, nc, nc, A, nc, ipiv, inv, nc, info) != CUSOLVER_STATUS_SUCCESS)
-        return set_error(ctx, TF_ERR_CUDA, "cusolverDnDgetrs");
-    TF_CK(launch_symmetrize(inv, nc, nc, 0, 1, ctx->stream));
-    ctx->launches += 2;  // k_set_identity, k_symmetrize
+    if (use_cg(ctx)) {  // symmetric J: a symmetric coarse inverse for conjugate gradients
+        TF_CK(launch_symmetrize(inv, nc, nc, 0, 1, ctx->stream));
+        ctx->launches += 1;
+    }
     ctx->coarse_ok = true;
     return TF_OK;
 }
@@ -1889,15 +1859,13 @@ void tf_destroy(tf_ctx* ctx) {
                      &ctx->ilu_lo_idx, &ctx->ilu_up_ptr, &ctx->ilu_up_idx, &ctx->ilu_lu, &ctx->ilu_uinv, &ctx->ilu_y};
     for (DevBuf* b : adj) dfree(*b);
     if (ctx->ilu_graph) cudaGraphExecDestroy(ctx->ilu_graph);
-    DevBuf* coarse[] = {&ctx->node_d, &ctx->node_mask, &ctx->agg_m, &ctx->pmode_d, &ctx->coarse_a, &ctx->coarse_inv, &ctx->coarse_r, &ctx->coarse_ipiv,
+    DevBuf* coarse[] = {&ctx->node_d, &ctx->node_mask, &ctx->agg_m, &ctx->pmode_d, &ctx->coarse_inv, &ctx->coarse_r,
                         &ctx->coarse_info, &ctx->coarse_work, &ctx->ca_agg_slot_ptr, &ctx->ca_slot_agg,
                         &ctx->ca_slot_ptr, &ctx->ca_blk, &ctx->ca_blk_row, &ctx->ca_empty};
     for (DevBuf* b : coarse) dfree(*b);
-    if (ctx->dn) cusolverDnDestroy(ctx->dn);
     DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_ptr_d, &ctx->bc_agg_nodes_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
-                     &ctx->bc_ptr_a_d, &ctx->bc_ptr_c_d, &ctx->bc_info_d, &ctx->bc_piv_d};
+                     &ctx->bc_order_d, &ctx->bc_info_d};
     for (DevBuf* b : bcb) dfree(*b);
-    if (ctx->cb) cublasDestroy(ctx->cb);
     if (ctx->h_coarse_info) cudaFreeHost(ctx->h_coarse_info);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);
     if (ctx->h_du2) cudaFreeHost(ctx->h_du2);

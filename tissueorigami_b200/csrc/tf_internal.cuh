@@ -291,7 +291,7 @@ int spmv_grid(int n_nodes);
 // w.partials must hold 4 * plan.n_cta doubles.
 // threads: CTA width, 256 (three CTAs per SM, for batches of many tissues) or 768 (one per SM).
 int persistent_max_grid(int device, int threads);
-// Coarse operator of the two-level preconditioner, column-major dense n_coarse^2: entry
+// Coarse operator of the two-level preconditioner, row-major dense n_coarse^2: entry
 // (6a+r, 6b+c) = sum over the Jacobian blocks k in rows of aggregate a and columns of
 // aggregate b of P_row(k)[:, r]^T J_k P_col(k)[:, c]. Blocks are listed per (aggregate, slot)
 // with slot_agg[slot] = b, summed in list order (deterministic). Coarse unknowns whose mode is
@@ -316,7 +316,17 @@ struct CoarseAssembly {
 };
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
                                    size_t a_cm_doubles, cudaStream_t s);
-cudaError_t launch_set_identity(double* m, int n, cudaStream_t s);
+
+// --- dense inverses of the coarse operators (tf_dense.cu) -------------------------------------
+// In-place Gauss-Jordan inverse with partial pivoting of column-major matrices (a row-major
+// matrix in, its row-major inverse out). Batched: matrix t of order order[t] at a + base[t], leading
+// dimension ld, one CTA each; info[t] = 0, or k + 1 when step k met a zero pivot.
+cudaError_t launch_invert_batched(double* a, const int64_t* base, const int32_t* order, int ld, int count,
+                                  int32_t* info, cudaStream_t s);
+// One n x n matrix over a cooperative grid; scratch holds invert_coop_scratch_bytes(n); *status = 0,
+// k + 1 for a zero pivot at step k, -1 when a grid barrier timed out.
+size_t invert_coop_scratch_bytes(int n);
+cudaError_t launch_invert_coop(double* a, int n, void* scratch, int32_t* status, int device, cudaStream_t s);
 // m = (m + m^T) / 2 for count matrices of order n, leading dimension ld, stride doubles apart
 cudaError_t launch_symmetrize(double* m, int n, int ld, long long stride, int count, cudaStream_t s);
 // Rows [r0, r1) of part k of n of the rows [b0, b1), cut at multiples of G from b0 (G = 1: the

@@ -1512,7 +1512,7 @@ __global__ void k_coarse_assemble(KrylovWork w, CoarseAssembly ca, const double*
             a_cm[ca.tissue_base[tt] + (size_t)C + (size_t)R * ca.ld] = sum;
         } else {
             const int R = 6 * a + r, C = 6 * ca.slot_agg[s] + c;
-            a_cm[(size_t)R + (size_t)C * ca.n_coarse] = sum;
+            a_cm[(size_t)C + (size_t)R * ca.n_coarse] = sum;  // row-major
         }
     }
 }
@@ -1543,11 +1543,6 @@ __global__ void k_symmetrize(double* m, int n, int ld, long long stride, int cou
     a[(size_t)c * ld + r] = v;
 }
 
-__global__ void k_set_identity(double* m, int n) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < (size_t)n * n) m[i] = (i % (size_t)(n + 1) == 0) ? 1.0 : 0.0;
-}
-
 }  // namespace
 
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
@@ -1574,12 +1569,6 @@ cudaError_t launch_group_jacobi_setup(const KrylovWork& w, int G, cudaStream_t s
 cudaError_t launch_symmetrize(double* m, int n, int ld, long long stride, int count, cudaStream_t s) {
     const long long total = (long long)n * n * count;
     if (total > 0) k_symmetrize<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(m, n, ld, stride, count);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_set_identity(double* m, int n, cudaStream_t s) {
-    const size_t total = (size_t)n * n;
-    k_set_identity<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(m, n);
     return cudaGetLastError();
 }
 
