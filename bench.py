@@ -221,7 +221,7 @@ def run_b200(args) -> None:
     L = capi.load()
     t = make_tissue(args.workload)
     precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0,
-               "two_level": capi.TF_PRECOND_TWO_LEVEL}[args.precond]
+               "two_level": capi.TF_PRECOND_TWO_LEVEL, "multilevel": capi.TF_PRECOND_MULTILEVEL}[args.precond]
     s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent,
                                         smoother_nodes=args.smoother_nodes)
     sched = s.autotune(t.x, t.dt)
@@ -256,7 +256,7 @@ def run_b200(args) -> None:
     if args.profile_region:
         torch.cuda.cudart().cudaProfilerStart()
     ms, iters, kry, launches, worst = 0.0, 0, 0, 0, 0
-    solve_ms, solve_launches = 0.0, 0
+    solve_ms, solve_launches, kry_cg, methods = 0.0, 0, 0, set()
     for _ in range(args.steps):
         flush.zero_()  # L2 flush between timed steps (outside the step's event window)
         torch.cuda.synchronize()
@@ -267,6 +267,8 @@ def run_b200(args) -> None:
         launches += st.gpu_launches
         solve_ms += st.ms_solve_kernel
         solve_launches += st.solve_launches
+        kry_cg += st.krylov_iters_cg
+        methods.add(int(st.krylov_method))
         worst = max(worst, rc)
     torch.cuda.synchronize()
     if args.profile_region:
@@ -312,7 +314,10 @@ def run_b200(args) -> None:
 
     # the preconditioner as built by the solves (two-level stands down to block-Jacobi when it cannot help)
     pc_eff, n_coarse, refreshes = s.preconditioner()
-    sched["precond_effective"] = {0: "block_jacobi", 1: "ilu0", 2: "two_level"}.get(pc_eff, pc_eff)
+    sched["precond_effective"] = {0: "block_jacobi", 1: "ilu0", 2: "two_level", 3: "multilevel"}.get(pc_eff, pc_eff)
+    sched["krylov_method"] = {1: "bicgstab", 2: "conjugate gradients",
+                              3: "conjugate gradients, finished by bicgstab on indefinite solves"}.get(max(methods), "none")
+    sched["krylov_iters_cg_share"] = kry_cg / max(kry, 1)
     sched["coarse_unknowns"] = n_coarse
     sched["coarse_refreshes"] = refreshes
     sched["smoother_block_nodes"] = s.smoother_block()
@@ -346,20 +351,34 @@ def run_b200(args) -> None:
     # and three node-wise phases (p/phat: r,p,v,D -> p,phat; s/shat: r,v,D -> s,shat;
     # x/r: x,phat,shat,s,t,rhat -> x,r); plus one setup pass (diagonal inverses, r, rhat, p, v)
     # D^-1 is 72 G bytes per node with blocks of G nodes (a prism column's 3G x 3G inverse); with
-    # G > 1 it is set up by a separate kernel before the launch
+    # G > 1 it is set up by a separate kernel before the launch. Per conjugate-gradient iteration
+    # one SpMV (plus the p re-read of its dot) and three node-wise phases (p = z + beta p:
+    # z,p -> p; x += alpha p: x,p -> x; r -= alpha q, z = D^-1 r with (r,z), (r,r): r,q,D -> r,z
+    # and the two dot vectors re-read).
     G = sched.get("smoother_block_nodes", 1)
     per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 72 * G + 4 * 24 + 72 * G + 8 * 24)
+    per_iter_cg = bytes_spmv + 24.0 * N + N * (3 * 24 + 3 * 24 + 4 * 24 + 72 * G + 2 * 24)
     per_setup = N * ((72.0 + 72 if G == 1 else 0.0) + 24 + 4 * 24)
-    if args.precond == "two_level" and sched.get("coarse_unknowns", 0) > 0:
+    if sched.get("precond_effective") == "two_level" and sched.get("coarse_unknowns", 0) > 0:
         # two applications of the coarse correction per iteration, each reading the node modes
         # (d_i, mask) in the restriction and the prolongation and updating the preconditioned
         # vector once more; the coarse inverse is read once per solve into shared memory
         per_iter += 2.0 * N * (25 + 25 + 48)
+        per_iter_cg += N * (25 + 25 + 48)
         per_setup += 8.0 * sched["coarse_unknowns"] ** 2
+    if sched.get("precond_effective") == "multilevel":
+        # per application: the node modes (d_i, mask) and the leaf node list in the restriction and
+        # the prolongation, the preconditioned vector updated once more, the leaf inverses W_a
+        # (288 bytes a leaf of ~64 nodes); the coarser levels and the top rows are below 1 %
+        ml_app = N * (2 * (24 + 1 + 4) + 48 + 288.0 / 64)
+        per_iter += 2.0 * ml_app
+        per_iter_cg += ml_app
+    kry_bi = kry - kry_cg
     if solve_launches > 0:
-        bytes_solve = (kry * per_iter + solve_launches * per_setup) / solve_launches
+        bytes_solve = (kry_bi * per_iter + kry_cg * per_iter_cg + solve_launches * per_setup) / solve_launches
         r_solve = roof("bicgstab_persistent", bytes_solve, solve_ms / solve_launches)
-        r_solve["bicgstab_iterations_per_launch"] = kry / solve_launches
+        r_solve["krylov_iterations_per_launch"] = kry / solve_launches
+        r_solve["cg_iterations_per_launch"] = kry_cg / solve_launches
         # the element kernel's own bound is FP64, not HBM: the closed-form tangent costs ~15.2 k
         # flops per prism (counted from the kernel: ~640 per Gauss point for F, Fe, J, their
         # inverses and the spatial gradients, 648 for the nodal forces, ~85 per tangent block and
@@ -656,7 +675,7 @@ def main():
     ap.add_argument("--no-sequential", action="store_true",
                     help="batch workload: skip the sequential single-tissue comparison (profiling runs)")
     ap.add_argument("--n-tissues", type=int, default=256, help="tissues of the batch workload")
-    ap.add_argument("--precond", choices=["block_jacobi", "ilu0", "two_level"], default="two_level",
+    ap.add_argument("--precond", choices=["block_jacobi", "ilu0", "two_level", "multilevel"], default="two_level",
                     help="Krylov preconditioner of the single-tissue workloads")
     ap.add_argument("--persistent", type=int, choices=[0, 1], default=1,
                     help="solve path of the single-tissue workloads (tf_params.persistent)")

@@ -52,7 +52,16 @@ extern "C" {
 #define TF_PRECOND_TWO_LEVEL 2    /* default: block-Jacobi + additive coarse correction on  */
                                   /* node-range aggregates with rigid-body modes, one coarse */
                                   /* operator per tissue; needs the persistent solve (a one- */
-                                  /* tissue context with persistent = 0 uses block-Jacobi)  */
+                                  /* tissue context with persistent = 0 uses block-Jacobi). */
+                                  /* A tissue too large for one dense coarse operator (its   */
+                                  /* aggregates would exceed 2048 nodes) takes the          */
+                                  /* multilevel space below instead                         */
+#define TF_PRECOND_MULTILEVEL 3   /* block-Jacobi + additive multilevel coarse correction:   */
+                                  /* rigid-body modes of nested spatial sets (recursive      */
+                                  /* bisection of the prism columns; leaves of ~16 columns,  */
+                                  /* four sets per parent, a dense top of <= 160 sets), all  */
+                                  /* rebuilt from every J; single tissue, persistent solve   */
+                                  /* (a batch uses TF_PRECOND_TWO_LEVEL's space)             */
 
 #define TF_KRYLOV_AUTO 0      /* conjugate gradients when J is symmetric (no internal     */
                               /* viscosity), else BiCGStab (persistent solve)             */
@@ -114,6 +123,8 @@ typedef struct tf_step_stats {
     int32_t solve_launches;     /* number of those launches                                 */
     int32_t krylov_method;      /* 1 BiCGStab, 2 conjugate gradients, 3 CG fell back to     */
                                 /* BiCGStab on some solve (the largest over the call)       */
+    int32_t krylov_iters_cg;    /* the conjugate-gradient iterations in krylov_iters_total  */
+                                /* (persistent solves; the rest are BiCGStab's)            */
 } tf_step_stats;
 
 /* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), Krylov rtol
@@ -296,7 +307,8 @@ int tf_time_step_device(tf_ctx* ctx, const double* d_x_n, double dt, double* d_x
 int tf_get_schedule(tf_ctx* ctx, int32_t* n_colours, int32_t* scatter, int32_t* elems_per_block);
 
 /* The preconditioner the context actually uses (TF_PRECOND_TWO_LEVEL stands down to
- * TF_PRECOND_BLOCK_JACOBI on the non-persistent path), the number of coarse unknowns of the
+ * TF_PRECOND_BLOCK_JACOBI on the non-persistent path and reports TF_PRECOND_MULTILEVEL where it
+ * took the multilevel space), the number of coarse unknowns of the
  * two-level space summed over the tissues (0 until the first solve, and 0 when a single tissue's
  * aggregates would be too large to help), and how many times the coarse operators have been
  * refactorised. */

@@ -536,6 +536,12 @@ def test_conjugate_gradients_fall_back_to_bicgstab_on_an_indefinite_system():
 
 @pytest.mark.parametrize("method", [capi.TF_KRYLOV_CG, capi.TF_KRYLOV_BICGSTAB])
 def test_ten_time_steps_small_rectangle_either_krylov_method(method):
+    """Ten steps of the small rectangle with either Krylov method, against the dense oracle. The
+    first Newton Jacobian of every step has one negative eigenvalue (about -1.9 against a largest
+    of 5.3e4: the rigid in-plane rotation, which only the drag resists, under the compressive
+    prestress of the fresh growth increment), so conjugate gradients may meet a non-positive
+    curvature there and hand the solve to BiCGStab (method 3); the later iterations are positive
+    definite."""
     t = mesh.small_rectangle()
     x_ref, _, it_ref, _ = O.simulate_dense(t, n_steps=10)
     with NewtonRaphsonSolver.from_tissue(t, krylov_rtol=1e-14, krylov_method=method) as s:
@@ -544,7 +550,7 @@ def test_ten_time_steps_small_rectangle_either_krylov_method(method):
         for _ in range(10):
             x, rc, st = s.runOneStep(x, t.dt)
             assert rc == capi.TF_OK
-            assert st["krylov_method"] == {capi.TF_KRYLOV_CG: 2, capi.TF_KRYLOV_BICGSTAB: 1}[method]
+            assert st["krylov_method"] in {capi.TF_KRYLOV_CG: (2, 3), capi.TF_KRYLOV_BICGSTAB: (1,)}[method]
             its.append(st["newton_iters"])
     assert its == it_ref
     assert np.abs(x - x_ref).max() <= 1e-9 * t.size

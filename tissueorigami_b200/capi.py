@@ -30,6 +30,7 @@ TF_NOALLOC_MAX_NODES = 16384
 TF_PRECOND_BLOCK_JACOBI = 0
 TF_PRECOND_ILU0 = 1
 TF_PRECOND_TWO_LEVEL = 2
+TF_PRECOND_MULTILEVEL = 3
 TF_KRYLOV_AUTO = 0
 TF_KRYLOV_BICGSTAB = 1
 TF_KRYLOV_CG = 2
@@ -86,7 +87,7 @@ class StepStats(ctypes.Structure):
                 ("ms_assemble", ctypes.c_double), ("ms_solve", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("gpu_launches", ctypes.c_int64),
                 ("ms_solve_kernel", ctypes.c_double), ("solve_launches", ctypes.c_int32),
-                ("krylov_method", ctypes.c_int32)]
+                ("krylov_method", ctypes.c_int32), ("krylov_iters_cg", ctypes.c_int32)]
 
     def as_dict(self):
         n = min(self.newton_iters, 32)
@@ -95,7 +96,8 @@ class StepStats(ctypes.Structure):
                 "du_norm": list(self.du_norm[:n]), "krylov_rel_res": list(self.krylov_rel_res[:n]),
                 "ms_assemble": self.ms_assemble, "ms_solve": self.ms_solve, "ms_total": self.ms_total,
                 "gpu_launches": int(self.gpu_launches), "ms_solve_kernel": self.ms_solve_kernel,
-                "solve_launches": int(self.solve_launches), "krylov_method": int(self.krylov_method)}
+                "solve_launches": int(self.solve_launches), "krylov_method": int(self.krylov_method),
+                "krylov_iters_cg": int(self.krylov_iters_cg)}
 
 
 _lib = None

@@ -31,6 +31,8 @@ constexpr int kChunk = 32;  // BiCGStab iterations per graph replay / status pol
 constexpr int kCoarseMaxAge = 64;  // solves between refreshes of the two-level coarse operator
 constexpr int kMaxAggNodes = 2048;  // largest useful two-level aggregate (nodes)
 constexpr int kBatchAggNodes = 256;  // aggregate size of a batch tissue's two-level space
+constexpr int kMlLeafCols = 16;      // prism columns per leaf of the multilevel space
+constexpr int kMlTopMax = 160;       // sets of the multilevel space's densely inverted top level
 
 struct DevBuf {
     void* p = nullptr;
@@ -122,6 +124,15 @@ struct tf_ctx {
     int64_t bc_n_unit = 0;
     std::vector<int32_t> bc_tissue_agg0;
     DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_order_d, bc_info_d;
+    // multilevel coarse space of a single tissue (build_ml): leaves, levels, set-up lists
+    bool ml_active = false;
+    int col_G = 1;  // nodes per prism column when the mesh numbers columns consecutively, else 1
+    int ml_levels = 0, ml_n_leaf = 0, ml_n_slots = 0, ml_n_out = 0, ml_n_diag = 0, ml_n_top = 0, ml_nct = 0;
+    int32_t ml_span[kMlMaxLevels] = {0}, ml_count[kMlMaxLevels] = {0}, ml_set0[kMlMaxLevels] = {0};
+    std::vector<int32_t> h_slot_agg, h_agg_slot_ptr;  // host copies of the last coarse_space_upload's slots
+    DevBuf ml_leaf_ptr_d, ml_leaf_nodes_d, ml_cen_d, ml_w_d, ml_top_d, ml_top_work, ml_info_d, ml_leaf_m_d, ml_part_d,
+        ml_pstart_d, ml_first_cta_d, ml_slot_a_d, ml_out_ptr_d, ml_out_slots_d, ml_out_set_d, ml_out_col_d, ml_out_dst_d,
+        ml_pairs_d;
 
     // multicolour block ILU(0) (precond == TF_PRECOND_ILU0)
     std::vector<int32_t> ilu_colour_ptr;
@@ -138,6 +149,7 @@ struct tf_ctx {
     int32_t* h_flags = nullptr;     // pinned
 
     int32_t last_method = 0;  // Krylov method of the current call's solves (KM_*; the largest seen)
+    int64_t cg_iters = 0;     // conjugate-gradient iterations of the current call's solves
     int scatter = TF_SCATTER_ATOMIC;
     int teams = 32;
     bool tuned = false;
@@ -717,8 +729,9 @@ int build_plan_all(tf_ctx* ctx) {
 }
 
 BatchPlan make_plan(tf_ctx* c) {
-    BatchPlan p;
+    BatchPlan p{};
     p.cg = use_cg(c) ? 1 : 0;
+    p.warm = 0;
     p.agg_per_cta = (c->coarse_m > 0 && c->coarse_ok) ? c->coarse_m : 0;
     p.n_coarse = c->n_coarse;
     p.node_d = dptr<double>(c->node_d);
@@ -732,6 +745,26 @@ BatchPlan make_plan(tf_ctx* c) {
     p.agg_ptr = dptr<int32_t>(c->bc_agg_ptr_d);
     p.agg_nodes = dptr<int32_t>(c->bc_agg_nodes_d);
     p.coarse_base = dptr<int64_t>(c->bc_base_d);
+    // the partial-moment slots were laid out for ml_nct CTAs
+    p.ml = (c->ml_active && c->coarse_ok && !c->plan_ncta.empty() && c->plan_ncta[0] == c->ml_nct) ? 1 : 0;
+    if (p.ml) {
+        p.agg_ptr = dptr<int32_t>(c->ml_leaf_ptr_d);
+        p.agg_nodes = dptr<int32_t>(c->ml_leaf_nodes_d);
+    }
+    p.ml_levels = c->ml_levels;
+    p.ml_n_leaf = c->ml_n_leaf;
+    for (int l = 0; l < kMlMaxLevels; ++l) {
+        p.ml_span[l] = c->ml_span[l];
+        p.ml_count[l] = c->ml_count[l];
+        p.ml_set0[l] = c->ml_set0[l];
+    }
+    p.ml_cen = dptr<double>(c->ml_cen_d);
+    p.ml_w = dptr<double>(c->ml_w_d);
+    p.ml_top_inv = dptr<double>(c->ml_top_d);
+    p.ml_leaf_m = dptr<double>(c->ml_leaf_m_d);
+    p.ml_part = dptr<double>(c->ml_part_d);
+    p.ml_pstart = dptr<int32_t>(c->ml_pstart_d);
+    p.ml_first_cta = dptr<int32_t>(c->ml_first_cta_d);
     p.n_tissues = c->T;
     p.n_cta = (int32_t)c->plan_list_ptr.size() - 1;
     p.cta_list_ptr = dptr<int32_t>(c->plan_list_ptr_d);
@@ -827,13 +860,13 @@ int krylov_status_to_tf(int ks) {
 // below 1e-6 of its initial norm dropped and listed in `empty`) of the aggregates with node
 // boundaries agg0, the per-aggregate block lists of the coarse assembly, all uploaded.
 int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg_ptr, const std::vector<int32_t>& agg_nodes,
-                        std::vector<int32_t>& empty) {
+                        std::vector<int32_t>& empty, bool raw = false) {
     const int N = ctx->N, n_agg = (int)agg_ptr.size() - 1;
     std::vector<double> X((size_t)N * 3, 0.0);
     for (int e = 0; e < ctx->E; ++e)
         for (int a = 0; a < 6; ++a)
             for (int d = 0; d < 3; ++d) X[(size_t)ctx->conn[(size_t)e * 6 + a] * 3 + d] = ctx->xref[(size_t)e * 18 + a * 3 + d];
-    std::vector<double> pm((size_t)N * 18, 0.0), nd((size_t)N * 3, 0.0), am((size_t)n_agg * 36, 0.0);
+    std::vector<double> pm(raw ? 0 : (size_t)N * 18, 0.0), nd((size_t)N * 3, 0.0), am(raw ? 0 : (size_t)n_agg * 36, 0.0);
     std::vector<uint8_t> nmask(N, 0);
     empty.clear();
     for (int i = 0; i < N; ++i)
@@ -860,6 +893,7 @@ int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg_ptr, const 
                 if (nmask[node] >> d & 1)
                     for (int q = 0; q < 6; ++q) B[q * len + 3 * i + d] = Bi[d][q];
         }
+        if (raw) continue;  // raw rigid modes (multilevel space): node_d and the mask are all it needs
         // modified Gram-Schmidt (two passes) on the explicit columns, the same operations applied
         // to coefficient vectors, so that the orthonormal columns are B m_q; a mode whose norm
         // falls below 1e-6 of its initial norm is dropped
@@ -933,10 +967,12 @@ int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg_ptr, const 
         if (e == cudaSuccess && bytes) e = cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice);
         return e;
     };
-    TF_CK(up(ctx->pmode_d, pm.data(), sizeof(double) * pm.size()));
+    TF_CK(up(ctx->pmode_d, pm.data(), raw ? 0 : sizeof(double) * pm.size()));
     TF_CK(up(ctx->node_d, nd.data(), sizeof(double) * nd.size()));
     TF_CK(up(ctx->node_mask, nmask.data(), nmask.size()));
-    TF_CK(up(ctx->agg_m, am.data(), sizeof(double) * am.size()));
+    TF_CK(up(ctx->agg_m, am.data(), raw ? 0 : sizeof(double) * am.size()));
+    ctx->h_slot_agg = slot_agg;
+    ctx->h_agg_slot_ptr = agg_slot_ptr;
     TF_CK(up(ctx->ca_agg_slot_ptr, agg_slot_ptr.data(), sizeof(int32_t) * agg_slot_ptr.size()));
     TF_CK(up(ctx->ca_slot_agg, slot_agg.data(), sizeof(int32_t) * slot_agg.size()));
     TF_CK(up(ctx->ca_slot_ptr, slot_ptr.data(), sizeof(int32_t) * slot_ptr.size()));
@@ -948,24 +984,27 @@ int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg_ptr, const 
 }
 
 int build_batch_coarse(tf_ctx* ctx);
+int build_ml(tf_ctx* ctx);
 
 int build_coarse(tf_ctx* ctx) {
     ctx->coarse_dirty = false;
     ctx->coarse_m = 0;
     ctx->bc_active = false;
-    if (ctx->params.precond != TF_PRECOND_TWO_LEVEL) return TF_OK;
+    if (ctx->params.precond != TF_PRECOND_TWO_LEVEL && ctx->params.precond != TF_PRECOND_MULTILEVEL) return TF_OK;
+    ctx->ml_active = false;
     if (ctx->T > 1) return build_batch_coarse(ctx);
     if (ctx->plan_ncta.empty()) return TF_OK;
     const int N = ctx->N, nct = ctx->plan_ncta[0];
     if (nct <= 0) return TF_OK;
+    if (ctx->params.precond == TF_PRECOND_MULTILEVEL) return build_ml(ctx);
     int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
     while (m > 1 && N / (nct * m) < 8) --m;
     // each CTA's 6m rows of the n_coarse = 6 nct m inverse must fit its shared-memory block
     while (m > 1 && (size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) --m;
     if ((size_t)36 * nct * m * m * sizeof(float) > (size_t)kCoarseSmemBytes) return TF_OK;
     // aggregates much larger than this no longer cut the iteration count (measured on the 2 M-node
-    // slab: 6,800-node aggregates left it unchanged); such tissues solve with block-Jacobi alone
-    if (N / (nct * m) > kMaxAggNodes) return TF_OK;
+    // slab: 6,800-node aggregates left it unchanged); such tissues take the multilevel space
+    if (N / (nct * m) > kMaxAggNodes) return build_ml(ctx);
     const int nw = ctx->persist_threads / 32;
     while (m > 1 && nw / m < 1) --m;
     const int n_agg = nct * m, nc = 6 * n_agg;
@@ -1131,6 +1170,234 @@ int build_batch_coarse(tf_ctx* ctx) {
     return TF_OK;
 }
 
+// ---- multilevel coarse space of a single tissue -------------------------------------------
+//
+// The tissue's prism columns (col_G consecutive nodes, or single nodes) are split by recursive
+// coordinate bisection into a power of two of leaves of about kMlLeafCols columns, in the
+// bisection's order, so that 4^k consecutive leaves form a subtree: a compact patch. Level l
+// groups 4^(l-1) consecutive leaves; levels are added until one has at most kMlTopMax sets (at
+// least two levels), whose operator is inverted densely. Every set's six rigid modes are taken
+// about its node centroid. The persistent solve's CTA lc owns the leaves
+// [n_leaf lc / nct, n_leaf (lc + 1) / nct); a set of level >= 2 gets one partial-moment slot for
+// every CTA whose leaves overlap it (pstart / first_cta), so the restriction needs one group
+// barrier and no atomics. The set-up lists name, for every diagonal block below the top and every
+// nonzero block of the top operator, the leaf pairs whose blocks sum into it.
+int build_ml(tf_ctx* ctx) {
+    const int N = ctx->N, nct = ctx->plan_ncta.empty() ? 0 : ctx->plan_ncta[0];
+    if (nct <= 0) return TF_OK;
+    std::vector<double> X((size_t)N * 3, 0.0);
+    for (int e = 0; e < ctx->E; ++e)
+        for (int a = 0; a < 6; ++a)
+            for (int d = 0; d < 3; ++d) X[(size_t)ctx->conn[(size_t)e * 6 + a] * 3 + d] = ctx->xref[(size_t)e * 18 + a * 3 + d];
+    // leaves hold whole smoother groups (the solve's G > 1 path walks them), else whole columns
+    const int cg = ctx->smooth_G > 1 ? ctx->smooth_G : ((ctx->col_G > 1 && N % ctx->col_G == 0) ? ctx->col_G : 1);
+    const int ncol = N / cg;
+    const double want = std::max(1.0, (double)ncol / kMlLeafCols);
+    int n_leaf = 1 << (int)std::lround(std::log2(want));
+    while (n_leaf > ncol) n_leaf >>= 1;
+    if (n_leaf < 2) return TF_OK;  // too small for a coarse space: block-Jacobi alone
+    std::vector<int32_t> reps(ncol), cuts;
+    for (int k = 0; k < ncol; ++k) reps[k] = k * cg;
+    bisect_nodes(X, reps.data(), ncol, n_leaf, cuts);
+    std::vector<int32_t> leaf_ptr(1, 0), leaf_nodes;
+    leaf_nodes.reserve(N);
+    for (int k = 0; k < n_leaf; ++k) {
+        std::sort(reps.begin() + cuts[k], reps.begin() + cuts[k + 1]);
+        for (int q = cuts[k]; q < cuts[k + 1]; ++q)
+            for (int j = 0; j < cg; ++j) leaf_nodes.push_back(reps[q] + j);
+        leaf_ptr.push_back((int32_t)leaf_nodes.size());
+    }
+    if ((int)leaf_nodes.size() != N) return set_error(ctx, TF_ERR_STATE, "multilevel leaves do not cover the nodes");
+    // levels
+    int L = 1;
+    int32_t span[kMlMaxLevels] = {0}, count[kMlMaxLevels] = {0}, set0[kMlMaxLevels] = {0};
+    span[0] = 1;
+    count[0] = n_leaf;
+    do {
+        if (L == kMlMaxLevels) return TF_OK;
+        span[L] = span[L - 1] * 4;
+        count[L] = (n_leaf + span[L] - 1) / span[L];
+        ++L;
+    } while (count[L - 1] > kMlTopMax);
+    for (int l = 1; l < L; ++l) set0[l] = set0[l - 1] + count[l - 1];
+    const int n_sets = set0[L - 1] + count[L - 1], n_top = count[L - 1], n_below = set0[L - 1];
+    // centroids: leaves from their nodes, higher sets node-weighted from their leaves
+    std::vector<double> cen((size_t)n_sets * 3, 0.0);
+    std::vector<double> wsum(n_sets, 0.0);
+    for (int a = 0; a < n_leaf; ++a) {
+        const int n = leaf_ptr[a + 1] - leaf_ptr[a];
+        for (int k = leaf_ptr[a]; k < leaf_ptr[a + 1]; ++k)
+            for (int d = 0; d < 3; ++d) cen[(size_t)a * 3 + d] += X[(size_t)leaf_nodes[k] * 3 + d] / n;
+        for (int l = 1; l < L; ++l) {
+            const int g = set0[l] + a / span[l];
+            for (int d = 0; d < 3; ++d) cen[(size_t)g * 3 + d] += cen[(size_t)a * 3 + d] * n;
+            wsum[g] += n;
+        }
+    }
+    for (int g = count[0]; g < n_sets; ++g)
+        for (int d = 0; d < 3; ++d) cen[(size_t)g * 3 + d] /= std::max(wsum[g], 1.0);
+    // leaf modes and the leaf-pair block lists
+    {
+        std::vector<int32_t> empty;
+        const int rc = coarse_space_upload(ctx, leaf_ptr, leaf_nodes, empty, true);
+        if (rc != TF_OK) return rc;
+    }
+    const std::vector<int32_t>& sptr = ctx->h_agg_slot_ptr;
+    const std::vector<int32_t>& sagg = ctx->h_slot_agg;
+    const int n_slots = (int)sagg.size();
+    std::vector<int32_t> slot_a(n_slots);
+    for (int a = 0; a < n_leaf; ++a)
+        for (int q = sptr[a]; q < sptr[a + 1]; ++q) slot_a[q] = a;
+    // set-up outputs: the diagonal block of every set below the top, then the top's blocks
+    std::vector<int32_t> out_ptr(1, 0), out_slots, out_set, out_col, out_dst;
+    for (int l = 0; l + 1 < L; ++l)
+        for (int S = 0; S < count[l]; ++S) {
+            const int a0 = S * span[l], a1 = std::min(n_leaf, (S + 1) * span[l]);
+            for (int a = a0; a < a1; ++a)
+                for (int q = sptr[a]; q < sptr[a + 1]; ++q)
+                    if (sagg[q] >= a0 && sagg[q] < a1) out_slots.push_back(q);
+            out_ptr.push_back((int32_t)out_slots.size());
+            out_set.push_back(set0[l] + S);
+            out_col.push_back(set0[l] + S);
+            out_dst.push_back(set0[l] + S);
+        }
+    const int n_diag = (int)out_set.size();
+    {
+        const int sp = span[L - 1];
+        std::vector<std::pair<int32_t, int32_t>> items;  // (column top set, slot)
+        for (int S = 0; S < n_top; ++S) {
+            items.clear();
+            for (int a = S * sp; a < std::min(n_leaf, (S + 1) * sp); ++a)
+                for (int q = sptr[a]; q < sptr[a + 1]; ++q) items.push_back({sagg[q] / sp, q});
+            std::sort(items.begin(), items.end());
+            for (size_t k = 0; k < items.size(); ++k) {
+                out_slots.push_back(items[k].second);
+                if (k + 1 == items.size() || items[k + 1].first != items[k].first) {
+                    const int T = items[k].first;
+                    out_ptr.push_back((int32_t)out_slots.size());
+                    out_set.push_back(set0[L - 1] + S);
+                    out_col.push_back(set0[L - 1] + T);
+                    out_dst.push_back(S * n_top + T);
+                }
+            }
+        }
+    }
+    // partial-moment slots of the sets of levels >= 2 for this plan's CTA split
+    std::vector<int32_t> cta_of(n_leaf, 0);
+    for (int c = 0; c < nct; ++c)
+        for (int a = (int)((long long)n_leaf * c / nct); a < (int)((long long)n_leaf * (c + 1) / nct); ++a) cta_of[a] = c;
+    std::vector<int32_t> pstart(n_sets + 1, 0), first_cta(n_sets, 0);
+    for (int l = 0; l < L; ++l)
+        for (int S = 0; S < count[l]; ++S) {
+            const int g = set0[l] + S;
+            int np = 0;
+            if (l > 0) {
+                const int a0 = S * span[l], a1 = std::min(n_leaf, (S + 1) * span[l]);
+                first_cta[g] = cta_of[a0];
+                np = cta_of[a1 - 1] - cta_of[a0] + 1;
+            }
+            pstart[g + 1] = pstart[g] + np;
+        }
+    // every CTA stages the top moments and one motion per overlapping set in the solve's
+    // shared coarse vector
+    for (int c = 0; c < nct; ++c) {
+        const int l0 = (int)((long long)n_leaf * c / nct), l1 = (int)((long long)n_leaf * (c + 1) / nct);
+        int jobs = 0;
+        for (int l = 1; l < L && l1 > l0; ++l) jobs += (l1 - 1) / span[l] - l0 / span[l] + 1;
+        if (6 * (n_top + jobs) > kMaxCoarse) return TF_OK;  // too many levels for the staging: block-Jacobi
+    }
+    auto up = [&](DevBuf& b, const void* h, size_t bytes) -> cudaError_t {
+        cudaError_t e = dalloc(b, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess && bytes) e = cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice);
+        return e;
+    };
+    const int n6 = 6 * n_top;
+    TF_CK(up(ctx->ml_leaf_ptr_d, leaf_ptr.data(), sizeof(int32_t) * leaf_ptr.size()));
+    TF_CK(up(ctx->ml_leaf_nodes_d, leaf_nodes.data(), sizeof(int32_t) * leaf_nodes.size()));
+    TF_CK(up(ctx->ml_cen_d, cen.data(), sizeof(double) * cen.size()));
+    TF_CK(up(ctx->ml_pstart_d, pstart.data(), sizeof(int32_t) * pstart.size()));
+    TF_CK(up(ctx->ml_first_cta_d, first_cta.data(), sizeof(int32_t) * first_cta.size()));
+    TF_CK(up(ctx->ml_slot_a_d, slot_a.data(), sizeof(int32_t) * slot_a.size()));
+    TF_CK(up(ctx->ml_out_ptr_d, out_ptr.data(), sizeof(int32_t) * out_ptr.size()));
+    TF_CK(up(ctx->ml_out_slots_d, out_slots.data(), sizeof(int32_t) * out_slots.size()));
+    TF_CK(up(ctx->ml_out_set_d, out_set.data(), sizeof(int32_t) * out_set.size()));
+    TF_CK(up(ctx->ml_out_col_d, out_col.data(), sizeof(int32_t) * out_col.size()));
+    TF_CK(up(ctx->ml_out_dst_d, out_dst.data(), sizeof(int32_t) * out_dst.size()));
+    TF_CK(dalloc(ctx->ml_w_d, sizeof(double) * 36 * (size_t)std::max(n_below, 1)));
+    TF_CK(dalloc(ctx->ml_top_d, sizeof(double) * (size_t)n6 * n6));
+    TF_CK(dalloc(ctx->ml_top_work, invert_coop_scratch_bytes(n6)));
+    TF_CK(dalloc(ctx->ml_info_d, sizeof(int32_t)));
+    TF_CK(dalloc(ctx->ml_leaf_m_d, sizeof(double) * 6 * (size_t)n_leaf));
+    TF_CK(dalloc(ctx->ml_part_d, sizeof(double) * 6 * (size_t)std::max(pstart[n_sets], 1)));
+    // zero once: a CTA without leaves (more CTAs than leaves) never writes its slots
+    TF_CK(cudaMemset(ctx->ml_part_d.p, 0, sizeof(double) * 6 * (size_t)std::max(pstart[n_sets], 1)));
+    TF_CK(dalloc(ctx->ml_pairs_d, sizeof(double) * 36 * (size_t)std::max(n_slots, 1)));
+    if (!ctx->h_coarse_info) TF_CK(cudaMallocHost(&ctx->h_coarse_info, sizeof(int32_t)));
+    for (int l = 0; l < kMlMaxLevels; ++l) {
+        ctx->ml_span[l] = span[l];
+        ctx->ml_count[l] = count[l];
+        ctx->ml_set0[l] = set0[l];
+    }
+    ctx->ml_levels = L;
+    ctx->ml_n_leaf = n_leaf;
+    ctx->ml_n_slots = n_slots;
+    ctx->ml_n_out = (int)out_set.size();
+    ctx->ml_n_diag = n_diag;
+    ctx->ml_n_top = n_top;
+    ctx->ml_nct = nct;
+    ctx->n_coarse = 6 * n_sets;
+    ctx->ml_active = true;
+    ctx->coarse_age = 0;
+    ctx->coarse_ok = false;
+    return TF_OK;
+}
+
+// The multilevel operators from the current J: leaf-pair blocks, every set's diagonal block and
+// its pseudo-inverse, the top operator and its Gauss-Jordan inverse (symmetrised for conjugate
+// gradients). A singular top operator leaves the solve with block-Jacobi alone (coarse_ok false).
+int ml_setup(tf_ctx* ctx) {
+    ctx->coarse_ok = false;
+    MlSetup m;
+    m.n_slots = ctx->ml_n_slots;
+    m.n_out = ctx->ml_n_out;
+    m.n_diag = ctx->ml_n_diag;
+    m.n_top = ctx->ml_n_top;
+    m.slot_a = dptr<int32_t>(ctx->ml_slot_a_d);
+    m.slot_agg = dptr<int32_t>(ctx->ca_slot_agg);
+    m.slot_ptr = dptr<int32_t>(ctx->ca_slot_ptr);
+    m.blk = dptr<int32_t>(ctx->ca_blk);
+    m.blk_row = dptr<int32_t>(ctx->ca_blk_row);
+    m.node_d = dptr<double>(ctx->node_d);
+    m.node_mask = dptr<uint8_t>(ctx->node_mask);
+    m.leaf_cen = dptr<double>(ctx->ml_cen_d);
+    m.set_cen = dptr<double>(ctx->ml_cen_d);
+    m.out_ptr = dptr<int32_t>(ctx->ml_out_ptr_d);
+    m.out_slots = dptr<int32_t>(ctx->ml_out_slots_d);
+    m.out_set = dptr<int32_t>(ctx->ml_out_set_d);
+    m.out_col = dptr<int32_t>(ctx->ml_out_col_d);
+    m.out_dst = dptr<int32_t>(ctx->ml_out_dst_d);
+    m.pairs = dptr<double>(ctx->ml_pairs_d);
+    m.w_blocks = dptr<double>(ctx->ml_w_d);
+    m.top = dptr<double>(ctx->ml_top_d);
+    m.dflags = dptr<int32_t>(ctx->dflags);
+    TF_CK(launch_ml_setup(make_work(ctx), m, ctx->stream));
+    const int n6 = 6 * ctx->ml_n_top;
+    int32_t* info = dptr<int32_t>(ctx->ml_info_d);
+    TF_CK(launch_invert_coop(m.top, n6, ctx->ml_top_work.p, info, ctx->device, ctx->stream));
+    ctx->launches += 6;  // pairs, blocks, pinv6, top fix, Gauss-Jordan, unswap
+    TF_CK(cudaMemcpyAsync(ctx->h_coarse_info, info, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->h_coarse_info < 0) return set_error(ctx, TF_ERR_STATE, "multilevel top inverse: grid barrier timed out");
+    if (*ctx->h_coarse_info != 0) return TF_OK;  // singular top operator: block-Jacobi only
+    if (use_cg(ctx)) {
+        TF_CK(launch_symmetrize(m.top, n6, n6, 0, 1, ctx->stream));
+        ctx->launches += 1;
+    }
+    ctx->coarse_ok = true;
+    return TF_OK;
+}
+
+
 int batch_coarse_setup(tf_ctx* ctx) {
     const int T = ctx->T, ld = ctx->bc_ld;
     CoarseAssembly ca;
@@ -1210,7 +1477,8 @@ int coarse_setup(tf_ctx* ctx) {
 }
 
 bool use_persistent(tf_ctx* ctx) {
-    return (ctx->params.precond == TF_PRECOND_BLOCK_JACOBI || ctx->params.precond == TF_PRECOND_TWO_LEVEL) &&
+    return (ctx->params.precond == TF_PRECOND_BLOCK_JACOBI || ctx->params.precond == TF_PRECOND_TWO_LEVEL ||
+            ctx->params.precond == TF_PRECOND_MULTILEVEL) &&
            ctx->persistent_grid_max > 0 && (ctx->params.persistent || ctx->T > 1);
 }
 
@@ -1219,7 +1487,9 @@ bool use_persistent(tf_ctx* ctx) {
 int krylov_solve(tf_ctx* ctx) {
     KrylovWork w = make_work(ctx);
     if (use_persistent(ctx)) {
-        if (ctx->params.precond == TF_PRECOND_TWO_LEVEL) {
+        if (ctx->params.precond == TF_PRECOND_TWO_LEVEL || ctx->params.precond == TF_PRECOND_MULTILEVEL) {
+            if (ctx->ml_active && (ctx->plan_ncta.empty() || ctx->plan_ncta[0] != ctx->ml_nct))
+                ctx->coarse_dirty = true;  // the CTA split changed: lay the partial slots out again
             if (ctx->coarse_dirty) {
                 const int crc = build_coarse(ctx);
                 if (crc != TF_OK) return crc;
@@ -1234,6 +1504,14 @@ int krylov_solve(tf_ctx* ctx) {
                 const int crc = coarse_setup(ctx);
                 if (crc != TF_OK) return crc;
                 ctx->coarse_age = 0;
+                ++ctx->coarse_refreshes;
+            }
+            // the multilevel operators are rebuilt from every J (a few set-up kernels, about one
+            // SpMV of traffic): an operator kept from an indefinite first Newton iterate would
+            // leave conjugate gradients an indefinite preconditioner for the positive definite rest
+            if (ctx->ml_active) {
+                const int crc = ml_setup(ctx);
+                if (crc != TF_OK) return crc;
                 ++ctx->coarse_refreshes;
             }
         }
@@ -1264,16 +1542,21 @@ int krylov_solve(tf_ctx* ctx) {
             return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
         }
         if (plan.cg) {
-            // Tissues whose conjugate gradients met a non-positive curvature (J indefinite, e.g.
-            // compressed elements whose geometric stiffness outweighs the rest) are solved again by
-            // BiCGStab in a second launch with only them active; the others keep their CG result.
-            std::vector<int32_t> redo(ctx->T, 0);
+            // Tissues whose conjugate gradients met a non-positive curvature (J indefinite: e.g.
+            // the growth's compressive prestress outweighing the drag on a rigid in-plane rotation)
+            // are finished by BiCGStab in a second launch with only them active, starting from the
+            // iterate and residual CG reached; the others keep their CG result.
+            std::vector<int32_t> redo(ctx->T, 0), cg_iters(ctx->T, 0);
             bool any = false;
             for (int t = 0; t < ctx->T; ++t)
-                if ((ctx->T == 1 || ctx->h_active[t]) && ctx->h_tsc[t].status == KS_INDEFINITE) redo[t] = any = 1;
+                if ((ctx->T == 1 || ctx->h_active[t]) && ctx->h_tsc[t].status == KS_INDEFINITE) {
+                    redo[t] = any = 1;
+                    cg_iters[t] = ctx->h_tsc[t].iter;
+                }
             if (any) {
                 BatchPlan p2 = plan;
                 p2.cg = 0;
+                p2.warm = 1;
                 TF_CK(cudaMemcpyAsync(ctx->active_d.p, redo.data(), sizeof(int32_t) * ctx->T, cudaMemcpyHostToDevice,
                                       ctx->stream));
                 TF_CK(cudaMemsetAsync(ctx->queue_head_d.p, 0, sizeof(int32_t), ctx->stream));
@@ -1298,12 +1581,19 @@ int krylov_solve(tf_ctx* ctx) {
                     return set_error(ctx, TF_ERR_STATE, "persistent solve: grid barrier timed out");
                 }
                 for (int t = 0; t < ctx->T; ++t)
-                    if (redo[t]) ctx->h_tsc[t].method = KM_CG_FALLBACK;
+                    if (redo[t]) {
+                        ctx->h_tsc[t].method = KM_CG_FALLBACK;
+                        ctx->h_tsc[t].iter += cg_iters[t];  // iterations of both methods
+                        ctx->cg_iters += cg_iters[t];
+                    }
             }
         }
         *ctx->h_sc = ctx->h_tsc[0];
         for (int t = 0; t < ctx->T; ++t)
-            if (ctx->T == 1 || ctx->h_active[t]) ctx->last_method = std::max(ctx->last_method, ctx->h_tsc[t].method);
+            if (ctx->T == 1 || ctx->h_active[t]) {
+                ctx->last_method = std::max(ctx->last_method, ctx->h_tsc[t].method);
+                if (ctx->h_tsc[t].method == KM_CG) ctx->cg_iters += ctx->h_tsc[t].iter;
+            }
         ctx->last_solve_iters = 0;
         for (int t = 0; t < ctx->T; ++t)
             if (ctx->T == 1 || ctx->h_active[t]) ctx->last_solve_iters = std::max(ctx->last_solve_iters, ctx->h_tsc[t].iter);
@@ -1506,6 +1796,7 @@ int call_begin(tf_ctx* ctx, tf_step_stats* st) {
     std::memset(st, 0, sizeof(*st));
     ctx->launches = 0;
     ctx->last_method = 0;
+    ctx->cg_iters = 0;
     ctx->solve_kernel_ms = 0.0;
     ctx->solve_kernel_launches = 0;
     TF_CK(cudaEventRecord(ctx->ev_call[0], ctx->stream));
@@ -1522,6 +1813,7 @@ int call_end(tf_ctx* ctx, tf_step_stats* st) {
     st->ms_solve_kernel = ctx->solve_kernel_ms;
     st->solve_launches = ctx->solve_kernel_launches;
     st->krylov_method = ctx->last_method;
+    st->krylov_iters_cg = (int32_t)std::min<int64_t>(ctx->cg_iters, INT32_MAX);
     return TF_OK;
 }
 
@@ -1669,10 +1961,13 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         tf_default_params(&ctx->params);
     // the two-level preconditioner runs in the persistent solve (which a batch always uses); a
     // single tissue solved in chunks stands down to block-Jacobi
-    if (ctx->params.precond == TF_PRECOND_TWO_LEVEL && T == 1 && !ctx->params.persistent)
+    // a batch takes the multilevel choice as two-level (its own per-tissue coarse space)
+    if (ctx->params.precond == TF_PRECOND_MULTILEVEL && T > 1) ctx->params.precond = TF_PRECOND_TWO_LEVEL;
+    if ((ctx->params.precond == TF_PRECOND_TWO_LEVEL || ctx->params.precond == TF_PRECOND_MULTILEVEL) && T == 1 &&
+        !ctx->params.persistent)
         ctx->params.precond = TF_PRECOND_BLOCK_JACOBI;
     if (ctx->params.precond != TF_PRECOND_BLOCK_JACOBI && !(ctx->params.precond == TF_PRECOND_ILU0 && T == 1) &&
-        ctx->params.precond != TF_PRECOND_TWO_LEVEL)
+        ctx->params.precond != TF_PRECOND_TWO_LEVEL && ctx->params.precond != TF_PRECOND_MULTILEVEL)
         return TF_ERR_UNSUPPORTED;
     if (ctx->params.krylov_max_iters <= 0 || ctx->params.max_newton_iters < 0) return TF_ERR_ARGUMENT;
     ctx->device = ctx->params.device;
@@ -1733,7 +2028,8 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         int sms = 0;
         TF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
         ctx->persist_threads = (T == 1 && ((int64_t)ctx->N >= (int64_t)sms * 256 ||
-                                           ctx->params.precond == TF_PRECOND_TWO_LEVEL))
+                                           ctx->params.precond == TF_PRECOND_TWO_LEVEL ||
+                                           ctx->params.precond == TF_PRECOND_MULTILEVEL))
                                    ? 768
                                    : 256;
         ctx->persistent_grid_max = coop ? persistent_max_grid(ctx->device, ctx->persist_threads) : 0;
@@ -1759,7 +2055,8 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
     rc = build_plan_all(ctx);
     if (rc != TF_OK) return rc;
     if (ctx->T > 1 && ctx->persistent_grid_max == 0) return TF_ERR_UNSUPPORTED;
-    if (ctx->params.precond == TF_PRECOND_TWO_LEVEL && ctx->persistent_grid_max == 0)
+    if ((ctx->params.precond == TF_PRECOND_TWO_LEVEL || ctx->params.precond == TF_PRECOND_MULTILEVEL) &&
+        ctx->persistent_grid_max == 0)
         ctx->params.precond = TF_PRECOND_BLOCK_JACOBI;
     ctx->h_fixmask.assign(N, 0);
     if (ctx->params.scatter == TF_SCATTER_COLOURED && ctx->n_colours == 0) return TF_ERR_UNSUPPORTED;
@@ -1779,7 +2076,8 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
             // auto: columns of two or three nodes (the wing disc's three-node columns cut the
             // iterations by 16 %; the large slab's four-node columns cut none and cost 16 % more
             // time per step, so they keep node blocks unless asked for)
-            int cs = sn == 0 ? column_size(ctx) : 1;
+            ctx->col_G = column_size(ctx);
+            int cs = sn == 0 ? ctx->col_G : 1;
             for (int t = 0; t < ctx->T; ++t)
                 if ((ctx->tissue_node0[t + 1] - ctx->tissue_node0[t]) % cs != 0) cs = 1;
             ctx->smooth_G = sn >= 2 ? sn : (cs <= 3 ? cs : 1);
@@ -1866,6 +2164,11 @@ void tf_destroy(tf_ctx* ctx) {
     DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_ptr_d, &ctx->bc_agg_nodes_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
                      &ctx->bc_order_d, &ctx->bc_info_d};
     for (DevBuf* b : bcb) dfree(*b);
+    DevBuf* mlb[] = {&ctx->ml_leaf_ptr_d, &ctx->ml_leaf_nodes_d, &ctx->ml_cen_d, &ctx->ml_w_d, &ctx->ml_top_d,
+                     &ctx->ml_top_work, &ctx->ml_info_d, &ctx->ml_leaf_m_d, &ctx->ml_part_d, &ctx->ml_pstart_d,
+                     &ctx->ml_first_cta_d, &ctx->ml_slot_a_d, &ctx->ml_out_ptr_d, &ctx->ml_out_slots_d,
+                     &ctx->ml_out_set_d, &ctx->ml_out_col_d, &ctx->ml_out_dst_d, &ctx->ml_pairs_d};
+    for (DevBuf* b : mlb) dfree(*b);
     if (ctx->h_coarse_info) cudaFreeHost(ctx->h_coarse_info);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);
     if (ctx->h_du2) cudaFreeHost(ctx->h_du2);
@@ -1965,6 +2268,7 @@ int tf_newton_iteration(tf_ctx* ctx, const double* uk, const double* un, double 
     TF_CK(cudaMemcpyAsync(ctx->un.p, un, bytes, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
     ctx->last_method = 0;
+    ctx->cg_iters = 0;
     rc = assemble_system(ctx, dt);
     if (rc != TF_OK) return rc;
     rc = krylov_solve(ctx);
@@ -2070,6 +2374,7 @@ int tf_solve(tf_ctx* ctx, const double* bsr_vals, const double* g, double* du, i
     TF_CK(cudaMemcpyAsync(ctx->g.p, g, bytes, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemsetAsync(ctx->dflags.p, 0, sizeof(int32_t), ctx->stream));
     ctx->last_method = 0;
+    ctx->cg_iters = 0;
     rc = krylov_solve(ctx);
     if (rc != TF_OK) return rc;
     KrylovScalars sc = *ctx->h_sc;
@@ -2322,8 +2627,8 @@ int tf_time_step(tf_ctx* ctx, const double* x_n, double dt, double* x_out, tf_st
 
 int tf_get_preconditioner(tf_ctx* ctx, int32_t* precond, int32_t* n_coarse, int32_t* coarse_refreshes) {
     if (!ctx) return TF_ERR_ARGUMENT;
-    if (precond) *precond = ctx->params.precond;
-    if (n_coarse) *n_coarse = (ctx->coarse_m > 0 || ctx->bc_active) ? ctx->n_coarse : 0;
+    if (precond) *precond = ctx->ml_active ? TF_PRECOND_MULTILEVEL : ctx->params.precond;
+    if (n_coarse) *n_coarse = (ctx->coarse_m > 0 || ctx->bc_active || ctx->ml_active) ? ctx->n_coarse : 0;
     if (coarse_refreshes) *coarse_refreshes = ctx->coarse_refreshes;
     return TF_OK;
 }

@@ -108,6 +108,8 @@ struct NodeArgs {
     const int32_t* tissue_active;  // [T] (NULL: all active)
 };
 
+constexpr int kMlMaxLevels = 10;  // levels of the multilevel coarse space (leaves .. top)
+
 // CTA plan of the batched persistent solve: tissue t owns CTAs [cta0[t], cta0[t]+ncta[t]) and
 // node rows [row0[t], row0[t+1]); each tissue has its own barrier, scalars and partials
 // (4 doubles per CTA of the tissue, starting at 4*cta0[t]).
@@ -130,6 +132,9 @@ struct BatchPlan {
     // conjugate gradients instead of BiCGStab (every tissue's J symmetric: no internal viscosity);
     // a tissue whose CG ends with KS_INDEFINITE is solved again by a BiCGStab launch
     int32_t cg;
+    // BiCGStab starts from the iterate x and residual r already in the work vectors (those that
+    // conjugate gradients left when it met a non-positive curvature) instead of x = 0, r = b
+    int32_t warm;
     // tissues solved by one CTA each (the packing CTAs' tissues), heaviest first: once its group
     // tissue (if any) is solved, every CTA takes the next one (atomic ticket in queue_head, zeroed
     // before each launch), so these tissues are spread over the CTAs as they become free
@@ -165,6 +170,29 @@ struct BatchPlan {
     const int32_t* agg_ptr;      // [aggregates+1]
     const int32_t* agg_nodes;    // [N] node ids, aggregate after aggregate
     const int64_t* coarse_base;  // [T]
+    // multilevel coarse space of a single tissue (ml = 1; agg_per_cta = batch_coarse = 0): the
+    // tissue's prism columns split by recursive coordinate bisection into ml_n_leaf leaves (node
+    // lists in agg_ptr / agg_nodes, node_d relative to the leaf centroid); a set of level l
+    // (l = 1: the leaves) is ml_span[l-1] consecutive leaves, the top level L = ml_levels is
+    // inverted densely. Every set has the six rigid modes about its centroid (fixed / slave DoFs
+    // zeroed), and
+    //   M^-1 r = D^-1 r + sum_{l < L} sum_S Q_S W_S Q_S^T r + Q_L A_L^-1 Q_L^T r,
+    // W_S the pseudo-inverse of the set's diagonal block Q_S^T J Q_S (an additive multilevel
+    // Schwarz preconditioner, symmetric positive semi-definite for an SPD J). CTA lc of the
+    // tissue's nct applies it on the leaves [n_leaf lc / nct, n_leaf (lc + 1) / nct).
+    int32_t ml;
+    int32_t ml_levels;
+    int32_t ml_n_leaf;
+    int32_t ml_span[kMlMaxLevels];  // leaves per set of each level (4^(l-1))
+    int32_t ml_count[kMlMaxLevels]; // sets of each level
+    int32_t ml_set0[kMlMaxLevels];  // first index of each level's sets in the per-set arrays
+    const double* ml_cen;        // [sets][3] centroids, level after level
+    const double* ml_w;          // [sets below the top][36] W_S row-major (index: set0[l-1] + S)
+    const double* ml_top_inv;    // [6 ml_count[L-1]]^2 row-major inverse of the top operator
+    double* ml_leaf_m;           // [n_leaf][6] raw moments Q_a^T r of the leaves (scratch)
+    double* ml_part;             // [partials][6] per-CTA partial moments of the sets of levels >= 2
+    const int32_t* ml_pstart;    // [sets+1] first partial of each set (levels >= 2)
+    const int32_t* ml_first_cta; // [sets] first CTA of the group whose leaves overlap the set
 };
 
 constexpr int kMaxAggPerCta = 4;
@@ -316,6 +344,41 @@ struct CoarseAssembly {
 };
 cudaError_t launch_coarse_assemble(const KrylovWork& w, const CoarseAssembly& ca, const double* pmode, double* a_cm,
                                    size_t a_cm_doubles, cudaStream_t s);
+
+// --- multilevel coarse space (tf_multilevel.cu) -----------------------------------------------
+// Set-up of the multilevel preconditioner from the current J, every solve:
+//  pairs:  C_s = sum over the blocks k of leaf pair s (row leaf slot_a[s], column leaf
+//          slot_agg[s], blocks listed in slot_ptr / blk / blk_row) of P_i^T J_k P_j, P_i the
+//          masked rigid modes of node i about its leaf centroid (node_d, node_mask); one warp per
+//          pair, 36 sums in fixed order.
+//  blocks: output o (out_ptr / out_slots) = sum over its pairs of T_a^T C_s T_b, T the transport
+//          of a rigid motion from the output's row / column set centroid to the leaf centroids;
+//          output o < n_diag is set out_set[o]'s diagonal block (to W after pinv6), the others
+//          are blocks (out_set[o], out_col[o]) of the dense top operator (6 n_top, row-major).
+//  pinv6:  W = V diag(1 / lambda) V^T over the eigenpairs of the symmetric 6 x 6 block with
+//          lambda > 1e-12 lambda_max (cyclic Jacobi rotations), in place.
+struct MlSetup {
+    int32_t n_slots, n_out, n_diag, n_top;
+    const int32_t* slot_a;
+    const int32_t* slot_agg;
+    const int32_t* slot_ptr;
+    const int32_t* blk;
+    const int32_t* blk_row;
+    const double* node_d;
+    const uint8_t* node_mask;
+    const double* leaf_cen;   // [n_leaf][3]
+    const double* set_cen;    // [sets][3] (indexed by out_set / out_col)
+    const int32_t* out_ptr;   // [n_out+1]
+    const int32_t* out_slots;
+    const int32_t* out_set;   // [n_out] global set index of the row set
+    const int32_t* out_col;   // [n_out] global set index of the column set
+    const int32_t* out_dst;   // [n_out] destination: block index in w_blocks (diag) or top block (S * n_top + T)
+    double* pairs;            // [n_slots][36]
+    double* w_blocks;         // [n_diag][36]
+    double* top;              // [6 n_top]^2
+    int32_t* dflags;
+};
+cudaError_t launch_ml_setup(const KrylovWork& w, const MlSetup& m, cudaStream_t s);
 
 // --- dense inverses of the coarse operators (tf_dense.cu) -------------------------------------
 // In-place Gauss-Jordan inverse with partial pivoting of column-major matrices (a row-major

@@ -788,6 +788,226 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
 // for a batch tissue with the two-level preconditioner): PH 0 p = r + beta (p - omega v),
 // phat = M^-1 p; PH 1 s = r - alpha v, shat = M^-1 s (BiCGStab); PH 2 r = r - alpha q (q in v),
 // z = M^-1 r (z in phat; conjugate gradients). Returns false when a group barrier timed out.
+// The aggregates of tissue t a CTA of its group preconditions (batch two-level space), or its
+// leaves (multilevel space of a single tissue).
+__device__ __forceinline__ void ml_or_batch_range(const BatchPlan& plan, int t, int lc, int nct, int& b0, int& b1) {
+    b0 = b1 = 0;
+    if (plan.batch_coarse) {
+        const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
+        b0 = g0 + (int)((long long)na * lc / nct);
+        b1 = g0 + (int)((long long)na * (lc + 1) / nct);
+    } else if (plan.ml) {
+        b0 = (int)((long long)plan.ml_n_leaf * lc / nct);
+        b1 = (int)((long long)plan.ml_n_leaf * (lc + 1) / nct);
+    }
+}
+
+// Multilevel additive coarse correction (plan.ml) applied by CTA lc of nct on its leaves [l0, l1):
+//  A  the smoother on the leaves' nodes (vin updated, out = D^-1 u) and the raw leaf moments
+//     m_a = sum_i P_i^T u_i (force, torque about the leaf centroid) into ml_leaf_m;
+//  B  the CTA's partial moment of every set of levels 2..L that overlaps its leaves (its leaves'
+//     moments moved to the set centroid: torque += (c_a - c_S) x force) at the CTA's slot;
+//  -- group barrier --
+//  C  every top set's moment (its partials summed in CTA order) into cs[0, 6 n_top); after it in
+//     cs the motion of each overlapping set: W_S m_S below the top, the set's rows of the top
+//     inverse times the top moments at the top;
+//  D  each leaf's motion W_a m_a plus every ancestor's motion moved to the leaf centroid
+//     (u += w x (c_a - c_S)), prolonged to the leaf's nodes: out_i += mask_i o (u + w x d_i).
+// Jobs (level, set) are numbered in level order and dealt to the warps round-robin, the same
+// numbering in C and D. Every sum has a fixed order.
+template <int PH>
+__device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, int l0, int l1, double alpha,
+                           double beta, double omega, GridBarrier* bar, int nct, double* cs) {
+    double* vin = phase_in<PH>(w);
+    double* out = phase_out<PH>(w);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int G = plan.group, L = plan.ml_levels;
+    // A
+    for (int a = l0 + warp; a < l1; a += nw) {
+        const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (G > 1) {  // whole smoother groups, each group's nodes consecutive: one DoF per lane
+            const int n3 = 3 * G, gpw = 32 / n3, gl = lane / n3, rr = lane - gl * n3;
+            const int ng = (k1 - k0) / G;
+            for (int q = 0; q < ng; q += gpw) {
+                const bool valid = gl < gpw && q + gl < ng;
+                const int g = plan.agg_nodes[k0 + (valid ? q + gl : q) * G] / G;
+                const double u = group_dof_update_apply<PH>(w, g, rr, n3, valid, alpha, beta, omega, vin, out);
+                if (valid) {
+                    const int n = g * G + rr / 3, i = rr % 3;
+                    const double ui = ((plan.node_mask[n] >> i) & 1) ? u : 0.0;
+                    const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+                    acc[i] += ui;
+                    if (i == 0) {
+                        acc[4] += dz * ui;
+                        acc[5] -= dy * ui;
+                    } else if (i == 1) {
+                        acc[3] -= dz * ui;
+                        acc[5] += dx * ui;
+                    } else {
+                        acc[3] += dy * ui;
+                        acc[4] -= dx * ui;
+                    }
+                }
+            }
+        }
+        for (int k = k0 + lane; G == 1 && k < k1; k += 32) {
+            const int n = plan.agg_nodes[k];
+            double u[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                u[i] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+                vin[d] = u[i];
+            }
+            apply_dinv(w.dinv, n, vin, out);
+            const int mk = plan.node_mask[n];
+            const double u0 = (mk & 1) ? u[0] : 0.0, u1 = (mk & 2) ? u[1] : 0.0, u2 = (mk & 4) ? u[2] : 0.0;
+            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+            acc[0] += u0;
+            acc[1] += u1;
+            acc[2] += u2;
+            acc[3] += dy * u2 - dz * u1;
+            acc[4] += dz * u0 - dx * u2;
+            acc[5] += dx * u1 - dy * u0;
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            if (lane == q) plan.ml_leaf_m[6 * (size_t)a + q] = acc[q];
+    }
+    __syncthreads();
+    // B
+    int job = 0;
+    for (int lev = 2; lev <= L; ++lev) {
+        const int span = plan.ml_span[lev - 1];
+        const int s0 = l0 / span, s1 = l1 > l0 ? (l1 - 1) / span : s0 - 1;  // none for an empty range
+        for (int S = s0; S <= s1; ++S, ++job) {
+            if (job % nw != warp) continue;
+            const int gS = plan.ml_set0[lev - 1] + S;
+            const double* cS = plan.ml_cen + 3 * (size_t)gS;
+            const int a0 = max(l0, S * span), a1 = min(l1, (S + 1) * span);
+            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int a = a0 + lane; a < a1; a += 32) {
+                const double* m = plan.ml_leaf_m + 6 * (size_t)a;
+                const double* ca = plan.ml_cen + 3 * (size_t)a;
+                const double dx = ca[0] - cS[0], dy = ca[1] - cS[1], dz = ca[2] - cS[2];
+                const double f0 = m[0], f1 = m[1], f2 = m[2];
+                acc[0] += f0;
+                acc[1] += f1;
+                acc[2] += f2;
+                acc[3] += m[3] + dy * f2 - dz * f1;
+                acc[4] += m[4] + dz * f0 - dx * f2;
+                acc[5] += m[5] + dx * f1 - dy * f0;
+            }
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+            double* dst = plan.ml_part + 6 * (size_t)(plan.ml_pstart[gS] + lc - plan.ml_first_cta[gS]);
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (lane == q) dst[q] = acc[q];
+        }
+    }
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    // C
+    const int nt = plan.ml_count[L - 1], gt0 = plan.ml_set0[L - 1], n6 = 6 * nt;
+    for (int e = threadIdx.x; e < n6; e += blockDim.x) {
+        const int gS = gt0 + e / 6, q = e % 6;
+        double v = 0.0;
+        for (int k = plan.ml_pstart[gS]; k < plan.ml_pstart[gS + 1]; ++k) v += __ldcg(plan.ml_part + 6 * (size_t)k + q);
+        cs[e] = v;
+    }
+    __syncthreads();
+    double* ys = cs + n6;
+    job = 0;
+    for (int lev = 2; lev <= L; ++lev) {
+        const int span = plan.ml_span[lev - 1];
+        const int s0 = l0 / span, s1 = l1 > l0 ? (l1 - 1) / span : s0 - 1;  // none for an empty range
+        for (int S = s0; S <= s1; ++S, ++job) {
+            if (job % nw != warp) continue;
+            const int gS = plan.ml_set0[lev - 1] + S;
+            if (lev < L) {
+                double mq = 0.0;
+                if (lane < 6)
+                    for (int k = plan.ml_pstart[gS]; k < plan.ml_pstart[gS + 1]; ++k)
+                        mq += __ldcg(plan.ml_part + 6 * (size_t)k + lane);
+                double m[6];
+#pragma unroll
+                for (int p = 0; p < 6; ++p) m[p] = __shfl_sync(0xffffffffu, mq, p);
+                if (lane < 6) {
+                    const double* W = plan.ml_w + 36 * (size_t)gS + 6 * lane;
+                    double v = 0.0;
+#pragma unroll
+                    for (int p = 0; p < 6; ++p) v += W[p] * m[p];
+                    ys[6 * job + lane] = v;
+                }
+            } else {
+                const double* rows = plan.ml_top_inv + (size_t)(6 * S) * n6;
+                double y[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                for (int c = lane; c < n6; c += 32) {
+                    const double x = cs[c];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) y[q] += __ldg(rows + (size_t)q * n6 + c) * x;
+                }
+#pragma unroll
+                for (int q = 0; q < 6; ++q)
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) y[q] += __shfl_xor_sync(0xffffffffu, y[q], off);
+#pragma unroll
+                for (int q = 0; q < 6; ++q)
+                    if (lane == q) ys[6 * job + q] = y[q];
+            }
+        }
+    }
+    __syncthreads();
+    // D
+    for (int a = l0 + warp; a < l1; a += nw) {
+        const double* ma = plan.ml_leaf_m + 6 * (size_t)a;
+        const double* Wa = plan.ml_w + 36 * (size_t)a;
+        double m[6], y[6];
+#pragma unroll
+        for (int p = 0; p < 6; ++p) m[p] = ma[p];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            double v = 0.0;
+#pragma unroll
+            for (int p = 0; p < 6; ++p) v += __ldg(Wa + q * 6 + p) * m[p];
+            y[q] = v;
+        }
+        const double* ca = plan.ml_cen + 3 * (size_t)a;
+        int jb = 0;
+        for (int lev = 2; lev <= L; ++lev) {
+            const int span = plan.ml_span[lev - 1];
+            const int s0 = l0 / span, s1 = (l1 - 1) / span, S = a / span;  // l1 > l0 here
+            const double* yS = ys + 6 * (jb + S - s0);
+            const double* cS = plan.ml_cen + 3 * (size_t)(plan.ml_set0[lev - 1] + S);
+            const double dx = ca[0] - cS[0], dy = ca[1] - cS[1], dz = ca[2] - cS[2];
+            y[0] += yS[0] + yS[4] * dz - yS[5] * dy;
+            y[1] += yS[1] + yS[5] * dx - yS[3] * dz;
+            y[2] += yS[2] + yS[3] * dy - yS[4] * dx;
+            y[3] += yS[3];
+            y[4] += yS[4];
+            y[5] += yS[5];
+            jb += s1 - s0 + 1;
+        }
+        const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
+        for (int k = k0 + lane; k < k1; k += 32) {
+            const int n = plan.agg_nodes[k];
+            const int mk = plan.node_mask[n];
+            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+            if (mk & 1) out[n * 3] += y[0] + y[4] * dz - y[5] * dy;
+            if (mk & 2) out[n * 3 + 1] += y[1] + y[5] * dx - y[3] * dz;
+            if (mk & 4) out[n * 3 + 2] += y[2] + y[3] * dy - y[4] * dx;
+        }
+    }
+    return true;
+}
+
 template <int PH>
 __device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int r0, int r1, int ba0,
                                     int ba1, double alpha, double beta, double omega, GridBarrier* bar, int nct,
@@ -795,6 +1015,7 @@ __device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, 
     if (plan.agg_per_cta > 0)
         return precond_phase<PH>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms);
     if (plan.batch_coarse) return precond_batch<PH>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs);
+    if (plan.ml) return precond_ml<PH>(w, plan, lc, ba0, ba1, alpha, beta, omega, bar, nct, cs);
     double* vin = phase_in<PH>(w);
     double* out = phase_out<PH>(w);
     if (plan.group > 1) {
@@ -821,7 +1042,7 @@ __device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, 
 __device__ __forceinline__ void precond_rows_dots(const KrylovWork& w, const BatchPlan& plan, int r0, int r1, int ba0,
                                                   int ba1, double& rz, double& rr) {
     __syncthreads();  // z of these rows may have been written by another warp of the CTA
-    if (plan.batch_coarse) {
+    if (plan.batch_coarse || plan.ml) {
         const int k0 = plan.agg_ptr[ba0], k1 = plan.agg_ptr[ba1];
         for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
             const int n = plan.agg_nodes[k];
@@ -884,12 +1105,8 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
     const int tr0 = plan.row0[t], tr1 = plan.row0[t + 1];
     int r0, r1;
     group_split(tr0, tr1, lc, nct, plan.group, r0, r1);
-    int ba0 = 0, ba1 = 0;  // this CTA's aggregates of a batch tissue with the two-level preconditioner
-    if (plan.batch_coarse) {
-        const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
-        ba0 = g0 + (int)((long long)na * lc / nct);
-        ba1 = g0 + (int)((long long)na * (lc + 1) / nct);
-    }
+    int ba0 = 0, ba1 = 0;  // this CTA's aggregates of a batch tissue / leaves of the multilevel space
+    ml_or_batch_range(plan, t, lc, nct, ba0, ba1);
     GridBarrier* bar = plan.barriers + t;
     double* part[2] = {w.partials + 4 * pbase, w.partials + 4 * pbase + 2 * nct};
     int pb = 0;
@@ -900,32 +1117,39 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
         for (int i = threadIdx.x; i < 36 * plan.agg_per_cta; i += blockDim.x)
             Ms[i] = plan.agg_m[(size_t)lc * plan.agg_per_cta * 36 + i];
     }
-    // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2
-    double v1[1] = {0.0};
+    // phase 0: block-Jacobi inverses, x = 0, r = rhat = b, p = v = 0, ||b||^2; warm start (the
+    // iterate x and residual r that conjugate gradients left): x, r kept, rhat = r, ||r||^2
+    double v0[2] = {0.0, 0.0};
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
         if (plan.group == 1) block_jacobi_row(w, n);  // G > 1: inverses set up before the launch
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const int d = n * 3 + i;
             const double b = w.b[d];
-            w.x[d] = 0.0;
-            w.r[d] = b;
-            w.rhat[d] = b;
+            double r = b;
+            if (plan.warm)
+                r = w.r[d];
+            else
+                w.x[d] = 0.0;
+            w.r[d] = r;
+            w.rhat[d] = r;
             w.p[d] = 0.0;
             w.v[d] = 0.0;
-            v1[0] += b * b;
+            v0[0] += b * b;
+            v0[1] += r * r;
         }
     }
-    write_partials<1>(v1, part[pb], lc, smem);
+    write_partials<2>(v0, part[pb], lc, smem);
     if (!group_barrier(bar, nct, w.dflags)) return false;
-    double t1[1], t2[2];
-    sum_partials<1>(part[pb], nct, t1, smem, sb);
+    double v1[1], t1[1], t2[2];
+    sum_partials<2>(part[pb], nct, t2, smem, sb);
     pb ^= 1;
-    const double bb = t1[0];
-    double rho = bb, rho_prev = 1.0, alpha = 1.0, omega = 1.0, rr = bb;
+    const double bb = t2[0];
+    double rr = t2[1];
+    double rho = rr, rho_prev = 1.0, alpha = 1.0, omega = 1.0;
     const double tol2 = rtol * rtol * bb;
     int it = 0, restarts = 0;
-    int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
+    int status = !isfinite(bb) || !isfinite(rr) ? KS_NONFINITE : (rr <= tol2 ? KS_CONVERGED : KS_RUNNING);
     while (status == KS_RUNNING) {
         // A: p = r + beta (p - omega v); phat = M^-1 p
         const double beta = (rho / rho_prev) * (alpha / omega);
@@ -1025,7 +1249,7 @@ __device__ bool solve_tissue(const KrylovWork& w, const BatchPlan& plan, int t, 
 // correction):  p = z + beta p  |  q = J p, (p, q)  |  x += alpha p, r -= alpha q, z = M^-1 r,
 // (r, z), (r, r). Same stopping rule as BiCGStab (||r||^2 <= rtol^2 ||b||^2). When (p, J p) <= 0
 // or (r, z) <= 0 before convergence (J or M not positive definite) the tissue's status is
-// KS_INDEFINITE and the host solves it again with BiCGStab. Returns false when a group barrier
+// KS_INDEFINITE and the host finishes it with BiCGStab from the iterate reached. Returns false when a group barrier
 // timed out.
 __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int pbase, double rtol,
                                 int max_iter, double* smem, double* sb, double* red, double* ys, double* Ms, double* cs,
@@ -1037,11 +1261,7 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
     int r0, r1;
     group_split(tr0, tr1, lc, nct, plan.group, r0, r1);
     int ba0 = 0, ba1 = 0;
-    if (plan.batch_coarse) {
-        const int g0 = plan.tissue_agg0[t], na = plan.tissue_agg0[t + 1] - g0;
-        ba0 = g0 + (int)((long long)na * lc / nct);
-        ba1 = g0 + (int)((long long)na * (lc + 1) / nct);
-    }
+    ml_or_batch_range(plan, t, lc, nct, ba0, ba1);
     GridBarrier* bar = plan.barriers + t;
     double* part[2] = {w.partials + 4 * pbase, w.partials + 4 * pbase + 2 * nct};
     int pb = 0;
