@@ -38,7 +38,7 @@ METRIC = "prism assemblies/s (FP64 implicit Newton step)"
 UNIT = "prisms*assemblies/s"
 
 
-def make_tissue(name: str):
+def make_tissue(name: str, slab_grid: str = "1000x500"):
     from tissueorigami_b200 import mesh
 
     if name == "wing_disc":
@@ -46,7 +46,8 @@ def make_tissue(name: str):
     if name == "small_rectangle":
         return mesh.small_rectangle()
     if name == "large_slab":
-        return mesh.large_slab()
+        nx, ny = (int(v) for v in slab_grid.lower().split("x"))
+        return mesh.large_slab(nx=nx, ny=ny)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -107,7 +108,7 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    t = make_tissue(args.workload)
+    t = make_tissue(args.workload, args.slab_grid)
     for _ in range(args.warmup):
         cpu_assembly_rate(t, seconds=1.0)
     rates, samples, secs = [], [], 0.0
@@ -219,7 +220,7 @@ def run_b200(args) -> None:
     from tissueorigami_b200.newton import NewtonRaphsonSolver
 
     L = capi.load()
-    t = make_tissue(args.workload)
+    t = make_tissue(args.workload, args.slab_grid)
     precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0,
                "two_level": capi.TF_PRECOND_TWO_LEVEL, "multilevel": capi.TF_PRECOND_MULTILEVEL}[args.precond]
     s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent,
@@ -669,6 +670,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=4.0,
                     help="CPU assembly sample per step of the reference arm (seconds)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--slab-grid", default="1000x500",
+                    help="in-plane points of the large_slab workload (a smaller slab for ncu captures)")
     ap.add_argument("--smoother-nodes", type=int, choices=[0, 1, 2, 3, 4], default=0,
                     help="block-Jacobi block of a single tissue: 0 = a prism column when the mesh "
                          "numbers it consecutively, 1 = one node")
