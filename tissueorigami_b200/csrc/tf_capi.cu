@@ -33,6 +33,8 @@ constexpr int kMaxAggNodes = 2048;  // largest useful two-level aggregate (nodes
 constexpr int kBatchAggNodes = 256;  // aggregate size of a batch tissue's two-level space
 constexpr int kMlLeafCols = 16;      // prism columns per leaf of the multilevel space
 constexpr int kMlTopMax = 160;       // sets of the multilevel space's densely inverted top level
+constexpr int kMlAutoNodes = 100000; // single tissues from this size take the multilevel space
+constexpr int kMlTopMaxAge = 8;      // solves between refreshes of the multilevel top inverse
 
 struct DevBuf {
     void* p = nullptr;
@@ -126,6 +128,9 @@ struct tf_ctx {
     DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_order_d, bc_info_d;
     // multilevel coarse space of a single tissue (build_ml): leaves, levels, set-up lists
     bool ml_active = false;
+    bool ml_top_ok = false, ml_top_fresh = false;  // the top inverse exists / was refreshed for this solve
+    int ml_top_age = 0;                            // solves since the top inverse was refreshed
+    int32_t last_solve_method = 0;                 // KM_* of the last persistent solve (largest over tissues)
     int col_G = 1;  // nodes per prism column when the mesh numbers columns consecutively, else 1
     int ml_levels = 0, ml_n_leaf = 0, ml_n_slots = 0, ml_n_out = 0, ml_n_diag = 0, ml_n_top = 0, ml_nct = 0;
     int32_t ml_span[kMlMaxLevels] = {0}, ml_count[kMlMaxLevels] = {0}, ml_set0[kMlMaxLevels] = {0};
@@ -996,7 +1001,11 @@ int build_coarse(tf_ctx* ctx) {
     if (ctx->plan_ncta.empty()) return TF_OK;
     const int N = ctx->N, nct = ctx->plan_ncta[0];
     if (nct <= 0) return TF_OK;
-    if (ctx->params.precond == TF_PRECOND_MULTILEVEL) return build_ml(ctx);
+    // the multilevel space when asked for, and for large tissues: the one-level space's
+    // per-CTA aggregates grow with the tissue (measured: a 180,000-node slab 364 CG iterations per
+    // solve with them against ~127 with the multilevel space; the 60,441-node wing disc 243
+    // against 226, but its solves are short enough that the multilevel set-up made the step slower)
+    if (ctx->params.precond == TF_PRECOND_MULTILEVEL || N >= kMlAutoNodes) return build_ml(ctx);
     int m = std::max(1, std::min(kMaxAggPerCta, 2048 / (6 * nct)));
     while (m > 1 && N / (nct * m) < 8) --m;
     // each CTA's 6m rows of the n_coarse = 6 nct m inverse must fit its shared-memory block
@@ -1347,6 +1356,7 @@ int build_ml(tf_ctx* ctx) {
     ctx->ml_nct = nct;
     ctx->n_coarse = 6 * n_sets;
     ctx->ml_active = true;
+    ctx->ml_top_ok = false;
     ctx->coarse_age = 0;
     ctx->coarse_ok = false;
     return TF_OK;
@@ -1355,11 +1365,11 @@ int build_ml(tf_ctx* ctx) {
 // The multilevel operators from the current J: leaf-pair blocks, every set's diagonal block and
 // its pseudo-inverse, the top operator and its Gauss-Jordan inverse (symmetrised for conjugate
 // gradients). A singular top operator leaves the solve with block-Jacobi alone (coarse_ok false).
-int ml_setup(tf_ctx* ctx) {
+int ml_setup(tf_ctx* ctx, bool refresh_top) {
     ctx->coarse_ok = false;
     MlSetup m;
     m.n_slots = ctx->ml_n_slots;
-    m.n_out = ctx->ml_n_out;
+    m.n_out = refresh_top ? ctx->ml_n_out : ctx->ml_n_diag;  // the diagonal blocks come first
     m.n_diag = ctx->ml_n_diag;
     m.n_top = ctx->ml_n_top;
     m.slot_a = dptr<int32_t>(ctx->ml_slot_a_d);
@@ -1380,19 +1390,26 @@ int ml_setup(tf_ctx* ctx) {
     m.w_blocks = dptr<double>(ctx->ml_w_d);
     m.top = dptr<double>(ctx->ml_top_d);
     m.dflags = dptr<int32_t>(ctx->dflags);
-    TF_CK(launch_ml_setup(make_work(ctx), m, ctx->stream));
-    const int n6 = 6 * ctx->ml_n_top;
-    int32_t* info = dptr<int32_t>(ctx->ml_info_d);
-    TF_CK(launch_invert_coop(m.top, n6, ctx->ml_top_work.p, info, ctx->device, ctx->stream));
-    ctx->launches += 6;  // pairs, blocks, pinv6, top fix, Gauss-Jordan, unswap
-    TF_CK(cudaMemcpyAsync(ctx->h_coarse_info, info, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    TF_CK(cudaStreamSynchronize(ctx->stream));
-    if (*ctx->h_coarse_info < 0) return set_error(ctx, TF_ERR_STATE, "multilevel top inverse: grid barrier timed out");
-    if (*ctx->h_coarse_info != 0) return TF_OK;  // singular top operator: block-Jacobi only
-    if (use_cg(ctx)) {
-        TF_CK(launch_symmetrize(m.top, n6, n6, 0, 1, ctx->stream));
-        ctx->launches += 1;
+    TF_CK(launch_ml_setup(make_work(ctx), m, refresh_top, ctx->stream));
+    ctx->launches += 3;  // pairs, blocks, pinv6
+    if (refresh_top) {
+        ctx->ml_top_ok = false;
+        const int n6 = 6 * ctx->ml_n_top;
+        int32_t* info = dptr<int32_t>(ctx->ml_info_d);
+        TF_CK(launch_invert_coop(m.top, n6, ctx->ml_top_work.p, info, ctx->device, ctx->stream));
+        ctx->launches += 3;  // top fix, Gauss-Jordan, unswap
+        TF_CK(cudaMemcpyAsync(ctx->h_coarse_info, info, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        TF_CK(cudaStreamSynchronize(ctx->stream));
+        if (*ctx->h_coarse_info < 0) return set_error(ctx, TF_ERR_STATE, "multilevel top inverse: grid barrier timed out");
+        if (*ctx->h_coarse_info != 0) return TF_OK;  // singular top operator: block-Jacobi only
+        if (use_cg(ctx)) {
+            TF_CK(launch_symmetrize(m.top, n6, n6, 0, 1, ctx->stream));
+            ctx->launches += 1;
+        }
+        ctx->ml_top_ok = true;
+        ctx->ml_top_age = 0;
     }
+    if (!ctx->ml_top_ok) return TF_OK;
     ctx->coarse_ok = true;
     return TF_OK;
 }
@@ -1509,10 +1526,18 @@ int krylov_solve(tf_ctx* ctx) {
             // the multilevel operators are rebuilt from every J (a few set-up kernels, about one
             // SpMV of traffic): an operator kept from an indefinite first Newton iterate would
             // leave conjugate gradients an indefinite preconditioner for the positive definite rest
+            // (The dense top inverse, a Gauss-Jordan elimination with one grid barrier per step,
+            // is the expensive part: it is refreshed on the first solve, after kMlTopMaxAge solves,
+            // after a solve needed 1.3x the iterations of the first one since the refresh, and
+            // after conjugate gradients met an indefinite system, since a top inverse taken from
+            // an indefinite J would stay indefinite for the positive definite ones that follow.)
             if (ctx->ml_active) {
-                const int crc = ml_setup(ctx);
+                const bool top = !ctx->ml_top_ok || ctx->ml_top_age >= kMlTopMaxAge || ctx->last_solve_method == KM_CG_FALLBACK ||
+                                 (ctx->ml_top_age > 1 && ctx->last_solve_iters * 10 > ctx->coarse_base_iters * 13);
+                const int crc = ml_setup(ctx, top);
                 if (crc != TF_OK) return crc;
                 ++ctx->coarse_refreshes;
+                if (top) ctx->ml_top_fresh = true;
             }
         }
         const BatchPlan plan = make_plan(ctx);
@@ -1600,6 +1625,14 @@ int krylov_solve(tf_ctx* ctx) {
         if ((ctx->coarse_m > 0 || ctx->bc_active) && ctx->coarse_ok) {
             if (ctx->coarse_age == 0) ctx->coarse_base_iters = ctx->last_solve_iters;
             ++ctx->coarse_age;
+        }
+        ctx->last_solve_method = 0;
+        for (int t = 0; t < ctx->T; ++t)
+            if (ctx->T == 1 || ctx->h_active[t]) ctx->last_solve_method = std::max(ctx->last_solve_method, ctx->h_tsc[t].method);
+        if (ctx->ml_active && ctx->coarse_ok) {
+            if (ctx->ml_top_fresh) ctx->coarse_base_iters = ctx->last_solve_iters;
+            ctx->ml_top_fresh = false;
+            ++ctx->ml_top_age;
         }
         return TF_OK;
     }

@@ -378,7 +378,9 @@ struct MlSetup {
     double* top;              // [6 n_top]^2
     int32_t* dflags;
 };
-cudaError_t launch_ml_setup(const KrylovWork& w, const MlSetup& m, cudaStream_t s);
+// top = false: the diagonal blocks and their pseudo-inverses only (m.n_out = m.n_diag), the top
+// operator left as it is
+cudaError_t launch_ml_setup(const KrylovWork& w, const MlSetup& m, bool top, cudaStream_t s);
 
 // --- dense inverses of the coarse operators (tf_dense.cu) -------------------------------------
 // In-place Gauss-Jordan inverse with partial pivoting of column-major matrices (a row-major

@@ -221,15 +221,17 @@ __global__ void k_ml_top_fix(double* top, int n) {
 
 }  // namespace
 
-cudaError_t launch_ml_setup(const KrylovWork& w, const MlSetup& m, cudaStream_t s) {
+cudaError_t launch_ml_setup(const KrylovWork& w, const MlSetup& m, bool top, cudaStream_t s) {
     const int n6 = 6 * m.n_top;
-    cudaError_t e = cudaMemsetAsync(m.top, 0, sizeof(double) * (size_t)n6 * n6, s);
-    if (e != cudaSuccess) return e;
+    if (top) {
+        cudaError_t e = cudaMemsetAsync(m.top, 0, sizeof(double) * (size_t)n6 * n6, s);
+        if (e != cudaSuccess) return e;
+    }
     const int wpb = kMlThreads / 32;
     if (m.n_slots > 0) k_ml_pairs<<<(m.n_slots + wpb - 1) / wpb, kMlThreads, 0, s>>>(w, m);
     if (m.n_out > 0) k_ml_blocks<<<(m.n_out + wpb - 1) / wpb, kMlThreads, 0, s>>>(m);
     if (m.n_diag > 0) k_ml_pinv6<<<(m.n_diag + 127) / 128, 128, 0, s>>>(m.w_blocks, m.n_diag, m.dflags);
-    if (n6 > 0) k_ml_top_fix<<<(n6 + 255) / 256, 256, 0, s>>>(m.top, n6);
+    if (top && n6 > 0) k_ml_top_fix<<<(n6 + 255) / 256, 256, 0, s>>>(m.top, n6);
     return cudaGetLastError();
 }
 
