@@ -224,7 +224,7 @@ def run_b200(args) -> None:
     precond = {"block_jacobi": capi.TF_PRECOND_BLOCK_JACOBI, "ilu0": capi.TF_PRECOND_ILU0,
                "two_level": capi.TF_PRECOND_TWO_LEVEL, "multilevel": capi.TF_PRECOND_MULTILEVEL}[args.precond]
     s = NewtonRaphsonSolver.from_tissue(t, device=local, precond=precond, persistent=args.persistent,
-                                        smoother_nodes=args.smoother_nodes)
+                                        smoother_nodes=args.smoother_nodes, packing=bool(args.packing))
     sched = s.autotune(t.x, t.dt)
     sched["precond"] = args.precond
     sched["solve"] = {0: "graph-replayed iteration kernels", 1: "persistent cooperative kernel"}[args.persistent]
@@ -319,6 +319,10 @@ def run_b200(args) -> None:
     sched["krylov_method"] = {1: "bicgstab", 2: "conjugate gradients",
                               3: "conjugate gradients, finished by bicgstab on indefinite solves"}.get(max(methods), "none")
     sched["krylov_iters_cg_share"] = kry_cg / max(kry, 1)
+    # the reference detects node-node packing after every step's growth; the pairs it finds add
+    # forces and Jacobian blocks to the Newton iterations
+    sched["packing"] = ({"detection": "every step (device)", "pairs_last_step": int(len(s.packing()[0]))}
+                        if args.packing else "off")
     sched["coarse_unknowns"] = n_coarse
     sched["coarse_refreshes"] = refreshes
     sched["smoother_block_nodes"] = s.smoother_block()
@@ -670,6 +674,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=4.0,
                     help="CPU assembly sample per step of the reference arm (seconds)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--packing", type=int, choices=[0, 1], default=1,
+                    help="node-node packing detection every step and its terms (the reference's default)")
     ap.add_argument("--slab-grid", default="1000x500",
                     help="in-plane points of the large_slab workload (a smaller slab for ncu captures)")
     ap.add_argument("--smoother-nodes", type=int, choices=[0, 1, 2, 3, 4], default=0,

@@ -355,6 +355,29 @@ int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drate
  * every SM. The element kernel's own ceiling: its closed-form tangent is compute-bound. */
 int tf_measure_fp64(int32_t device, double* tflops);
 
+/* Packing (node-node contact): Simulation::detectPacingNodes (Simulation.cpp:7997-8153) after
+ * every time step's growth, with the node masses of Simulation::updateNodeMasses (:7587-7596),
+ * and in every Newton iteration the forces and Jacobian blocks of
+ * Simulation::calculatePackingForcesImplicit3D / calculatePackingJacobian3D (:7307-7575):
+ * pairs of apical (or basal) nodes that share no element and lie closer than 0.4 x the local
+ * average element side, force 5000 m S(d) along the pair (m the pair's average mass, S a sigmoid
+ * centred at 0.6 x packingThreshold). enabled != 0 turns it on with node_placement[N] (0 basal,
+ * 1 apical, 2 other: never packs); tf_time_step / tf_time_step_device then detect the pairs of
+ * each step on the device. Single tissue without slave-master pairs (TF_ERR_UNSUPPORTED
+ * otherwise); while a step has pairs, tf_solve_direct returns TF_ERR_UNSUPPORTED; the adjoint
+ * does not support packing. The two-level and multilevel coarse operators leave the pairs' blocks
+ * outside the element pattern out (a preconditioner only); the solves include them. */
+int tf_set_packing(tf_ctx* ctx, int32_t enabled, const int32_t* node_placement);
+/* Detect the pairs at host positions x [N*3] with the current growth tensors (masses from them),
+ * as the step prologue does; for hosts that run their own step loop (and for tests). */
+int tf_detect_packing(tf_ctx* ctx, const double* x, int32_t* n_pairs);
+/* The pairs of the last detection: their number, up to max_pairs pairs (i < j, the reference's
+ * visiting order) in pairs[2*max_pairs], Simulation::packingThreshold, the node masses [N] and the
+ * derivative blocks dF_i/dx_i [P][9] (row-major; the reference adds -D at (i, i), (j, j) and +D at
+ * (i, j), (j, i)) of the last assembly. Any output may be NULL. */
+int tf_get_packing(tf_ctx* ctx, int32_t max_pairs, int32_t* n_pairs, int32_t* pairs, double* threshold, double* mass,
+                   double* dfdx);
+
 /* Dense inverse utility (no reference counterpart): inverts `count` column-major n x n matrices
  * `a` of host memory in place on `device` with the Gauss-Jordan kernels that invert the two-level
  * preconditioner's coarse operators (partial pivoting; one CTA per matrix, or each matrix over a

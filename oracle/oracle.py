@@ -56,6 +56,10 @@ def lib():
         L.tfo_viscosity_surfaces.argtypes = [c_int, c_int, _I, _D, _U, _U, _D]
         L.tfo_detect_packing.argtypes = [c_int, c_int, _I, _D, _I, _U, _U, c_int, _I, _D]
         L.tfo_detect_packing.restype = c_int
+        L.tfo_node_masses.argtypes = [c_int, c_int, _I, _D, _D, _D]
+        L.tfo_node_masses.restype = None
+        L.tfo_packing_terms.argtypes = [c_int, _I, _D, _D, c_double, _D, _D]
+        L.tfo_packing_terms.restype = None
         _lib = L
     return _lib
 
@@ -230,6 +234,52 @@ def detect_packing(t, x):
     return pairs[:n], thr.value
 
 
+def node_masses(t, fg):
+    """Node masses after the step's growth (Simulation::updateNodeMasses): det(Fg) x reference
+    volume / 6 from every element of the node."""
+    mass = np.zeros(t.n_nodes)
+    lib().tfo_node_masses(t.n_nodes, t.n_elems, _i(_c(t.conn, np.int32)), _d(_c(t.xref, np.float64)),
+                          _d(_c(fg, np.float64)), _d(mass))
+    return mass
+
+
+def packing_terms(t, x, pairs, mass, threshold):
+    """Packing forces [N,3] and the pairs' 3x3 derivative blocks dF_i/dx_i [P,3,3] at positions x
+    (Simulation::calculatePackingForcesImplicit3D / calculatePackingJacobian3D)."""
+    pairs = _c(np.asarray(pairs).reshape(-1, 2), np.int32)
+    forces = np.zeros((t.n_nodes, 3))
+    dfdx = np.zeros((max(pairs.shape[0], 1), 3, 3))
+    if pairs.shape[0]:
+        lib().tfo_packing_terms(pairs.shape[0], _i(pairs), _d(_c(x, np.float64)), _d(_c(mass, np.float64)),
+                                float(threshold), _d(forces), _d(dfdx))
+    return forces, dfdx[:pairs.shape[0]]
+
+
+def add_packing(t, J, g, x, pairs, mass, threshold):
+    """J + the packing Jacobian blocks (-D at (i, i) and (j, j), +D at (i, j) and (j, i)) and g +
+    the packing forces, both with the fixed DoFs' rows and columns left out (calcutateFixedK runs
+    after the packing terms, NewtonRaphsonSolver.cpp:195-219); D is symmetric, so J = K^T holds."""
+    import scipy.sparse as sp
+
+    forces, D = packing_terms(t, x, pairs, mass, threshold)
+    free = (np.asarray(t.fixed).reshape(-1) == 0)
+    g = g + np.where(free, forces.reshape(-1), 0.0)
+    if len(pairs) == 0:
+        return J, g
+    rows, cols, vals = [], [], []
+    for p, (i, j) in enumerate(np.asarray(pairs)):
+        for (a, b, sgn) in ((i, i, -1.0), (i, j, 1.0), (j, j, -1.0), (j, i, 1.0)):
+            for r in range(3):
+                for c in range(3):
+                    R, C = 3 * a + r, 3 * b + c
+                    if free[R] and free[C]:
+                        rows.append(R)
+                        cols.append(C)
+                        vals.append(sgn * D[p, r, c])
+    n = 3 * t.n_nodes
+    return (J + sp.csr_matrix((vals, (rows, cols)), shape=(n, n))).tocsr(), g
+
+
 def bsr_to_scipy(rowptr, colidx, vals, n_nodes):
     import scipy.sparse as sp
 
@@ -302,10 +352,13 @@ def sparse_direct_solve(J, g, perm=None):
     return du
 
 
-def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0, perm=None):
+def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0, perm=None,
+                       packing=None):
     """Simulation::updateStepNR with sparse assembly of J = K^T and SuperLU (scipy) as the
     direct solve standing in for Pardiso. No slave-master pairs. Returns (x, iterations, norms).
-    perm: optional fill-reducing DoF order for the factorisation (nested_dissection)."""
+    perm: optional fill-reducing DoF order for the factorisation (nested_dissection).
+    packing: optional (pairs, masses, threshold) of the step; its forces and Jacobian are added
+    at every iteration's positions."""
     rowptr, colidx = block_pattern(t)
     un = np.array(x_n, dtype=np.float64, copy=True).reshape(-1, 3)
     uk = un.copy()
@@ -316,6 +369,8 @@ def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter
     while not converged:
         vals, g = assemble_bsr(t, uk, un, visc_surface, inv_fg, rowptr, colidx, dt=dt, threads=threads)
         J = bsr_to_scipy(rowptr, colidx, vals, t.n_nodes)
+        if packing is not None:
+            J, g = add_packing(t, J, g, uk, *packing)
         du = sparse_direct_solve(J, g, perm)
         d = float(np.sqrt(np.sum(du * du)))
         norms.append(d)
@@ -327,10 +382,14 @@ def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter
     return uk, it, np.array(norms)
 
 
-def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0, reorder=False, positions=None):
+def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0, reorder=False, positions=None,
+                    packing=False, pair_counts=None):
     """n time steps with the growth prologue and the sparse Newton step. reorder: factorise in
     nested-dissection order (large meshes). positions: optional list that receives the positions
-    at the start of every step and after the last."""
+    at the start of every step and after the last. packing: node masses and packing pairs
+    detected after each step's growth (Simulation::runOneStep, Simulation.cpp:6065-6076), their
+    forces and Jacobian in every Newton iteration; pair_counts: optional list of each step's
+    number of pairs."""
     x = np.array(t.x, dtype=np.float64, copy=True)
     fg = np.array(t.fg, dtype=np.float64, copy=True)
     iters, traces = [], []
@@ -340,7 +399,14 @@ def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0, reorder=F
             positions.append(x.copy())
         fg, inv, _, _ = grow(t, x, fg)
         vs = viscosity_surfaces(t, x)
-        x, it, norms = newton_step_sparse(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads, perm=perm)
+        pk = None
+        if packing:
+            pairs, thr = detect_packing(t, x)
+            pk = (pairs, node_masses(t, fg), thr)
+            if pair_counts is not None:
+                pair_counts.append(len(pairs))
+        x, it, norms = newton_step_sparse(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads, perm=perm,
+                                          packing=pk)
         iters.append(it)
         traces.append(norms)
     if positions is not None:

@@ -1224,4 +1224,90 @@ int tfo_detect_packing(int n_nodes, int n_elems, const int32_t* conn, const doub
     return np;
 }
 
+
+// Simulation::updateNodeMasses (Simulation.cpp:7587-7596) with ShapeBase::assignVolumesToNodes
+// (ShapeBase.cpp:3749-3753): every node collects GrownVolume / 6 of each of its elements,
+// GrownVolume = det(Fg) x the reference volume (ShapeBase.cpp:1498). The reference volume is
+// Prism::calculateReferenceVolume (Prism.cpp:890-923) through
+// ShapeBase::calculateVolumeForInputShapeStructure (ShapeBase.cpp:3364-3400): the prism's eight
+// triangular faces, each the base of a tetrahedron with the element's centre as apex, |height| x
+// area / 3 summed.
+void tfo_node_masses(int n_nodes, int n_elems, const int32_t* conn, const double* xref, const double* fg,
+                     double* mass) {
+    static const int faces[8][3] = {{0, 1, 2}, {3, 4, 5}, {0, 1, 3}, {1, 3, 4}, {1, 2, 4}, {2, 4, 5}, {0, 2, 3}, {2, 3, 5}};
+    for (int n = 0; n < n_nodes; ++n) mass[n] = 0.0;
+    for (int e = 0; e < n_elems; ++e) {
+        const double* X = xref + (size_t)e * 18;
+        double c[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < 6; ++a)
+            for (int d = 0; d < 3; ++d) c[d] += X[a * 3 + d];
+        for (int d = 0; d < 3; ++d) c[d] /= 6.0;
+        double vol = 0.0;
+        for (int f = 0; f < 8; ++f) {
+            const double* p0 = X + faces[f][0] * 3;
+            const double* p1 = X + faces[f][1] * 3;
+            const double* p2 = X + faces[f][2] * 3;
+            double v1[3], v2[3], vm[3];
+            for (int d = 0; d < 3; ++d) {
+                v1[d] = p1[d] - p0[d];
+                v2[d] = p2[d] - p0[d];
+                vm[d] = c[d] - p0[d];
+            }
+            const double b[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+            const double nb = std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+            const double area = nb / 2.0;
+            double h = (vm[0] * b[0] + vm[1] * b[1] + vm[2] * b[2]) / nb;
+            if (h < 0) h = -h;
+            vol += 1.0 / 3.0 * (h * area);
+        }
+        const double* F = fg + (size_t)e * 9;
+        const double det = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+                           F[2] * (F[3] * F[7] - F[4] * F[6]);
+        const double per_node = det * vol / 6.0;
+        for (int a = 0; a < 6; ++a) mass[conn[(size_t)e * 6 + a]] += per_node;
+    }
+}
+
+// Simulation::calculatePackingForcesImplicit3D (Simulation.cpp:7307-7424) and
+// calculatePackingJacobian3D (:7426-7575) for the pairs of one step at positions x: with
+// e = (x_i - x_j) / d (d = |x_i - x_j|; e = (1, 0, 0) and d = 1e-3 when d <= 1e-3),
+// S = 1 / (1 + exp(5 / thr * 2 * (d - 0.6 thr))) and m the pair's average mass, F_i = 5000 m S e
+// is added to forces[i] and subtracted from forces[j]; dfdx[p] = 5000 m [S / d (I - e e^T) +
+// dS/dd e e^T], dS/dd = -2 * 5 / thr * S (1 - S), is the 3 x 3 block the reference adds to K as
+// -dfdx at (i, i) and (j, j) and +dfdx at (i, j) and (j, i). Row-major blocks; forces may be NULL.
+void tfo_packing_terms(int n_pairs, const int32_t* pairs, const double* x, const double* mass, double thr,
+                       double* forces, double* dfdx) {
+    const double zero_threshold = 1e-3, multiplier = 5000.0, saturation = 5.0;
+    for (int p = 0; p < n_pairs; ++p) {
+        const int i = pairs[2 * p], j = pairs[2 * p + 1];
+        const double dx = x[(size_t)i * 3] - x[(size_t)j * 3], dy = x[(size_t)i * 3 + 1] - x[(size_t)j * 3 + 1],
+                     dz = x[(size_t)i * 3 + 2] - x[(size_t)j * 3 + 2];
+        double d = std::pow(dx * dx + dy * dy + dz * dz, 0.5);
+        const double m = 0.5 * (mass[i] + mass[j]);
+        double e[3] = {1.0, 0.0, 0.0};
+        if (d > zero_threshold) {
+            e[0] = dx / d;
+            e[1] = dy / d;
+            e[2] = dz / d;
+        } else {
+            d = zero_threshold;
+        }
+        const double shifted = d - 0.6 * thr;
+        const double S = 1 / (1 + std::exp(saturation / thr * 2.0 * shifted));
+        const double fmag = multiplier * m * S;
+        if (forces)
+            for (int k = 0; k < 3; ++k) {
+                forces[(size_t)i * 3 + k] += fmag * e[k];
+                forces[(size_t)j * 3 + k] -= fmag * e[k];
+            }
+        const double dS = (-saturation / thr * 2.0) * S * (1 - S);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                const double ee = e[r] * e[c];
+                const double v = ((r == c ? 1.0 : 0.0) - ee) * (S / d) + ee * dS;
+                dfdx[(size_t)p * 9 + r * 3 + c] = v * (multiplier * m);
+            }
+    }
+}
+
 }  // extern "C"

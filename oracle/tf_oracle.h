@@ -150,6 +150,17 @@ int tfo_detect_packing(int n_nodes, int n_elems, const int32_t* conn, const doub
                        const int32_t* node_placement, const uint8_t* exposed, const uint8_t* peripodial,
                        int max_pairs, int32_t* pairs, double* packing_threshold);
 
+/* Node masses of one step (Simulation::updateNodeMasses, Simulation.cpp:7587-7596): every node
+ * collects det(Fg) x the element's reference volume / 6 from each of its elements. */
+void tfo_node_masses(int n_nodes, int n_elems, const int32_t* conn, const double* xref, const double* fg,
+                     double* mass);
+
+/* Packing forces (added to forces[3N], may be NULL) and the 3 x 3 derivative blocks dfdx[P][9] of
+ * the pairs of one step at positions x (Simulation::calculatePackingForcesImplicit3D and
+ * calculatePackingJacobian3D, Simulation.cpp:7307-7575); thr = Simulation::packingThreshold. */
+void tfo_packing_terms(int n_pairs, const int32_t* pairs, const double* x, const double* mass, double thr,
+                       double* forces, double* dfdx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,7 @@ over its full number of steps.
 import math
 
 import numpy as np
+import pytest
 
 from oracle import oracle as O
 from tissueorigami_b200 import mesh
@@ -136,3 +137,40 @@ def test_detector_matches_literal_loops_on_perturbed_meshes():
     x = t.x + rng.normal(0.0, 0.6, t.x.shape)
     pairs = O.detect_packing(t, x)[0]
     np.testing.assert_array_equal(pairs, _literal_detect(t, x))
+
+
+def test_packing_jacobian_matches_finite_differences_of_the_forces():
+    """The oracle's calculatePackingJacobian3D restatement is the derivative of its
+    calculatePackingForcesImplicit3D restatement (central differences, h = 1e-6, 1e-7 relative)."""
+    t = mesh.stacked_sheets()
+    fg, _, _, _ = O.grow(t, t.x, t.fg)
+    pairs, thr = O.detect_packing(t, t.x)
+    assert len(pairs) == 45
+    mass = O.node_masses(t, fg)
+    rng = np.random.default_rng(3)
+    x = t.x + rng.normal(0.0, 0.05, t.x.shape)
+    _, D = O.packing_terms(t, x, pairs, mass, thr)
+    h = 1e-6
+    for p in (0, 17, 44):
+        i, j = pairs[p]
+        num = np.zeros((3, 3))
+        for c in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[i, c] += h
+            xm[i, c] -= h
+            fp, _ = O.packing_terms(t, xp, pairs[p:p + 1], mass, thr)
+            fm, _ = O.packing_terms(t, xm, pairs[p:p + 1], mass, thr)
+            num[:, c] = (fp[i] - fm[i]) / (2 * h)
+        assert np.abs(num - D[p]).max() <= 1e-7 * np.abs(D[p]).max()
+        assert np.allclose(D[p], D[p].T, rtol=0, atol=1e-12 * np.abs(D[p]).max())
+
+
+def test_node_masses_sum_to_the_grown_volume():
+    """Each prism hands det(Fg) x its volume to its six nodes: the masses sum to the grown volume
+    of both sheets (2 x 18 x 10 x 4 um^3 times det(Fg))."""
+    t = mesh.stacked_sheets()
+    fg, _, _, _ = O.grow(t, t.x, t.fg)
+    mass = O.node_masses(t, fg)
+    det = np.linalg.det(fg.reshape(-1, 3, 3))
+    assert np.allclose(det, det[0])
+    assert mass.sum() == pytest.approx(2 * 18.0 * 10.0 * 4.0 * det[0], rel=1e-13)

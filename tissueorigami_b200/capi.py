@@ -52,7 +52,8 @@ EXPORTS = [
     "tf_get_growth", "tf_time_step", "tf_time_step_device", "tf_get_schedule", "tf_autotune",
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
-    "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64", "tf_invert_dense",
+    "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64", "tf_invert_dense", "tf_set_packing", "tf_detect_packing",
+    "tf_get_packing",
     "tf_set_grid_growth", "tf_set_time", "tf_get_time", "tf_set_external_force", "tf_newton_iteration",
     "tf_get_krylov_method",
 ]
@@ -157,6 +158,9 @@ def load(build_if_missing: bool = True):
     L.tf_solve_bsr_noalloc.argtypes = [c_int, _P, _P, _P, _P, _P, c_double, c_int, _P, _I, _D]
     L.tf_measure_fp64.argtypes = [c_int, _D]
     L.tf_invert_dense.argtypes = [c_int, c_int, c_int, c_int, _D, _I]
+    L.tf_set_packing.argtypes = [_P, c_int, _I]
+    L.tf_detect_packing.argtypes = [_P, _D, _I]
+    L.tf_get_packing.argtypes = [_P, c_int, _I, _I, _D, _D, _D]
     L.tf_set_grid_growth.argtypes = [_P, c_int, ctypes.POINTER(GridGrowth), c_int, _D, _D, _I]
     L.tf_set_time.argtypes = [_P, c_double]
     L.tf_set_external_force.argtypes = [_P, _D]

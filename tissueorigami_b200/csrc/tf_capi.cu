@@ -126,6 +126,12 @@ struct tf_ctx {
     int64_t bc_n_unit = 0;
     std::vector<int32_t> bc_tissue_agg0;
     DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_order_d, bc_info_d;
+    // packing (tf_set_packing): detection per step, pairs and their blocks outside the pattern
+    bool pk_on = false;
+    int pk_hash_bits = 10, pk_capacity = 0, pk_pairs_n = 0;
+    std::vector<int32_t> h_pk_pairs;
+    DevBuf pk_place_d, pk_v0_d, pk_mass_d, pk_prm_d, pk_bucket_cnt_d, pk_bucket_start_d, pk_bucket_nodes_d,
+        pk_node_cnt_d, pk_node_start_d, pk_scan_d, pk_pairs_d, pk_ptr_d, pk_col_d, pk_blk_d, pk_vals_d, pk_dfdx_d, pk_x_d;
     // multilevel coarse space of a single tissue (build_ml): leaves, levels, set-up lists
     bool ml_active = false;
     bool ml_top_ok = false, ml_top_fresh = false;  // the top inverse exists / was refreshed for this solve
@@ -551,6 +557,11 @@ KrylovWork make_work(tf_ctx* c) {
     w.n_partials = (int32_t)(c->partials.bytes / sizeof(double));
     w.sc = dptr<KrylovScalars>(c->sc);
     w.dflags = dptr<int32_t>(c->dflags);
+    const bool pk = c->pk_on && c->pk_pairs_n > 0;
+    w.pk_ptr = pk ? dptr<int32_t>(c->pk_ptr_d) : nullptr;
+    w.pk_col = pk ? dptr<int32_t>(c->pk_col_d) : nullptr;
+    w.pk_blk = pk ? dptr<int32_t>(c->pk_blk_d) : nullptr;
+    w.pk_vals = pk ? dptr<double>(c->pk_vals_d) : nullptr;
     return w;
 }
 
@@ -836,6 +847,116 @@ int assemble_system(tf_ctx* ctx, double dt) {
     na.tissue_active = dptr<int32_t>(ctx->active_d);
     TF_CK(launch_node_terms(na, ctx->stream));
     ctx->launches += 1;
+    if (ctx->pk_on && ctx->pk_pairs_n > 0) {
+        PackTerms pt;
+        pt.n_pairs = ctx->pk_pairs_n;
+        pt.pairs = dptr<int32_t>(ctx->pk_pairs_d);
+        pt.x = dptr<double>(ctx->uk);
+        pt.mass = dptr<double>(ctx->pk_mass_d);
+        pt.prm = dptr<PackParams>(ctx->pk_prm_d);
+        pt.fixmask = dptr<uint8_t>(ctx->fixmask);
+        pt.diag = dptr<int32_t>(ctx->diag_d);
+        pt.vals = dptr<double>(ctx->vals);
+        pt.g = dptr<double>(ctx->g);
+        pt.pk_vals = dptr<double>(ctx->pk_vals_d);
+        pt.dfdx = dptr<double>(ctx->pk_dfdx_d);
+        TF_CK(launch_packing_terms(pt, ctx->stream));
+        ctx->launches += 1;
+    }
+    return TF_OK;
+}
+
+// The step's packing pairs at positions x (device [N][3]) with the current Fg: node masses,
+// thresholds and pairs on the device; the pair list comes back to the host, which lays out the
+// rows of the extra blocks (i, j) and (j, i) for the SpMVs.
+int packing_detect(tf_ctx* ctx, const double* x) {
+    const int N = ctx->N;
+    const int before = ctx->pk_pairs_n;
+    // the captured Krylov graphs hold the packing rows' pointers (make_work): drop them whenever
+    // the step has pairs or had some, so the next chunked solve captures the current ones
+    struct DropGraphs {
+        tf_ctx* c;
+        int before;
+        ~DropGraphs() {
+            if (before == 0 && c->pk_pairs_n == 0) return;
+            if (c->krylov_graph) {
+                cudaGraphExecDestroy(c->krylov_graph);
+                c->krylov_graph = nullptr;
+            }
+            if (c->ilu_graph) {
+                cudaGraphExecDestroy(c->ilu_graph);
+                c->ilu_graph = nullptr;
+            }
+        }
+    } drop{ctx, before};
+    PackArgs a;
+    a.n_nodes = N;
+    a.n_elems = ctx->E;
+    a.elems = dptr<ElemRecord>(ctx->elems);
+    a.x = x;
+    a.fg = dptr<double>(ctx->fg);
+    a.v0 = dptr<double>(ctx->pk_v0_d);
+    a.exposed = dptr<uint8_t>(ctx->exposed);
+    a.peripodial = dptr<uint8_t>(ctx->peripodial);
+    a.placement = dptr<int8_t>(ctx->pk_place_d);
+    a.rowptr = dptr<int32_t>(ctx->rowptr_d);
+    a.colidx = dptr<int32_t>(ctx->colidx_d);
+    a.mass = dptr<double>(ctx->pk_mass_d);
+    a.prm = dptr<PackParams>(ctx->pk_prm_d);
+    a.hash_bits = ctx->pk_hash_bits;
+    a.bucket_cnt = dptr<int32_t>(ctx->pk_bucket_cnt_d);
+    a.bucket_start = dptr<int32_t>(ctx->pk_bucket_start_d);
+    a.bucket_nodes = dptr<int32_t>(ctx->pk_bucket_nodes_d);
+    a.node_cnt = dptr<int32_t>(ctx->pk_node_cnt_d);
+    a.node_start = dptr<int32_t>(ctx->pk_node_start_d);
+    a.scan_tmp = dptr<int32_t>(ctx->pk_scan_d);
+    a.pairs = dptr<int32_t>(ctx->pk_pairs_d);
+    a.capacity = ctx->pk_capacity;
+    TF_CK(launch_packing_detect(a, ctx->stream));
+    ctx->launches += 14;
+    int32_t total = 0;
+    TF_CK(cudaMemcpyAsync(&total, a.node_start + N, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    ctx->pk_pairs_n = 0;
+    ctx->h_pk_pairs.clear();
+    if (total <= 0) return TF_OK;
+    if (total > ctx->pk_capacity) {
+        ctx->pk_capacity = total + total / 2;
+        TF_CK(dalloc(ctx->pk_pairs_d, sizeof(int32_t) * 2 * (size_t)ctx->pk_capacity));
+        TF_CK(dalloc(ctx->pk_vals_d, sizeof(double) * 18 * (size_t)ctx->pk_capacity));
+        TF_CK(dalloc(ctx->pk_dfdx_d, sizeof(double) * 9 * (size_t)ctx->pk_capacity));
+        TF_CK(dalloc(ctx->pk_col_d, sizeof(int32_t) * 2 * (size_t)ctx->pk_capacity));
+        TF_CK(dalloc(ctx->pk_blk_d, sizeof(int32_t) * 2 * (size_t)ctx->pk_capacity));
+        a.pairs = dptr<int32_t>(ctx->pk_pairs_d);
+        a.capacity = ctx->pk_capacity;
+    }
+    TF_CK(launch_packing_pairs(a, ctx->stream));
+    ctx->launches += 1;
+    ctx->h_pk_pairs.resize((size_t)2 * total);
+    TF_CK(cudaMemcpyAsync(ctx->h_pk_pairs.data(), a.pairs, sizeof(int32_t) * 2 * (size_t)total, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    // extra blocks by row: row i holds (i, j) = block 2p, row j holds (j, i) = block 2p + 1
+    std::vector<int32_t> ptr((size_t)N + 1, 0), col((size_t)2 * total), blk((size_t)2 * total);
+    for (int p = 0; p < total; ++p) {
+        ptr[ctx->h_pk_pairs[2 * p] + 1]++;
+        ptr[ctx->h_pk_pairs[2 * p + 1] + 1]++;
+    }
+    for (int n = 0; n < N; ++n) ptr[n + 1] += ptr[n];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int p = 0; p < total; ++p) {
+        const int i = ctx->h_pk_pairs[2 * p], j = ctx->h_pk_pairs[2 * p + 1];
+        col[fill[i]] = j;
+        blk[fill[i]++] = 2 * p;
+        col[fill[j]] = i;
+        blk[fill[j]++] = 2 * p + 1;
+    }
+    TF_CK(dalloc(ctx->pk_ptr_d, sizeof(int32_t) * ptr.size()));
+    TF_CK(cudaMemcpyAsync(ctx->pk_ptr_d.p, ptr.data(), sizeof(int32_t) * ptr.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->pk_col_d.p, col.data(), sizeof(int32_t) * col.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->pk_blk_d.p, blk.data(), sizeof(int32_t) * blk.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));  // the host vectors go out of scope
+    ctx->pk_pairs_n = total;
     return TF_OK;
 }
 
@@ -1883,6 +2004,7 @@ int prologue(tf_ctx* ctx, double dt) {
                                    dptr<uint8_t>(ctx->exposed), dptr<uint8_t>(ctx->peripodial),
                                    dptr<double>(ctx->visc_surface), ctx->stream));
     ctx->launches += 2;
+    if (ctx->pk_on) return packing_detect(ctx, dptr<double>(ctx->un));  // after the growth (Simulation.cpp:6065-6076)
     return TF_OK;
 }
 
@@ -2197,6 +2319,11 @@ void tf_destroy(tf_ctx* ctx) {
     DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_ptr_d, &ctx->bc_agg_nodes_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
                      &ctx->bc_order_d, &ctx->bc_info_d};
     for (DevBuf* b : bcb) dfree(*b);
+    DevBuf* pkb[] = {&ctx->pk_place_d, &ctx->pk_v0_d, &ctx->pk_mass_d, &ctx->pk_prm_d, &ctx->pk_bucket_cnt_d,
+                     &ctx->pk_bucket_start_d, &ctx->pk_bucket_nodes_d, &ctx->pk_node_cnt_d, &ctx->pk_node_start_d,
+                     &ctx->pk_scan_d, &ctx->pk_pairs_d, &ctx->pk_ptr_d, &ctx->pk_col_d, &ctx->pk_blk_d, &ctx->pk_vals_d,
+                     &ctx->pk_dfdx_d, &ctx->pk_x_d};
+    for (DevBuf* b : pkb) dfree(*b);
     DevBuf* mlb[] = {&ctx->ml_leaf_ptr_d, &ctx->ml_leaf_nodes_d, &ctx->ml_cen_d, &ctx->ml_w_d, &ctx->ml_top_d,
                      &ctx->ml_top_work, &ctx->ml_info_d, &ctx->ml_leaf_m_d, &ctx->ml_part_d, &ctx->ml_pstart_d,
                      &ctx->ml_first_cta_d, &ctx->ml_slot_a_d, &ctx->ml_out_ptr_d, &ctx->ml_out_slots_d,
@@ -2267,6 +2394,7 @@ int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
     }
     for (int32_t m : ms)
         if (dm[m] != m) return set_error(ctx, TF_ERR_ARGUMENT, "a master DoF is itself a slave");
+    if (n_pairs > 0 && ctx->pk_on) return set_error(ctx, TF_ERR_UNSUPPORTED, "slave-master pairs with packing");
     const bool changed = dm != ctx->dofmap;
     ctx->dofmap = dm;
     ctx->slave = sl;
@@ -2286,6 +2414,113 @@ int tf_set_external_force(tf_ctx* ctx, const double* f) {
     TF_CK(dalloc(ctx->ext_force, sizeof(double) * 3 * (size_t)ctx->N));
     TF_CK(cudaMemcpy(ctx->ext_force.p, f, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyHostToDevice));
     ctx->has_ext_force = true;
+    return TF_OK;
+}
+
+int tf_set_packing(tf_ctx* ctx, int32_t enabled, const int32_t* node_placement) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!enabled) {
+        if (ctx->pk_pairs_n > 0) {  // graphs captured with packing rows
+            if (ctx->krylov_graph) cudaGraphExecDestroy(ctx->krylov_graph);
+            if (ctx->ilu_graph) cudaGraphExecDestroy(ctx->ilu_graph);
+            ctx->krylov_graph = nullptr;
+            ctx->ilu_graph = nullptr;
+        }
+        ctx->pk_on = false;
+        ctx->pk_pairs_n = 0;
+        return TF_OK;
+    }
+    if (!node_placement) return TF_ERR_ARGUMENT;
+    if (ctx->T != 1 || !ctx->slave.empty())
+        return set_error(ctx, TF_ERR_UNSUPPORTED, "packing: single tissue without slave-master pairs");
+    const int N = ctx->N, E = ctx->E;
+    std::vector<int8_t> pl(N);
+    int eligible = 0;
+    for (int n = 0; n < N; ++n) {
+        pl[n] = (int8_t)((node_placement[n] == 0 || node_placement[n] == 1) ? node_placement[n] : 2);
+        eligible += pl[n] != 2;
+    }
+    // reference volumes (Prism::calculateReferenceVolume, Prism.cpp:890-923, with
+    // ShapeBase::calculateVolumeForInputShapeStructure, ShapeBase.cpp:3364-3400): eight triangular
+    // faces, each the base of a tetrahedron with the element centre, |height| x area / 3 summed
+    static const int faces[8][3] = {{0, 1, 2}, {3, 4, 5}, {0, 1, 3}, {1, 3, 4}, {1, 2, 4}, {2, 4, 5}, {0, 2, 3}, {2, 3, 5}};
+    std::vector<double> v0(E);
+    for (int e = 0; e < E; ++e) {
+        const double* X = ctx->xref.data() + (size_t)e * 18;
+        double c[3] = {0, 0, 0};
+        for (int k = 0; k < 6; ++k)
+            for (int d = 0; d < 3; ++d) c[d] += X[k * 3 + d] / 6.0;
+        double vol = 0.0;
+        for (const auto& f : faces) {
+            double v1[3], v2[3], vm[3];
+            for (int d = 0; d < 3; ++d) {
+                v1[d] = X[f[1] * 3 + d] - X[f[0] * 3 + d];
+                v2[d] = X[f[2] * 3 + d] - X[f[0] * 3 + d];
+                vm[d] = c[d] - X[f[0] * 3 + d];
+            }
+            const double b[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+            const double nb = std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+            vol += std::fabs((vm[0] * b[0] + vm[1] * b[1] + vm[2] * b[2]) / nb) * (nb / 2.0) / 3.0;
+        }
+        v0[e] = vol;
+    }
+    int bits = 10;
+    while (bits < 24 && (1 << bits) < 2 * eligible) ++bits;
+    const int H = 1 << bits;
+    TF_CK(dalloc(ctx->pk_place_d, (size_t)N));
+    TF_CK(cudaMemcpy(ctx->pk_place_d.p, pl.data(), (size_t)N, cudaMemcpyHostToDevice));
+    TF_CK(dalloc(ctx->pk_v0_d, sizeof(double) * (size_t)E));
+    TF_CK(cudaMemcpy(ctx->pk_v0_d.p, v0.data(), sizeof(double) * (size_t)E, cudaMemcpyHostToDevice));
+    TF_CK(dalloc(ctx->pk_mass_d, sizeof(double) * (size_t)N));
+    TF_CK(dalloc(ctx->pk_prm_d, sizeof(PackParams)));
+    TF_CK(dalloc(ctx->pk_bucket_cnt_d, sizeof(int32_t) * ((size_t)H + 1)));
+    TF_CK(dalloc(ctx->pk_bucket_start_d, sizeof(int32_t) * ((size_t)H + 1)));
+    TF_CK(dalloc(ctx->pk_bucket_nodes_d, sizeof(int32_t) * (size_t)std::max(eligible, 1)));
+    TF_CK(dalloc(ctx->pk_node_cnt_d, sizeof(int32_t) * ((size_t)N + 1)));
+    TF_CK(dalloc(ctx->pk_node_start_d, sizeof(int32_t) * ((size_t)N + 1)));
+    TF_CK(dalloc(ctx->pk_scan_d, sizeof(int32_t) * (size_t)std::max(scan_tmp_ints(H), scan_tmp_ints(N))));
+    TF_CK(dalloc(ctx->pk_x_d, sizeof(double) * 3 * (size_t)N));
+    ctx->pk_capacity = std::max(ctx->pk_capacity, 1024);
+    TF_CK(dalloc(ctx->pk_pairs_d, sizeof(int32_t) * 2 * (size_t)ctx->pk_capacity));
+    TF_CK(dalloc(ctx->pk_vals_d, sizeof(double) * 18 * (size_t)ctx->pk_capacity));
+    TF_CK(dalloc(ctx->pk_dfdx_d, sizeof(double) * 9 * (size_t)ctx->pk_capacity));
+    TF_CK(dalloc(ctx->pk_col_d, sizeof(int32_t) * 2 * (size_t)ctx->pk_capacity));
+    TF_CK(dalloc(ctx->pk_blk_d, sizeof(int32_t) * 2 * (size_t)ctx->pk_capacity));
+    ctx->pk_hash_bits = bits;
+    ctx->pk_pairs_n = 0;
+    ctx->pk_on = true;
+    return TF_OK;
+}
+
+int tf_detect_packing(tf_ctx* ctx, const double* x, int32_t* n_pairs) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!x) return TF_ERR_ARGUMENT;
+    if (!ctx->pk_on) return set_error(ctx, TF_ERR_STATE, "packing is not enabled (tf_set_packing)");
+    TF_CK(cudaMemcpyAsync(ctx->pk_x_d.p, x, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyHostToDevice, ctx->stream));
+    rc = packing_detect(ctx, dptr<double>(ctx->pk_x_d));
+    if (rc != TF_OK) return rc;
+    if (n_pairs) *n_pairs = ctx->pk_pairs_n;
+    return TF_OK;
+}
+
+int tf_get_packing(tf_ctx* ctx, int32_t max_pairs, int32_t* n_pairs, int32_t* pairs, double* threshold, double* mass,
+                   double* dfdx) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (max_pairs < 0) return TF_ERR_ARGUMENT;
+    if (n_pairs) *n_pairs = ctx->pk_on ? ctx->pk_pairs_n : 0;
+    if (!ctx->pk_on) return TF_OK;
+    const int np = std::min(max_pairs, ctx->pk_pairs_n);
+    if (pairs && np > 0) std::memcpy(pairs, ctx->h_pk_pairs.data(), sizeof(int32_t) * 2 * (size_t)np);
+    if (threshold) {
+        PackParams prm;
+        TF_CK(cudaMemcpy(&prm, ctx->pk_prm_d.p, sizeof(PackParams), cudaMemcpyDeviceToHost));
+        *threshold = prm.threshold;
+    }
+    if (mass) TF_CK(cudaMemcpy(mass, ctx->pk_mass_d.p, sizeof(double) * (size_t)ctx->N, cudaMemcpyDeviceToHost));
+    if (dfdx && np > 0) TF_CK(cudaMemcpy(dfdx, ctx->pk_dfdx_d.p, sizeof(double) * 9 * (size_t)np, cudaMemcpyDeviceToHost));
     return TF_OK;
 }
 
@@ -2772,6 +3007,7 @@ int tf_solve_direct(tf_ctx* ctx, const double* bsr_vals, const double* g, double
     if (rc != TF_OK) return rc;
     if (!bsr_vals || !g || !du) return TF_ERR_ARGUMENT;
     if (!ctx->slave.empty()) return set_error(ctx, TF_ERR_UNSUPPORTED, "direct solve: no slave-master pairs");
+    if (ctx->pk_on && ctx->pk_pairs_n > 0) return set_error(ctx, TF_ERR_UNSUPPORTED, "direct solve: packing blocks");
     const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
     TF_CK(cudaMemcpyAsync(ctx->vals.p, bsr_vals, sizeof(double) * 9 * (size_t)ctx->nnzb, cudaMemcpyHostToDevice, ctx->stream));
     TF_CK(cudaMemcpyAsync(ctx->g.p, g, bytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -2818,8 +3054,8 @@ int tf_adjoint_forward(tf_ctx* ctx, const double* x0, int32_t n_steps, double dt
     int rc = check_ctx(ctx);
     if (rc != TF_OK) return rc;
     if (!x0 || !x_final || n_steps <= 0 || checkpoint_every <= 0 || !(dt > 0)) return TF_ERR_ARGUMENT;
-    if (ctx->has_visc || !ctx->slave.empty() || ctx->T != 1) return set_error(ctx, TF_ERR_UNSUPPORTED,
-        "adjoint: single tissue without internal viscosity or slave-master pairs");
+    if (ctx->has_visc || !ctx->slave.empty() || ctx->T != 1 || ctx->pk_on) return set_error(ctx, TF_ERR_UNSUPPORTED,
+        "adjoint: single tissue without internal viscosity, slave-master pairs or packing");
     tf_step_stats local;
     tf_step_stats* st = stats ? stats : &local;
     rc = call_begin(ctx, st);

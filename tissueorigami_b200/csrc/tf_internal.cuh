@@ -285,6 +285,12 @@ struct KrylovWork {
     int32_t n_partials;                 // capacity in doubles
     KrylovScalars* sc;
     int32_t* dflags;
+    // packing blocks outside the element pattern (NULL when the step has no packing pair): row
+    // n's extra blocks are pk_vals[pk_blk[k]] at column pk_col[k], k in [pk_ptr[n], pk_ptr[n+1])
+    const int32_t* pk_ptr;
+    const int32_t* pk_col;
+    const int32_t* pk_blk;
+    const double* pk_vals;
 };
 
 cudaError_t launch_find_diag(const int32_t* rowptr, const int32_t* colidx, int32_t n, int32_t* diag,
@@ -381,6 +387,66 @@ struct MlSetup {
 // top = false: the diagonal blocks and their pseudo-inverses only (m.n_out = m.n_diag), the top
 // operator left as it is
 cudaError_t launch_ml_setup(const KrylovWork& w, const MlSetup& m, bool top, cudaStream_t s);
+
+// --- packing (tf_packing.cu) ------------------------------------------------------------------
+// Node-node contact of a single tissue (Simulation::detectPacingNodes, Simulation.cpp:7997-8153;
+// calculatePackingForcesImplicit3D / calculatePackingJacobian3D, :7307-7575).
+struct PackParams {
+    double bb0[2], bbs[2];  // bounding box minimum and size in x, y (Simulation::calculateBoundingBox)
+    double grid_sum[50];    // 10 x 5 grid of summed element side averages ([i * 5 + j]), then the
+    double grid_cnt[50];    //   squared detection thresholds (0.4 x the cell average)^2 in grid_sum
+    double col_sum, col_cnt;
+    double threshold;       // Simulation::packingThreshold = 0.4 x the columnar average side length
+    double cell;            // cell size of the candidate search: the largest detection threshold
+};
+struct PackArgs {
+    int32_t n_nodes, n_elems;
+    const ElemRecord* elems;
+    const double* x;             // [N][3] positions of the detection (the step's start)
+    const double* fg;            // [E][9]
+    const double* v0;            // [E] reference volumes
+    const uint8_t* exposed;      // [E] bit 0 apical, bit 1 basal exposed
+    const uint8_t* peripodial;   // [E]
+    const int8_t* placement;     // [N] 0 basal, 1 apical, other: never packs
+    const int32_t* rowptr;       // element pattern: nodes sharing an element with a node
+    const int32_t* colidx;
+    double* mass;                // [N]
+    PackParams* prm;
+    int32_t hash_bits;
+    int32_t* bucket_cnt;         // [2^hash_bits + 1]
+    int32_t* bucket_start;       // [2^hash_bits + 1]
+    int32_t* bucket_nodes;       // [N]
+    int32_t* node_cnt;           // [N + 1]
+    int32_t* node_start;         // [N + 1]
+    int32_t* scan_tmp;           // scan scratch
+    int32_t* pairs;              // [capacity][2]
+    int32_t capacity;
+};
+// masses, bounding box, thresholds, bucket fill and the per-node pair counts (node_start holds
+// their exclusive scan, node_start[N] the total)
+cudaError_t launch_packing_detect(const PackArgs& a, cudaStream_t s);
+// the pairs (i, j), i < j, in the reference's visiting order, into pairs[0 .. total) (total <= capacity)
+cudaError_t launch_packing_pairs(const PackArgs& a, cudaStream_t s);
+// Per Newton iteration: forces into g (free DoFs), -D into the diagonal blocks of i and j and +D
+// into the extra blocks (i, j) = pk_vals[2p], (j, i) = pk_vals[2p+1] (rows / columns of fixed DoFs
+// left out), D into dfdx[p] (the derivative block of pair p)
+struct PackTerms {
+    int32_t n_pairs;
+    const int32_t* pairs;
+    const double* x;             // [N][3] Newton iterate
+    const double* mass;
+    const PackParams* prm;
+    const uint8_t* fixmask;
+    const int32_t* diag;
+    double* vals;
+    double* g;
+    double* pk_vals;             // [2 P][9]
+    double* dfdx;                // [P][9]
+};
+cudaError_t launch_packing_terms(const PackTerms& a, cudaStream_t s);
+// Exclusive scan of n int32 counts into out[0 .. n] (out[n] = total); tmp holds scan_tmp_ints(n)
+int scan_tmp_ints(int n);
+cudaError_t launch_scan_i32(const int32_t* in, int32_t* out, int n, int32_t* tmp, cudaStream_t s);
 
 // --- dense inverses of the coarse operators (tf_dense.cu) -------------------------------------
 // In-place Gauss-Jordan inverse with partial pivoting of column-major matrices (a row-major

@@ -109,6 +109,22 @@ __device__ __forceinline__ void row_dot(const KrylovWork& w, int k0, int k1, con
     }
 }
 
+// y += the row's packing blocks outside the element pattern (none when w.pk_ptr is NULL); lane gl
+// of the row's G takes every G-th of them.
+template <int G>
+__device__ __forceinline__ void row_aux(const KrylovWork& w, int row, int gl, const double* __restrict__ xin,
+                                        double& y0, double& y1, double& y2) {
+    if (!w.pk_ptr) return;
+    for (int k = w.pk_ptr[row] + gl; k < w.pk_ptr[row + 1]; k += G) {
+        const int c = w.pk_col[k];
+        const double* B = w.pk_vals + (size_t)w.pk_blk[k] * 9;
+        const double x0 = __ldcg(xin + c * 3), x1 = __ldcg(xin + c * 3 + 1), x2 = __ldcg(xin + c * 3 + 2);
+        y0 += B[0] * x0 + B[1] * x1 + B[2] * x2;
+        y1 += B[3] * x0 + B[4] * x1 + B[5] * x2;
+        y2 += B[6] * x0 + B[7] * x1 + B[8] * x2;
+    }
+}
+
 __global__ void k_block_jacobi(KrylovWork w) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= w.n_nodes) return;
@@ -236,7 +252,10 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv(KrylovWork w, const doubl
     const int gl = threadIdx.x & (kGroup - 1);
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    if (row < w.n_nodes) row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+    if (row < w.n_nodes) {
+        row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+        row_aux<kGroup>(w, row, gl, xin, y0, y1, y2);
+    }
 #pragma unroll
     for (int off = kGroup / 2; off > 0; off >>= 1) {
         y0 += __shfl_xor_sync(0xffffffffu, y0, off);
@@ -285,7 +304,10 @@ __global__ void __launch_bounds__(kSpmvThreads) k_residual(KrylovWork w, const d
     const int gl = threadIdx.x & (kGroup - 1);
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    if (row < w.n_nodes) row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+    if (row < w.n_nodes) {
+        row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+        row_aux<kGroup>(w, row, gl, xin, y0, y1, y2);
+    }
 #pragma unroll
     for (int off = kGroup / 2; off > 0; off >>= 1) {
         y0 += __shfl_xor_sync(0xffffffffu, y0, off);
@@ -438,7 +460,10 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
     for (int rb = r0; rb < r1; rb += groups) {
         const int row = rb + threadIdx.x / kGroup;
         double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-        if (row < r1) row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+        if (row < r1) {
+            row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+            row_aux<kGroup>(w, row, gl, xin, y0, y1, y2);
+        }
 #pragma unroll
         for (int off = kGroup / 2; off > 0; off >>= 1) {
             y0 += __shfl_xor_sync(0xffffffffu, y0, off);

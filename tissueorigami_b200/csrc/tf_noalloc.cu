@@ -113,6 +113,8 @@ extern "C" int tf_solve_bsr_noalloc(int32_t n_nodes, const int32_t* d_rowptr, co
     w.n_partials = (int32_t)kPartials;
     w.sc = reinterpret_cast<KrylovScalars*>(w.partials + kPartials);
     w.dflags = reinterpret_cast<int32_t*>(reinterpret_cast<double*>(w.sc) + (sizeof(KrylovScalars) + 7) / 8);
+    w.pk_ptr = w.pk_col = w.pk_blk = nullptr;  // the caller's matrix is all there is
+    w.pk_vals = nullptr;
 
     // scalars, tickets and flags must start at zero; everything else is overwritten
     if (cudaMemsetAsync(w.sc, 0, sizeof(double) * kScalars, s) != cudaSuccess) return TF_ERR_CUDA;

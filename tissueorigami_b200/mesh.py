@@ -305,6 +305,34 @@ def _smooth_field(rng: np.random.Generator, xy: np.ndarray, length: float, n_fea
     return (np.cos(xy @ w.T + b) @ a) * math.sqrt(2.0 / n_feat)
 
 
+def stacked_sheets(nx: int = 10, ny: int = 6, spacing: float = 2.0, thickness: float = 4.0, gap: float = 0.5,
+                   E: float = 1000.0, n_steps: int = 3, **kw) -> Tissue:
+    """Two one-layer rectangles (small_rectangle of nx x ny nodes) in one tissue, the second one
+    mirrored through the plane between them so that the two apical surfaces face each other
+    across `gap`: every apical node of the lower sheet lies `gap` below one of the upper sheet,
+    which makes them packing pairs (the reference packs same-placement nodes that share no
+    element and are closer than 0.4 x the local average side length). Each sheet's basal nodes
+    are fixed in z. The upper sheet's prisms keep the reference's node order (0-2 basal, 3-5
+    apical) with nodes 1 and 2 (4 and 5) swapped, so their orientation stays positive."""
+    a = small_rectangle(nx=nx, ny=ny, spacing=spacing, thickness=thickness, E=E, n_steps=n_steps, **kw)
+    n = a.n_nodes
+    perm = [0, 2, 1, 3, 5, 4]
+    top = 2.0 * thickness + gap
+    xb = a.x.copy()
+    xb[:, 2] = top - xb[:, 2]
+    conn_b = a.conn[:, perm] + n
+    xref_b = a.xref.reshape(-1, 6, 3)[:, perm, :].copy()
+    xref_b[:, :, 2] = top - xref_b[:, :, 2]
+    cat = lambda u, v: np.concatenate([u, v])
+    t = Tissue("stacked_sheets", cat(a.conn, conn_b), cat(a.xref, xref_b.reshape(-1, 18)), cat(a.x, xb),
+               cat(a.lam, a.lam), cat(a.mu, a.mu), cat(a.eta, a.eta), cat(a.fixed, a.fixed),
+               cat(a.ext_visc, a.ext_visc), cat(a.exposed, a.exposed), cat(a.peripodial, a.peripodial),
+               cat(a.rates, a.rates), cat(a.angles, a.angles), cat(a.node_placement, a.node_placement),
+               cat(a.at_circumference, a.at_circumference), dt=a.dt, n_steps=n_steps,
+               newton_tol=a.newton_tol, seed=a.seed)
+    return t
+
+
 def large_slab(seed: int = 1002, nx: int = 1000, ny: int = 500, spacing: float = 0.5,
                layer_thickness: float = 1.0, n_layers: int = 3, E_median: float = 1000.0,
                sigma_log: float = 0.3, nu: float = 0.3, apical_visc: float = WING_DISC_APICAL_VISC,

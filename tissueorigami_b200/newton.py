@@ -43,13 +43,46 @@ class NewtonRaphsonSolver:
 
     # -- construction from a synthetic / loaded tissue ---------------------------------------
     @classmethod
-    def from_tissue(cls, t: Tissue, params: Optional[capi.Params] = None, **overrides):
+    def from_tissue(cls, t: Tissue, params: Optional[capi.Params] = None, packing: bool = False, **overrides):
+        """packing: run the reference's node-node packing (detection after every step's growth,
+        forces and Jacobian in every Newton iteration) with the tissue's node placements."""
         overrides.setdefault("newton_tol", t.newton_tol)
         s = cls(t.conn, t.xref, t.n_nodes, params, **overrides)
         s.set_material(t.lam, t.mu, t.eta)
         s.set_boundary(t.fixed, t.ext_visc, t.slave_master)
         s.set_growth(t.fg, t.rates, t.angles, t.exposed, t.peripodial)
+        if packing:
+            s.set_packing(t.node_placement)
         return s
+
+    # -- packing (Simulation::detectPacingNodes, calculatePackingForcesImplicit3D / Jacobian3D) --
+    def set_packing(self, node_placement=None):
+        """Turn packing on with node_placement[N] (0 basal, 1 apical, 2 other), or off with None."""
+        if node_placement is None:
+            capi.check(self._L.tf_set_packing(self._h, 0, None), "tf_set_packing", self._h)
+            return
+        pl = np.ascontiguousarray(node_placement, dtype=np.int32)
+        capi.check(self._L.tf_set_packing(self._h, 1, capi.iptr(pl)), "tf_set_packing", self._h)
+
+    def detect_packing(self, x):
+        """Detect the packing pairs at positions x with the current growth tensors; returns their count."""
+        n = ctypes.c_int32()
+        capi.check(self._L.tf_detect_packing(self._h, capi.dptr(_f64(x).reshape(-1)), ctypes.byref(n)),
+                   "tf_detect_packing", self._h)
+        return n.value
+
+    def packing(self):
+        """(pairs[P,2], packingThreshold, node masses[N], derivative blocks dF_i/dx_i [P,3,3] of the last assembly)."""
+        n = ctypes.c_int32()
+        capi.check(self._L.tf_get_packing(self._h, 0, ctypes.byref(n), None, None, None, None), "tf_get_packing", self._h)
+        P = n.value
+        pairs = np.zeros((max(P, 1), 2), np.int32)
+        dfdx = np.zeros((max(P, 1), 3, 3))
+        mass = np.zeros(self.n_nodes)
+        thr = ctypes.c_double()
+        capi.check(self._L.tf_get_packing(self._h, P, ctypes.byref(n), capi.iptr(pairs), ctypes.byref(thr),
+                                          capi.dptr(mass), capi.dptr(dfdx)), "tf_get_packing", self._h)
+        return pairs[:P], thr.value, mass, dfdx[:P]
 
     def close(self):
         if getattr(self, "_h", None):
