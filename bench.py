@@ -317,7 +317,8 @@ def run_b200(args) -> None:
     pc_eff, n_coarse, refreshes = s.preconditioner()
     sched["precond_effective"] = {0: "block_jacobi", 1: "ilu0", 2: "two_level", 3: "multilevel"}.get(pc_eff, pc_eff)
     sched["krylov_method"] = {1: "bicgstab", 2: "conjugate gradients",
-                              3: "conjugate gradients, finished by bicgstab on indefinite solves"}.get(max(methods), "none")
+                              3: "conjugate gradients, finished by bicgstab on indefinite solves",
+                              4: "minres on steps with packing pairs"}.get(max(methods), "none")
     sched["krylov_iters_cg_share"] = kry_cg / max(kry, 1)
     # the reference detects node-node packing after every step's growth; the pairs it finds add
     # forces and Jacobian blocks to the Newton iterations

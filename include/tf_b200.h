@@ -122,7 +122,9 @@ typedef struct tf_step_stats {
     double ms_solve_kernel;     /* device time inside the persistent BiCGStab launches      */
     int32_t solve_launches;     /* number of those launches                                 */
     int32_t krylov_method;      /* 1 BiCGStab, 2 conjugate gradients, 3 CG fell back to     */
-                                /* BiCGStab on some solve (the largest over the call)       */
+                                /* BiCGStab on some solve, 4 MINRES (a symmetric J with    */
+                                /* packing pairs; block preconditioner |D|); the largest    */
+                                /* over the call                                            */
     int32_t krylov_iters_cg;    /* the conjugate-gradient iterations in krylov_iters_total  */
                                 /* (persistent solves; the rest are BiCGStab's)            */
 } tf_step_stats;

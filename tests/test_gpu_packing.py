@@ -78,12 +78,15 @@ def test_steps_with_packing_match_oracle():
     counts_ref = []
     x_ref, _, it_ref, _ = O.simulate_sparse(t, n_steps=3, packing=True, pair_counts=counts_ref)
     assert counts_ref == [45, 15, 45]
-    with NewtonRaphsonSolver.from_tissue(t, packing=True, krylov_rtol=1e-14) as s:
+    with NewtonRaphsonSolver.from_tissue(t, packing=True) as s:
         x = t.x.copy()
         its, counts = [], []
         for _ in range(3):
             x, rc, st = s.runOneStep(x, t.dt)
             assert rc == capi.TF_OK
+            # the pairs' repulsion makes J indefinite (91 of 720 eigenvalues negative at the first
+            # iterate): MINRES with the |D| block preconditioner solves those systems
+            assert st["krylov_method"] == 4
             its.append(st["newton_iters"])
             counts.append(len(s.packing()[0]))
     assert counts == counts_ref
@@ -129,5 +132,7 @@ def test_device_detection_finds_no_pairs_in_the_benchmark_tissues(name):
         assert s.detect_packing(t.x) == 0
         _, thr, mass, _ = s.packing()
     _, thr_ref = O.detect_packing(t, t.x)
-    assert abs(thr - thr_ref) <= 1e-12 * thr_ref
+    # the threshold averages up to 6 M side lengths: the oracle sums them in order, the device
+    # with atomics; the order alone moves such a sum by up to ~n eps (2.7e-11 measured on the slab)
+    assert abs(thr - thr_ref) <= 1e-9 * thr_ref
     assert _rel(mass, O.node_masses(t, t.fg)) <= 1e-12

@@ -748,6 +748,8 @@ BatchPlan make_plan(tf_ctx* c) {
     BatchPlan p{};
     p.cg = use_cg(c) ? 1 : 0;
     p.warm = 0;
+    // a symmetric J with packing pairs is indefinite across every pair: MINRES
+    p.minres = (p.cg && c->pk_on && c->pk_pairs_n > 0) ? 1 : 0;
     p.agg_per_cta = (c->coarse_m > 0 && c->coarse_ok) ? c->coarse_m : 0;
     p.n_coarse = c->n_coarse;
     p.node_d = dptr<double>(c->node_d);

@@ -45,6 +45,7 @@ enum KrylovMethod : int32_t {
     KM_BICGSTAB = 1,     // BiCGStab
     KM_CG = 2,           // preconditioned conjugate gradients (symmetric J)
     KM_CG_FALLBACK = 3,  // CG met a non-positive curvature; BiCGStab solved the system
+    KM_MINRES = 4,       // MINRES with the |D| block preconditioner (symmetric J with packing pairs)
 };
 
 enum KrylovStatus : int32_t {
@@ -135,6 +136,8 @@ struct BatchPlan {
     // BiCGStab starts from the iterate x and residual r already in the work vectors (those that
     // conjugate gradients left when it met a non-positive curvature) instead of x = 0, r = b
     int32_t warm;
+    // MINRES instead (symmetric J that packing pairs make indefinite; block preconditioner only)
+    int32_t minres;
     // tissues solved by one CTA each (the packing CTAs' tissues), heaviest first: once its group
     // tissue (if any) is solved, every CTA takes the next one (atomic ticket in queue_head, zeroed
     // before each launch), so these tissues are spread over the CTAs as they become free

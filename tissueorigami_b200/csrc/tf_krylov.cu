@@ -478,12 +478,68 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
                 d0 += w.rhat[row * 3] * y0 + w.rhat[row * 3 + 1] * y1 + w.rhat[row * 3 + 2] * y2;
             } else if (KIND == 3) {
                 d0 += w.p[row * 3] * y0 + w.p[row * 3 + 1] * y1 + w.p[row * 3 + 2] * y2;
+            } else if (KIND == 4) {  // MINRES: (v, A v) and (v, r1), v in p, r1 in r
+                d0 += w.p[row * 3] * y0 + w.p[row * 3 + 1] * y1 + w.p[row * 3 + 2] * y2;
+                d1 += w.p[row * 3] * w.r[row * 3] + w.p[row * 3 + 1] * w.r[row * 3 + 1] + w.p[row * 3 + 2] * w.r[row * 3 + 2];
             } else {
                 d0 += w.s[row * 3] * y0 + w.s[row * 3 + 1] * y1 + w.s[row * 3 + 2] * y2;
                 d1 += y0 * y0 + y1 * y1 + y2 * y2;
             }
         }
     }
+}
+
+// |D_n|^-1 = V |Lambda|^-1 V^T of the symmetric part of node n's diagonal block (cyclic Jacobi
+// rotations): a symmetric positive definite block preconditioner for an indefinite symmetric J
+// (MINRES). An eigenvalue below 1e-300 in magnitude is taken as 1.
+__device__ __forceinline__ void block_abs_inverse_row(const KrylovWork& w, int n) {
+    const double* B = w.vals + (size_t)w.diag[n] * 9;
+    double A[9], V[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) A[r * 3 + c] = 0.5 * (B[r * 3 + c] + B[c * 3 + r]);
+    for (int sweep = 0; sweep < 12; ++sweep) {
+        const double off = A[1] * A[1] + A[2] * A[2] + A[5] * A[5];
+        const double dia = A[0] * A[0] + A[4] * A[4] + A[8] * A[8];
+        if (!(off > 1e-32 * dia)) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                const double apq = A[p * 3 + q];
+                if (apq == 0.0) continue;
+                const double tau = (A[q * 3 + q] - A[p * 3 + p]) / (2.0 * apq);
+                const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                const double c = 1.0 / sqrt(1.0 + tt * tt), s = tt * c;
+                for (int k = 0; k < 3; ++k) {
+                    const double akp = A[k * 3 + p], akq = A[k * 3 + q];
+                    A[k * 3 + p] = c * akp - s * akq;
+                    A[k * 3 + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double apk = A[p * 3 + k], aqk = A[q * 3 + k];
+                    A[p * 3 + k] = c * apk - s * aqk;
+                    A[q * 3 + k] = s * apk + c * aqk;
+                }
+                A[p * 3 + q] = A[q * 3 + p] = 0.0;
+                for (int k = 0; k < 3; ++k) {
+                    const double vkp = V[k * 3 + p], vkq = V[k * 3 + q];
+                    V[k * 3 + p] = c * vkp - s * vkq;
+                    V[k * 3 + q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    double inv[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double l = fabs(A[k * 4]);
+        inv[k] = (l > 1e-300 && isfinite(l)) ? 1.0 / l : 1.0;
+    }
+    double* D = w.dinv + (size_t)n * 9;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            D[r * 3 + c] = V[r * 3] * V[c * 3] * inv[0] + V[r * 3 + 1] * V[c * 3 + 1] * inv[1] + V[r * 3 + 2] * V[c * 3 + 2] * inv[2];
 }
 
 __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
@@ -1406,22 +1462,168 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
     return true;
 }
 
+// Preconditioned MINRES (Paige and Saunders' recurrences, as in the reference implementation
+// that SciPy's minres follows) on tissue t for a symmetric but indefinite J - the Jacobian of a
+// step with packing pairs, whose repulsion has a negative stiffness across each pair - with the
+// symmetric positive definite block preconditioner |D|^-1 (block_abs_inverse_row). Vectors: x, v
+// in p, A v in v, r1 in r, r2 in rhat, z = M^-1 r2 in phat, the direction w in s and its
+// predecessor in shat. Three group barriers per iteration: after v (the SpMV gathers it), after
+// the SpMV with (v, A v) and (v, r1), after r2 / z with (r2, z). Stops when the preconditioned
+// residual estimate phibar <= rtol phibar_0 (the host reports phibar / phibar_0 as the relative
+// residual). Returns false when a group barrier timed out.
+__device__ bool solve_tissue_minres(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int pbase, double rtol,
+                                    int max_iter, double* smem, double* sb) {
+    if (!plan.active[t]) return true;
+    const int nct = plan.ncta[t];
+    int r0, r1;
+    group_split(plan.row0[t], plan.row0[t + 1], lc, nct, plan.group, r0, r1);
+    GridBarrier* bar = plan.barriers + t;
+    double* part[2] = {w.partials + 4 * pbase, w.partials + 4 * pbase + 2 * nct};
+    int pb = 0;
+    double v2[2] = {0.0, 0.0};
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        block_abs_inverse_row(w, n);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            const double b = w.b[d];
+            w.x[d] = 0.0;
+            w.r[d] = b;
+            w.rhat[d] = b;
+            w.s[d] = 0.0;
+            w.shat[d] = 0.0;
+            v2[0] += b * b;
+        }
+        apply_dinv(w.dinv, n, w.rhat, w.phat);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) v2[1] += w.rhat[n * 3 + i] * w.phat[n * 3 + i];
+    }
+    write_partials<2>(v2, part[pb], lc, smem);
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    double t1[1], t2[2];
+    sum_partials<2>(part[pb], nct, t2, smem, sb);
+    pb ^= 1;
+    const double bb = t2[0];
+    double beta = t2[1] > 0.0 ? sqrt(t2[1]) : 0.0;
+    const double beta1 = beta;
+    double oldb = 0.0, dbar = 0.0, epsln = 0.0, phibar = beta1, cs = -1.0, sn = 0.0;
+    int it = 0;
+    int status = (!isfinite(bb) || !isfinite(t2[1])) ? KS_NONFINITE
+                 : (bb == 0.0 || beta1 == 0.0)       ? (bb == 0.0 ? KS_CONVERGED : KS_BREAKDOWN)
+                                                     : KS_RUNNING;
+    if (status == KS_RUNNING) {
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) w.p[n * 3 + i] = w.phat[n * 3 + i] / beta;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+    }
+    while (status == KS_RUNNING) {
+        double d0 = 0.0, d1 = 0.0;
+        spmv_rows<4>(w, r0, r1, w.p, w.v, d0, d1);
+        double v3[2] = {d0, d1};
+        write_partials<2>(v3, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+        sum_partials<2>(part[pb], nct, t2, smem, sb);
+        pb ^= 1;
+        const double c1 = it >= 1 ? beta / oldb : 0.0;
+        const double alfa = t2[0] - c1 * t2[1];
+        const double c2 = alfa / beta;
+        double e1[1] = {0.0};
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                const double y = w.v[d] - c1 * w.r[d] - c2 * w.rhat[d];
+                w.r[d] = w.rhat[d];
+                w.rhat[d] = y;
+            }
+            apply_dinv(w.dinv, n, w.rhat, w.phat);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) e1[0] += w.rhat[n * 3 + i] * w.phat[n * 3 + i];
+        }
+        write_partials<1>(e1, part[pb], lc, smem);
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+        sum_partials<1>(part[pb], nct, t1, smem, sb);
+        pb ^= 1;
+        oldb = beta;
+        if (!isfinite(t1[0]) || !isfinite(alfa)) {
+            status = KS_NONFINITE;
+            break;
+        }
+        beta = t1[0] > 0.0 ? sqrt(t1[0]) : 0.0;
+        const double oldeps = epsln;
+        const double delta = cs * dbar + sn * alfa;
+        const double gbar = sn * dbar - cs * alfa;
+        epsln = sn * beta;
+        dbar = -cs * beta;
+        const double gamma = sqrt(gbar * gbar + beta * beta);
+        if (!(gamma > 0.0)) {
+            status = KS_BREAKDOWN;
+            break;
+        }
+        cs = gbar / gamma;
+        sn = beta / gamma;
+        const double phi = cs * phibar;
+        phibar = sn * phibar;
+        // w2 <- w, w <- (v - oldeps w2_old - delta w) / gamma, x += phi w, next v = z / beta
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                const double wo = w.s[d], w2o = w.shat[d];
+                const double wn = (w.p[d] - oldeps * w2o - delta * wo) / gamma;
+                w.shat[d] = wo;
+                w.s[d] = wn;
+                w.x[d] += phi * wn;
+                w.p[d] = beta > 0.0 ? w.phat[d] / beta : 0.0;
+            }
+        ++it;
+        if (!isfinite(phibar))
+            status = KS_NONFINITE;
+        else if (phibar <= rtol * beta1 || beta == 0.0)
+            status = KS_CONVERGED;
+        else if (it >= max_iter)
+            status = KS_MAXIT;
+        else if (!group_barrier(bar, nct, w.dflags))
+            return false;
+    }
+    if (lc == 0 && threadIdx.x == 0) {
+        KrylovScalars* sc = plan.scalars + t;
+        const double rel = beta1 > 0.0 ? phibar / beta1 : 0.0;
+        sc->bb = bb;
+        sc->rr = rel * rel * bb;  // the relative residual the host reports is phibar / phibar_0
+        sc->rho = beta;
+        sc->rho_prev = oldb;
+        sc->alpha = cs;
+        sc->omega = sn;
+        sc->tol2 = rtol * rtol * bb;
+        sc->iter = it;
+        sc->max_iter = max_iter;
+        sc->status = status;
+        sc->method = KM_MINRES;
+    }
+    return true;
+}
+
 // Two builds of the persistent solve: one 768-thread CTA per SM (single tissues with the
 // two-level preconditioner, large tissues; up to 80 registers) and four 256-thread CTAs per SM
 // (batches, small block-Jacobi tissues; registers capped at 64 so that 32 warps per SM hide the
 // latency of the memory-bound batched solve).
-template <int THREADS, int MIN_BLOCKS, bool CG>
+// METHOD: 0 BiCGStab, 1 conjugate gradients, 2 MINRES (each its own build, so none pays the
+// others' registers).
+template <int THREADS, int MIN_BLOCKS, int METHOD>
 __device__ __forceinline__ bool solve_by(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int pbase,
                                          double rtol, int max_iter, double* smem, double* sb, double* red, double* ys,
                                          double* Ms, double* cs, float* cinv_s) {
-    if (CG) {
+    if (METHOD == 1) {
         bool indefinite = false;
         return solve_tissue_cg(w, plan, t, lc, pbase, rtol, max_iter, smem, sb, red, ys, Ms, cs, cinv_s, indefinite);
     }
+    if (METHOD == 2) return solve_tissue_minres(w, plan, t, lc, pbase, rtol, max_iter, smem, sb);
     return solve_tissue(w, plan, t, lc, pbase, rtol, max_iter, smem, sb, red, ys, Ms, cs, cinv_s);
 }
 
-template <int THREADS, int MIN_BLOCKS, bool CG>
+template <int THREADS, int MIN_BLOCKS, int METHOD>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(KrylovWork w, BatchPlan plan, double rtol,
                                                                         int max_iter) {
 
@@ -1438,7 +1640,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(Krylov
     if (j0 < plan.cta_list_ptr[blockIdx.x + 1]) {
         const int t = plan.cta_list[j0];
         if (plan.ncta[t] > 1 &&
-            !solve_by<THREADS, MIN_BLOCKS, CG>(w, plan, t, blockIdx.x - plan.cta0[t], plan.cta0[t], rtol, max_iter, smem,
+            !solve_by<THREADS, MIN_BLOCKS, METHOD>(w, plan, t, blockIdx.x - plan.cta0[t], plan.cta0[t], rtol, max_iter, smem,
                                                sb, red, ys, Ms, cs, cinv_s))
             return;
     }
@@ -1450,7 +1652,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) k_bicgstab_batched(Krylov
         const int q = ticket;
         __syncthreads();
         if (q >= plan.n_queue) break;
-        if (!solve_by<THREADS, MIN_BLOCKS, CG>(w, plan, plan.queue[q], 0, plan.n_cta + blockIdx.x, rtol, max_iter, smem, sb,
+        if (!solve_by<THREADS, MIN_BLOCKS, METHOD>(w, plan, plan.queue[q], 0, plan.n_cta + blockIdx.x, rtol, max_iter, smem, sb,
                                                red, ys, Ms, cs, cinv_s))
             return;
     }
@@ -1818,9 +2020,10 @@ cudaError_t launch_symmetrize(double* m, int n, int ld, long long stride, int co
 }
 
 namespace {
-void (*persist_kernel(int threads, bool cg))(KrylovWork, BatchPlan, double, int) {
-    if (cg) return threads == 768 ? k_bicgstab_batched<768, 1, true> : k_bicgstab_batched<256, 4, true>;
-    return threads == 768 ? k_bicgstab_batched<768, 1, false> : k_bicgstab_batched<256, 4, false>;
+void (*persist_kernel(int threads, int method))(KrylovWork, BatchPlan, double, int) {
+    if (method == 2) return threads == 768 ? k_bicgstab_batched<768, 1, 2> : k_bicgstab_batched<256, 4, 2>;
+    if (method == 1) return threads == 768 ? k_bicgstab_batched<768, 1, 1> : k_bicgstab_batched<256, 4, 1>;
+    return threads == 768 ? k_bicgstab_batched<768, 1, 0> : k_bicgstab_batched<256, 4, 0>;
 }
 }  // namespace
 
@@ -1829,8 +2032,8 @@ int persistent_max_grid(int device, int threads) {
     if (threads != 256 && threads != 768) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
     occ = 1 << 30;
-    for (int cg = 0; cg < 2; ++cg) {  // both methods' builds must fit the same plan
-        const auto kern = persist_kernel(threads, cg != 0);
+    for (int method = 0; method < 3; ++method) {  // every method's build must fit the same plan
+        const auto kern = persist_kernel(threads, method);
         int o = 0;
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemBytes) != cudaSuccess)
             return 0;
@@ -1855,7 +2058,8 @@ cudaError_t launch_bicgstab_batched(const KrylovWork& w, const BatchPlan& plan, 
     const size_t smem = plan.agg_per_cta > 0 ? sizeof(float) * 6 * plan.agg_per_cta * (size_t)plan.n_coarse : 0;
     if (smem > (size_t)kCoarseSmemBytes) return cudaErrorInvalidValue;
     if (threads != 256 && threads != 768) return cudaErrorInvalidValue;
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(persist_kernel(threads, plan.cg != 0)), dim3(plan.n_cta),
+    const int method = plan.minres ? 2 : (plan.cg ? 1 : 0);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(persist_kernel(threads, method)), dim3(plan.n_cta),
                                        dim3(threads), args, smem, s);
 }
 
