@@ -357,6 +357,22 @@ int tf_adjoint_backward(tf_ctx* ctx, const double* dL_dx_final, double* dL_drate
  * every SM. The element kernel's own ceiling: its closed-form tangent is compute-bound. */
 int tf_measure_fp64(int32_t device, double* tflops);
 
+/* Lumen (Lumen.cpp, added to the Newton system at NewtonRaphsonSolver.cpp:242-249): the pressure
+ * of the volume V = sum (1/6) (x3 x x1) . x2 enclosed by the apical triangles (element nodes 3,
+ * 4, 5) of the n_elems listed elements (the reference's lumen elements: apical, or single-layer
+ * elements spanning the tissue). The ideal volume V0 is V at positions x [N*3] (the constructor,
+ * Lumen.cpp:11-68) and grows by exp(ln(growth_fold) / 86400 s x t) to the end of every step
+ * (Lumen::growLumen; growth_fold <= 0: no growth). Every Newton iteration adds the forces
+ * -bulk_modulus (V - V0) / V0 / (6 V0) x 6 dV/dx and the Jacobian of Lumen::calculateJacobian:
+ * its triangle-local blocks in J, its rank-one part bulk / (36 V0^2) G G^T by a second Krylov
+ * solve (Sherman-Morrison), so a step with a lumen costs two solves per Newton iteration.
+ * n_elems = 0 removes the lumen. Single tissue, no slave-master pairs, persistent solve. */
+int tf_set_lumen(tf_ctx* ctx, int32_t n_elems, const int32_t* elems, double bulk_modulus, double growth_fold,
+                 const double* x);
+/* The enclosed volume at the last assembly, the step's ideal volume, and G [N*3] (the nodal sums
+ * of 6 dV/dx with fixed components zeroed; may be NULL). */
+int tf_get_lumen(tf_ctx* ctx, double* volume, double* ideal_volume, double* G);
+
 /* Packing (node-node contact): Simulation::detectPacingNodes (Simulation.cpp:7997-8153) after
  * every time step's growth, with the node masses of Simulation::updateNodeMasses (:7587-7596),
  * and in every Newton iteration the forces and Jacobian blocks of

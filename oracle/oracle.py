@@ -60,6 +60,10 @@ def lib():
         L.tfo_node_masses.restype = None
         L.tfo_packing_terms.argtypes = [c_int, _I, _D, _D, c_double, _D, _D]
         L.tfo_packing_terms.restype = None
+        L.tfo_lumen_volume.argtypes = [c_int, _I, _D]
+        L.tfo_lumen_volume.restype = c_double
+        L.tfo_lumen_terms.argtypes = [c_int, c_int, _I, _D, _U, c_double, c_double, _D, _D]
+        L.tfo_lumen_terms.restype = None
         _lib = L
     return _lib
 
@@ -280,6 +284,36 @@ def add_packing(t, J, g, x, pairs, mass, threshold):
     return (J + sp.csr_matrix((vals, (rows, cols)), shape=(n, n))).tocsr(), g
 
 
+def lumen_triangles(t, elems):
+    """The apical triangles (nodes 3, 4, 5) of the lumen elements (Lumen::Lumen, Lumen.cpp:11-68)."""
+    return _c(np.asarray(t.conn)[np.asarray(elems)][:, 3:6], np.int32)
+
+
+def lumen_volume(t, x, tri):
+    tri = _c(np.asarray(tri).reshape(-1, 3), np.int32)
+    return float(lib().tfo_lumen_volume(tri.shape[0], _i(tri), _d(_c(x, np.float64))))
+
+
+def lumen_terms(t, x, tri, bulk, ideal):
+    """Lumen pressure forces [N,3] and its Jacobian K[3N,3N] (the reference's storage, fixed rows
+    and columns left out) at positions x (Lumen::calculateResiduals / calculateJacobian)."""
+    tri = _c(np.asarray(tri).reshape(-1, 3), np.int32)
+    n = 3 * t.n_nodes
+    forces = np.zeros((t.n_nodes, 3))
+    K = np.zeros((n, n))
+    lib().tfo_lumen_terms(t.n_nodes, tri.shape[0], _i(tri), _d(_c(x, np.float64)), _u(_c(t.fixed, np.uint8)),
+                          float(bulk), float(ideal), _d(forces), _d(K))
+    return forces, K
+
+
+def add_lumen(t, J, g, x, tri, bulk, ideal):
+    """J + K_lumen^T (J = K^T) and g + the lumen forces."""
+    import scipy.sparse as sp
+
+    forces, K = lumen_terms(t, x, tri, bulk, ideal)
+    return (J + sp.csr_matrix(K.T)).tocsr(), g + forces.reshape(-1)
+
+
 def bsr_to_scipy(rowptr, colidx, vals, n_nodes):
     import scipy.sparse as sp
 
@@ -353,12 +387,12 @@ def sparse_direct_solve(J, g, perm=None):
 
 
 def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter=20, threads=0, perm=None,
-                       packing=None):
+                       packing=None, lumen=None):
     """Simulation::updateStepNR with sparse assembly of J = K^T and SuperLU (scipy) as the
     direct solve standing in for Pardiso. No slave-master pairs. Returns (x, iterations, norms).
     perm: optional fill-reducing DoF order for the factorisation (nested_dissection).
     packing: optional (pairs, masses, threshold) of the step; its forces and Jacobian are added
-    at every iteration's positions."""
+    at every iteration's positions. lumen: optional (triangles, bulk modulus, ideal volume)."""
     rowptr, colidx = block_pattern(t)
     un = np.array(x_n, dtype=np.float64, copy=True).reshape(-1, 3)
     uk = un.copy()
@@ -371,6 +405,8 @@ def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter
         J = bsr_to_scipy(rowptr, colidx, vals, t.n_nodes)
         if packing is not None:
             J, g = add_packing(t, J, g, uk, *packing)
+        if lumen is not None:
+            J, g = add_lumen(t, J, g, uk, *lumen)
         du = sparse_direct_solve(J, g, perm)
         d = float(np.sqrt(np.sum(du * du)))
         norms.append(d)
@@ -383,18 +419,27 @@ def newton_step_sparse(t, x_n, visc_surface, inv_fg, dt=None, tol=None, max_iter
 
 
 def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0, reorder=False, positions=None,
-                    packing=False, pair_counts=None):
+                    packing=False, pair_counts=None, lumen=None):
     """n time steps with the growth prologue and the sparse Newton step. reorder: factorise in
     nested-dissection order (large meshes). positions: optional list that receives the positions
     at the start of every step and after the last. packing: node masses and packing pairs
     detected after each step's growth (Simulation::runOneStep, Simulation.cpp:6065-6076), their
     forces and Jacobian in every Newton iteration; pair_counts: optional list of each step's
-    number of pairs."""
+    number of pairs. lumen: optional (lumen elements, bulk modulus, growth fold per day): the
+    ideal volume starts at the initial enclosed volume and grows as V0 exp(ln(fold) / 86400 t)
+    to the end of each step (Lumen::growLumen, Lumen.cpp:331-334; Simulation.cpp:6019)."""
     x = np.array(t.x, dtype=np.float64, copy=True)
     fg = np.array(t.fg, dtype=np.float64, copy=True)
     iters, traces = [], []
     perm = nested_dissection(t, *block_pattern(t)) if reorder else None
-    for _ in range(n_steps if n_steps is not None else t.n_steps):
+    lm = None
+    if lumen is not None:
+        tri = lumen_triangles(t, lumen[0])
+        v_init = lumen_volume(t, x, tri)
+        rate = np.log(lumen[2]) / 3600.0 / 24.0 if lumen[2] > 0 else 0.0
+    for step in range(n_steps if n_steps is not None else t.n_steps):
+        if lumen is not None:
+            lm = (tri, lumen[1], v_init * np.exp(rate * (step + 1) * t.dt))
         if positions is not None:
             positions.append(x.copy())
         fg, inv, _, _ = grow(t, x, fg)
@@ -406,7 +451,7 @@ def simulate_sparse(t, n_steps=None, max_iter=20, tol=None, threads=0, reorder=F
             if pair_counts is not None:
                 pair_counts.append(len(pairs))
         x, it, norms = newton_step_sparse(t, x, vs, inv, tol=tol, max_iter=max_iter, threads=threads, perm=perm,
-                                          packing=pk)
+                                          packing=pk, lumen=lm)
         iters.append(it)
         traces.append(norms)
     if positions is not None:

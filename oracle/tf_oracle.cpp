@@ -1310,4 +1310,93 @@ void tfo_packing_terms(int n_pairs, const int32_t* pairs, const double* x, const
     }
 }
 
+
+// Lumen (Lumen.cpp) over triangles tri[3t .. 3t+2] (the apical nodes 3, 4, 5 of each lumen
+// element, Lumen::Lumen, Lumen.cpp:11-68): Lumen::calculateCurrentVolume (:120-148) sums
+// (1/6) (x3 x x1) . x2 per triangle (xCap_k x = x_k x x, Lumen::updateMatrices :92-118).
+double tfo_lumen_volume(int n_tri, const int32_t* tri, const double* x) {
+    double vol = 0.0;
+    for (int t = 0; t < n_tri; ++t) {
+        const double* a = x + (size_t)tri[3 * t] * 3;
+        const double* b = x + (size_t)tri[3 * t + 1] * 3;
+        const double* c = x + (size_t)tri[3 * t + 2] * 3;
+        const double cx[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
+        vol += 1.0 / 6.0 * (cx[0] * b[0] + cx[1] * b[1] + cx[2] * b[2]);
+    }
+    return vol;
+}
+
+// Lumen::calculateResiduals (Lumen.cpp:150-192), calculateJacobian (:218-301) and
+// writeLumenJacobianToSystemJacobian (:303-329) at positions x with ideal volume V0:
+// rV = (V - V0) / V0; per triangle g1 = x2 x x3, g2 = x3 x x1, g3 = x1 x x2 (fixed components
+// zeroed); forces[3 node + j] += -bulk rV / (6 V0) g_k[j] on free DoFs; K (3N x 3N, the
+// reference's storage) += bulk / (36 V0^2) G G^T with G the nodal sum of the g_k, and per
+// triangle and corner pair i != j the block (node_i, node_j)[m][k] -= s[k][m] of
+// s = -/+ bulk rV / (6 V0) xCap (the reference's table: (0,1) -xCap3, (0,2) +xCap2, (1,0) +xCap3,
+// (1,2) -xCap1, (2,0) -xCap2, (2,1) +xCap1); rows and columns of fixed DoFs are left out.
+void tfo_lumen_terms(int n_nodes, int n_tri, const int32_t* tri, const double* x, const uint8_t* fixed,
+                     double bulk, double ideal, double* forces, double* K) {
+    const size_t n = (size_t)n_nodes * 3;
+    const double vol = tfo_lumen_volume(n_tri, tri, x);
+    const double rV = (vol - ideal) / ideal;
+    const double rv6 = rV / 6.0 / ideal;
+    std::vector<double> G(n, 0.0);
+    auto cross = [](const double* u, const double* v, double* o) {
+        o[0] = u[1] * v[2] - u[2] * v[1];
+        o[1] = u[2] * v[0] - u[0] * v[2];
+        o[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    for (int t = 0; t < n_tri; ++t) {
+        const double* xs[3] = {x + (size_t)tri[3 * t] * 3, x + (size_t)tri[3 * t + 1] * 3, x + (size_t)tri[3 * t + 2] * 3};
+        double g[3][3];
+        cross(xs[1], xs[2], g[0]);
+        cross(xs[2], xs[0], g[1]);
+        cross(xs[0], xs[1], g[2]);
+        for (int i = 0; i < 3; ++i) {
+            const int node = tri[3 * t + i];
+            for (int j = 0; j < 3; ++j) {
+                if (!fixed[(size_t)node * 3 + j]) {
+                    forces[(size_t)node * 3 + j] += -1.0 * bulk * rv6 * g[i][j];
+                } else {
+                    g[i][j] = 0.0;
+                }
+                G[(size_t)node * 3 + j] += g[i][j];
+            }
+        }
+    }
+    const double c1 = bulk / ideal / ideal / 36.0, c2 = bulk * rV / 6.0 / ideal;
+    for (size_t r = 0; r < n; ++r) {
+        if (fixed[r] || G[r] == 0.0) continue;
+        for (size_t c = 0; c < n; ++c)
+            if (!fixed[c]) K[r * n + c] += c1 * G[r] * G[c];
+    }
+    for (int t = 0; t < n_tri; ++t) {
+        double cap[3][9];
+        for (int k = 0; k < 3; ++k) {
+            const double* p = x + (size_t)tri[3 * t + k] * 3;
+            const double m[9] = {0.0, -p[2], p[1], p[2], 0.0, -p[0], -p[1], p[0], 0.0};
+            std::memcpy(cap[k], m, sizeof(m));
+        }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                if (i == j) continue;
+                int which = 0;
+                double sgn = 0.0;
+                if (i == 0 && j == 1) { which = 2; sgn = -1.0; }
+                if (i == 0 && j == 2) { which = 1; sgn = 1.0; }
+                if (i == 1 && j == 0) { which = 2; sgn = 1.0; }
+                if (i == 1 && j == 2) { which = 0; sgn = -1.0; }
+                if (i == 2 && j == 0) { which = 1; sgn = -1.0; }
+                if (i == 2 && j == 1) { which = 0; sgn = 1.0; }
+                const int ni = tri[3 * t + i], nj = tri[3 * t + j];
+                for (int k = 0; k < 3; ++k)
+                    for (int m = 0; m < 3; ++m) {
+                        const size_t R = (size_t)ni * 3 + m, C = (size_t)nj * 3 + k;
+                        if (fixed[R] || fixed[C]) continue;
+                        K[R * n + C] -= sgn * c2 * cap[which][k * 3 + m];
+                    }
+            }
+    }
+}
+
 }  // extern "C"

@@ -161,6 +161,13 @@ void tfo_node_masses(int n_nodes, int n_elems, const int32_t* conn, const double
 void tfo_packing_terms(int n_pairs, const int32_t* pairs, const double* x, const double* mass, double thr,
                        double* forces, double* dfdx);
 
+/* Lumen (Lumen.cpp): the enclosed volume of the triangles tri[3t..3t+2] (apical nodes of the
+ * lumen elements), and at positions x with ideal volume `ideal` the pressure forces (added to
+ * forces[3N], free DoFs) and the Jacobian (added to the dense reference-storage K[3N][3N]). */
+double tfo_lumen_volume(int n_tri, const int32_t* tri, const double* x);
+void tfo_lumen_terms(int n_nodes, int n_tri, const int32_t* tri, const double* x, const uint8_t* fixed,
+                     double bulk, double ideal, double* forces, double* K);
+
 #ifdef __cplusplus
 }
 #endif

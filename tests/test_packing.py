@@ -174,3 +174,29 @@ def test_node_masses_sum_to_the_grown_volume():
     det = np.linalg.det(fg.reshape(-1, 3, 3))
     assert np.allclose(det, det[0])
     assert mass.sum() == pytest.approx(2 * 18.0 * 10.0 * 4.0 * det[0], rel=1e-13)
+
+
+def test_lumen_jacobian_is_the_derivative_of_the_lumen_forces():
+    """The oracle's restatement of Lumen::calculateJacobian (with the rank-one term) is minus the
+    derivative of its Lumen::calculateResiduals forces and symmetric (central differences,
+    h = 1e-6, 1e-7 relative)."""
+    t = mesh.small_rectangle(nx=6, ny=4)
+    tri = O.lumen_triangles(t, np.nonzero(t.exposed & 1)[0])
+    rng = np.random.default_rng(1)
+    x = t.x + rng.normal(0, 0.1, t.x.shape)
+    ideal = 0.97 * O.lumen_volume(t, t.x, tri)
+    _, K = O.lumen_terms(t, x, tri, 1000.0, ideal)
+    n = 3 * t.n_nodes
+    free = t.fixed.reshape(-1) == 0
+    h = 1e-6
+    J = np.zeros((n, n))
+    for c in range(n):
+        xp, xm = x.copy().reshape(-1), x.copy().reshape(-1)
+        xp[c] += h
+        xm[c] -= h
+        fp, _ = O.lumen_terms(t, xp.reshape(-1, 3), tri, 1000.0, ideal)
+        fm, _ = O.lumen_terms(t, xm.reshape(-1, 3), tri, 1000.0, ideal)
+        J[:, c] = -(fp.reshape(-1) - fm.reshape(-1)) / (2 * h)
+    J *= np.outer(free, free)
+    assert np.abs(K - J).max() <= 1e-7 * np.abs(J).max()
+    assert np.abs(K - K.T).max() <= 1e-14 * np.abs(K).max()

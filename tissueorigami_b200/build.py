@@ -15,7 +15,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtf_b200.so")
 SOURCES = ["csrc/tf_capi.cu", "csrc/tf_element.cu", "csrc/tf_krylov.cu", "csrc/tf_noalloc.cu",
            "csrc/tf_adjoint.cu", "csrc/tf_direct.cu", "csrc/tf_bench.cu", "csrc/tf_dense.cu",
-           "csrc/tf_multilevel.cu", "csrc/tf_packing.cu"]
+           "csrc/tf_multilevel.cu", "csrc/tf_packing.cu", "csrc/tf_lumen.cu"]
 LIBS = ["-lcusolver", "-lcusparse"]  # tf_direct.cu only: the sparse direct solve timed beside the Krylov solve
 HEADERS = ["csrc/tf_internal.cuh", "../include/tf_b200.h"]
 

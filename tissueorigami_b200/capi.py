@@ -53,7 +53,7 @@ EXPORTS = [
     "tf_time_kernels", "tf_last_error", "tf_solve_bsr_noalloc", "tf_batch_create",
     "tf_get_tissue_stats", "tf_get_n_tissues", "tf_adjoint_forward", "tf_adjoint_backward",
     "tf_solve_direct", "tf_get_preconditioner", "tf_get_smoother_block", "tf_measure_fp64", "tf_invert_dense", "tf_set_packing", "tf_detect_packing",
-    "tf_get_packing",
+    "tf_get_packing", "tf_set_lumen", "tf_get_lumen",
     "tf_set_grid_growth", "tf_set_time", "tf_get_time", "tf_set_external_force", "tf_newton_iteration",
     "tf_get_krylov_method",
 ]
@@ -161,6 +161,8 @@ def load(build_if_missing: bool = True):
     L.tf_set_packing.argtypes = [_P, c_int, _I]
     L.tf_detect_packing.argtypes = [_P, _D, _I]
     L.tf_get_packing.argtypes = [_P, c_int, _I, _I, _D, _D, _D]
+    L.tf_set_lumen.argtypes = [_P, c_int, _I, c_double, c_double, _D]
+    L.tf_get_lumen.argtypes = [_P, _D, _D, _D]
     L.tf_set_grid_growth.argtypes = [_P, c_int, ctypes.POINTER(GridGrowth), c_int, _D, _D, _I]
     L.tf_set_time.argtypes = [_P, c_double]
     L.tf_set_external_force.argtypes = [_P, _D]

@@ -126,6 +126,12 @@ struct tf_ctx {
     int64_t bc_n_unit = 0;
     std::vector<int32_t> bc_tissue_agg0;
     DevBuf bc_tissue_agg0_d, bc_agg_ptr_d, bc_agg_nodes_d, bc_agg_tissue_d, bc_base_d, bc_unit_d, bc_order_d, bc_info_d;
+    // lumen (tf_set_lumen): triangles, ideal volume, the rank-one term's vector and solve scratch
+    bool lm_on = false, reuse_precond = false;
+    int lm_n_tri = 0;
+    double lm_bulk = 0.0, lm_v_init = 0.0, lm_rate = 0.0, lm_ideal = 0.0;
+    DevBuf lm_tri_d, lm_state_d, lm_part_d, lm_G_d, lm_y_d, lm_z_d, lm_gsave_d, lm_dot_part_d, lm_dots_d;
+    double* h_lm_dots = nullptr;  // pinned [2]
     // packing (tf_set_packing): detection per step, pairs and their blocks outside the pattern
     bool pk_on = false;
     int pk_hash_bits = 10, pk_capacity = 0, pk_pairs_n = 0;
@@ -865,6 +871,23 @@ int assemble_system(tf_ctx* ctx, double dt) {
         TF_CK(launch_packing_terms(pt, ctx->stream));
         ctx->launches += 1;
     }
+    if (ctx->lm_on) {
+        LumenArgs la;
+        la.n_nodes = ctx->N;
+        la.n_tri = ctx->lm_n_tri;
+        la.elems = dptr<ElemRecord>(ctx->elems);
+        la.tri_elem = dptr<int32_t>(ctx->lm_tri_d);
+        la.x = dptr<double>(ctx->uk);
+        la.fixmask = dptr<uint8_t>(ctx->fixmask);
+        la.bulk = ctx->lm_bulk;
+        la.state = dptr<LumenState>(ctx->lm_state_d);
+        la.part = dptr<double>(ctx->lm_part_d);
+        la.g = dptr<double>(ctx->g);
+        la.G = dptr<double>(ctx->lm_G_d);
+        la.vals = dptr<double>(ctx->vals);
+        TF_CK(launch_lumen_terms(la, ctx->stream));
+        ctx->launches += 3;
+    }
     return TF_OK;
 }
 
@@ -1113,6 +1136,7 @@ int coarse_space_upload(tf_ctx* ctx, const std::vector<int32_t>& agg_ptr, const 
 
 int build_batch_coarse(tf_ctx* ctx);
 int build_ml(tf_ctx* ctx);
+int newton_solve(tf_ctx* ctx);
 
 int build_coarse(tf_ctx* ctx) {
     ctx->coarse_dirty = false;
@@ -1630,6 +1654,9 @@ int krylov_solve(tf_ctx* ctx) {
         if (ctx->params.precond == TF_PRECOND_TWO_LEVEL || ctx->params.precond == TF_PRECOND_MULTILEVEL) {
             if (ctx->ml_active && (ctx->plan_ncta.empty() || ctx->plan_ncta[0] != ctx->ml_nct))
                 ctx->coarse_dirty = true;  // the CTA split changed: lay the partial slots out again
+        }
+        if ((ctx->params.precond == TF_PRECOND_TWO_LEVEL || ctx->params.precond == TF_PRECOND_MULTILEVEL) &&
+            !ctx->reuse_precond) {
             if (ctx->coarse_dirty) {
                 const int crc = build_coarse(ctx);
                 if (crc != TF_OK) return crc;
@@ -1872,7 +1899,7 @@ int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
         int rc = assemble_system(ctx, dt);
         if (rc != TF_OK) return rc;
         TF_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-        rc = krylov_solve(ctx);
+        rc = newton_solve(ctx);
         if (rc != TF_OK) return rc;
         KrylovWork w = make_work(ctx);
         if (persistent) {
@@ -1976,6 +2003,45 @@ int call_end(tf_ctx* ctx, tf_step_stats* st) {
 // The growth prologue of a step at the context's simulation time: the grid-based functions active
 // then (InitialTime <= t < FinalTime, Simulation.cpp:9041) give a per-element increment, applied
 // after the uniform one; then the growth update and the exposed areas.
+// The Newton system's solve: J du = g, and with a lumen (J + a G G^T) du = g by Sherman-Morrison
+// from two solves with the sparse J: y = J^-1 g, z = J^-1 G, du = y - a (G.y) / (1 + a G.z) z,
+// a = bulk / (36 V0^2) (the rank-one term of Lumen::calculateJacobian couples every lumen node,
+// so it stays out of the sparse J). The second solve reuses the first one's preconditioner; the
+// scalars left for the Newton loop carry both solves' iterations and the worse status.
+int newton_solve(tf_ctx* ctx) {
+    int rc = krylov_solve(ctx);
+    if (rc != TF_OK || !ctx->lm_on) return rc;
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    const KrylovScalars first = ctx->h_tsc[0];
+    TF_CK(cudaMemcpyAsync(ctx->lm_y_d.p, ctx->du.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->lm_gsave_d.p, ctx->g.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->g.p, ctx->lm_G_d.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->reuse_precond = true;
+    rc = krylov_solve(ctx);
+    ctx->reuse_precond = false;
+    if (rc != TF_OK) return rc;
+    TF_CK(cudaMemcpyAsync(ctx->lm_z_d.p, ctx->du.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    TF_CK(launch_dot2(3 * ctx->N, dptr<double>(ctx->lm_G_d), dptr<double>(ctx->lm_y_d), dptr<double>(ctx->lm_z_d),
+                      dptr<double>(ctx->lm_dot_part_d), dptr<double>(ctx->lm_dots_d), ctx->stream));
+    ctx->launches += 2;
+    TF_CK(cudaMemcpyAsync(ctx->h_lm_dots, ctx->lm_dots_d.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    TF_CK(cudaStreamSynchronize(ctx->stream));
+    const double a = ctx->lm_bulk / (36.0 * ctx->lm_ideal * ctx->lm_ideal);
+    const double coef = a * ctx->h_lm_dots[0] / (1.0 + a * ctx->h_lm_dots[1]);
+    TF_CK(cudaMemcpyAsync(ctx->du.p, ctx->lm_y_d.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    TF_CK(launch_axpy(3 * ctx->N, -coef, dptr<double>(ctx->lm_z_d), dptr<double>(ctx->du), ctx->stream));
+    TF_CK(cudaMemcpyAsync(ctx->g.p, ctx->lm_gsave_d.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->launches += 1;
+    KrylovScalars& sc = ctx->h_tsc[0];
+    const KrylovScalars second = sc;
+    sc = first;
+    sc.iter = first.iter + second.iter;
+    if (second.status != KS_CONVERGED) sc.status = second.status;
+    *ctx->h_sc = sc;
+    if (!std::isfinite(coef)) return set_error(ctx, TF_ERR_STATE, "lumen: 1 + a G.z vanished");
+    return TF_OK;
+}
+
 int prologue(tf_ctx* ctx, double dt) {
     const double* grid_inc = nullptr;
     GridStep gs;
@@ -2006,6 +2072,11 @@ int prologue(tf_ctx* ctx, double dt) {
                                    dptr<uint8_t>(ctx->exposed), dptr<uint8_t>(ctx->peripodial),
                                    dptr<double>(ctx->visc_surface), ctx->stream));
     ctx->launches += 2;
+    if (ctx->lm_on) {  // Lumen::growLumen(currSimTimeSec + dt) (Simulation.cpp:6019, Lumen.cpp:331-334)
+        ctx->lm_ideal = ctx->lm_v_init * std::exp(ctx->lm_rate * (ctx->sim_time + dt));
+        TF_CK(launch_lumen_set_ideal(dptr<LumenState>(ctx->lm_state_d), ctx->lm_ideal, ctx->stream));
+        ctx->launches += 1;
+    }
     if (ctx->pk_on) return packing_detect(ctx, dptr<double>(ctx->un));  // after the growth (Simulation.cpp:6065-6076)
     return TF_OK;
 }
@@ -2321,6 +2392,10 @@ void tf_destroy(tf_ctx* ctx) {
     DevBuf* bcb[] = {&ctx->bc_tissue_agg0_d, &ctx->bc_agg_ptr_d, &ctx->bc_agg_nodes_d, &ctx->bc_agg_tissue_d, &ctx->bc_base_d, &ctx->bc_unit_d,
                      &ctx->bc_order_d, &ctx->bc_info_d};
     for (DevBuf* b : bcb) dfree(*b);
+    DevBuf* lmb[] = {&ctx->lm_tri_d, &ctx->lm_state_d, &ctx->lm_part_d, &ctx->lm_G_d, &ctx->lm_y_d, &ctx->lm_z_d,
+                     &ctx->lm_gsave_d, &ctx->lm_dot_part_d, &ctx->lm_dots_d};
+    for (DevBuf* b : lmb) dfree(*b);
+    if (ctx->h_lm_dots) cudaFreeHost(ctx->h_lm_dots);
     DevBuf* pkb[] = {&ctx->pk_place_d, &ctx->pk_v0_d, &ctx->pk_mass_d, &ctx->pk_prm_d, &ctx->pk_bucket_cnt_d,
                      &ctx->pk_bucket_start_d, &ctx->pk_bucket_nodes_d, &ctx->pk_node_cnt_d, &ctx->pk_node_start_d,
                      &ctx->pk_scan_d, &ctx->pk_pairs_d, &ctx->pk_ptr_d, &ctx->pk_col_d, &ctx->pk_blk_d, &ctx->pk_vals_d,
@@ -2397,6 +2472,7 @@ int tf_set_boundary(tf_ctx* ctx, const uint8_t* fixed, const double* ext_visc,
     for (int32_t m : ms)
         if (dm[m] != m) return set_error(ctx, TF_ERR_ARGUMENT, "a master DoF is itself a slave");
     if (n_pairs > 0 && ctx->pk_on) return set_error(ctx, TF_ERR_UNSUPPORTED, "slave-master pairs with packing");
+    if (n_pairs > 0 && ctx->lm_on) return set_error(ctx, TF_ERR_UNSUPPORTED, "slave-master pairs with a lumen");
     const bool changed = dm != ctx->dofmap;
     ctx->dofmap = dm;
     ctx->slave = sl;
@@ -2416,6 +2492,65 @@ int tf_set_external_force(tf_ctx* ctx, const double* f) {
     TF_CK(dalloc(ctx->ext_force, sizeof(double) * 3 * (size_t)ctx->N));
     TF_CK(cudaMemcpy(ctx->ext_force.p, f, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyHostToDevice));
     ctx->has_ext_force = true;
+    return TF_OK;
+}
+
+int tf_set_lumen(tf_ctx* ctx, int32_t n_elems, const int32_t* elems, double bulk_modulus, double growth_fold,
+                 const double* x) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (n_elems <= 0) {
+        ctx->lm_on = false;
+        return TF_OK;
+    }
+    if (!elems || !x || !(bulk_modulus >= 0.0)) return TF_ERR_ARGUMENT;
+    if (ctx->T != 1 || !ctx->slave.empty() || !use_persistent(ctx))
+        return set_error(ctx, TF_ERR_UNSUPPORTED, "lumen: single tissue, no slave-master pairs, persistent solve");
+    // Lumen::calculateCurrentVolume at the given positions: the ideal volume of the constructor
+    double vol = 0.0;
+    for (int k = 0; k < n_elems; ++k) {
+        const int e = elems[k];
+        if (e < 0 || e >= ctx->E) return TF_ERR_ARGUMENT;
+        const int32_t* c = ctx->conn.data() + (size_t)e * 6;
+        const double* x1 = x + (size_t)c[3] * 3;
+        const double* x2 = x + (size_t)c[4] * 3;
+        const double* x3 = x + (size_t)c[5] * 3;
+        const double cx[3] = {x3[1] * x1[2] - x3[2] * x1[1], x3[2] * x1[0] - x3[0] * x1[2], x3[0] * x1[1] - x3[1] * x1[0]};
+        vol += 1.0 / 6.0 * (cx[0] * x2[0] + cx[1] * x2[1] + cx[2] * x2[2]);
+    }
+    if (!(std::fabs(vol) > 0.0)) return set_error(ctx, TF_ERR_ARGUMENT, "lumen: the triangles enclose no volume");
+    const size_t bytes = sizeof(double) * 3 * (size_t)ctx->N;
+    TF_CK(dalloc(ctx->lm_tri_d, sizeof(int32_t) * (size_t)n_elems));
+    TF_CK(cudaMemcpy(ctx->lm_tri_d.p, elems, sizeof(int32_t) * (size_t)n_elems, cudaMemcpyHostToDevice));
+    TF_CK(dalloc(ctx->lm_state_d, sizeof(LumenState)));
+    TF_CK(dalloc(ctx->lm_part_d, sizeof(double) * (size_t)lumen_partials(n_elems)));
+    TF_CK(dalloc(ctx->lm_G_d, bytes));
+    TF_CK(dalloc(ctx->lm_y_d, bytes));
+    TF_CK(dalloc(ctx->lm_z_d, bytes));
+    TF_CK(dalloc(ctx->lm_gsave_d, bytes));
+    TF_CK(dalloc(ctx->lm_dot_part_d, sizeof(double) * (size_t)dot2_partials()));
+    TF_CK(dalloc(ctx->lm_dots_d, 2 * sizeof(double)));
+    if (!ctx->h_lm_dots) TF_CK(cudaMallocHost(&ctx->h_lm_dots, 2 * sizeof(double)));
+    ctx->lm_n_tri = n_elems;
+    ctx->lm_bulk = bulk_modulus;
+    ctx->lm_v_init = vol;
+    ctx->lm_rate = growth_fold > 0.0 ? std::log(growth_fold) / 3600.0 / 24.0 : 0.0;  // Lumen.cpp:19-22
+    ctx->lm_ideal = vol;
+    LumenState st{vol, vol};
+    TF_CK(cudaMemcpy(ctx->lm_state_d.p, &st, sizeof(st), cudaMemcpyHostToDevice));
+    ctx->lm_on = true;
+    return TF_OK;
+}
+
+int tf_get_lumen(tf_ctx* ctx, double* volume, double* ideal_volume, double* G) {
+    int rc = check_ctx(ctx);
+    if (rc != TF_OK) return rc;
+    if (!ctx->lm_on) return set_error(ctx, TF_ERR_STATE, "no lumen (tf_set_lumen)");
+    LumenState st;
+    TF_CK(cudaMemcpy(&st, ctx->lm_state_d.p, sizeof(st), cudaMemcpyDeviceToHost));
+    if (volume) *volume = st.volume;
+    if (ideal_volume) *ideal_volume = st.ideal;
+    if (G) TF_CK(cudaMemcpy(G, ctx->lm_G_d.p, sizeof(double) * 3 * (size_t)ctx->N, cudaMemcpyDeviceToHost));
     return TF_OK;
 }
 
@@ -2541,7 +2676,7 @@ int tf_newton_iteration(tf_ctx* ctx, const double* uk, const double* un, double 
     ctx->cg_iters = 0;
     rc = assemble_system(ctx, dt);
     if (rc != TF_OK) return rc;
-    rc = krylov_solve(ctx);
+    rc = newton_solve(ctx);
     if (rc != TF_OK) return rc;
     const KrylovScalars sc = *ctx->h_sc;
     if (!ctx->slave.empty()) {
@@ -3056,8 +3191,9 @@ int tf_adjoint_forward(tf_ctx* ctx, const double* x0, int32_t n_steps, double dt
     int rc = check_ctx(ctx);
     if (rc != TF_OK) return rc;
     if (!x0 || !x_final || n_steps <= 0 || checkpoint_every <= 0 || !(dt > 0)) return TF_ERR_ARGUMENT;
-    if (ctx->has_visc || !ctx->slave.empty() || ctx->T != 1 || ctx->pk_on) return set_error(ctx, TF_ERR_UNSUPPORTED,
-        "adjoint: single tissue without internal viscosity, slave-master pairs or packing");
+    if (ctx->has_visc || !ctx->slave.empty() || ctx->T != 1 || ctx->pk_on || ctx->lm_on)
+        return set_error(ctx, TF_ERR_UNSUPPORTED,
+                         "adjoint: single tissue without internal viscosity, slave-master pairs, packing or lumen");
     tf_step_stats local;
     tf_step_stats* st = stats ? stats : &local;
     rc = call_begin(ctx, st);

@@ -451,6 +451,32 @@ cudaError_t launch_packing_terms(const PackTerms& a, cudaStream_t s);
 int scan_tmp_ints(int n);
 cudaError_t launch_scan_i32(const int32_t* in, int32_t* out, int n, int32_t* tmp, cudaStream_t s);
 
+// --- lumen (tf_lumen.cu) ----------------------------------------------------------------------
+struct LumenState {
+    double volume;  // enclosed volume at the last assembly
+    double ideal;   // the step's ideal volume
+};
+struct LumenArgs {
+    int32_t n_nodes, n_tri;
+    const ElemRecord* elems;
+    const int32_t* tri_elem;  // [n_tri] the lumen elements (apical triangle: nodes 3, 4, 5)
+    const double* x;          // [N][3] Newton iterate
+    const uint8_t* fixmask;
+    double bulk;
+    LumenState* state;
+    double* part;             // lumen_partials(n_tri) doubles
+    double* g;                // residual: += the pressure forces
+    double* G;                // [3N] nodal sums of 6 dV/dx (fixed components zeroed)
+    double* vals;             // J: += the triangle-local blocks
+};
+int lumen_partials(int n_tri);
+cudaError_t launch_lumen_terms(const LumenArgs& a, cudaStream_t s);
+cudaError_t launch_lumen_set_ideal(LumenState* state, double ideal, cudaStream_t s);
+// out[0] = (a, b1), out[1] = (a, b2) over n doubles; part holds dot2_partials() doubles
+int dot2_partials();
+cudaError_t launch_dot2(int n, const double* a, const double* b1, const double* b2, double* part, double* out,
+                        cudaStream_t s);
+
 // --- dense inverses of the coarse operators (tf_dense.cu) -------------------------------------
 // In-place Gauss-Jordan inverse with partial pivoting of column-major matrices (a row-major
 // matrix in, its row-major inverse out). Batched: matrix t of order order[t] at a + base[t], leading

@@ -55,6 +55,24 @@ class NewtonRaphsonSolver:
             s.set_packing(t.node_placement)
         return s
 
+    # -- lumen (Lumen.cpp) ------------------------------------------------------------------
+    def set_lumen(self, elems=None, bulk_modulus: float = 0.0, growth_fold: float = 0.0, x=None):
+        """Lumen on the apical triangles of `elems` (ideal volume: the volume at positions x), or
+        none with elems None."""
+        if elems is None or len(elems) == 0:
+            capi.check(self._L.tf_set_lumen(self._h, 0, None, 0.0, 0.0, None), "tf_set_lumen", self._h)
+            return
+        e = np.ascontiguousarray(elems, dtype=np.int32)
+        capi.check(self._L.tf_set_lumen(self._h, e.size, capi.iptr(e), float(bulk_modulus), float(growth_fold),
+                                        capi.dptr(_f64(x).reshape(-1))), "tf_set_lumen", self._h)
+
+    def lumen(self):
+        """(enclosed volume at the last assembly, ideal volume, G [N,3])."""
+        v, v0 = ctypes.c_double(), ctypes.c_double()
+        G = np.zeros((self.n_nodes, 3))
+        capi.check(self._L.tf_get_lumen(self._h, ctypes.byref(v), ctypes.byref(v0), capi.dptr(G)), "tf_get_lumen", self._h)
+        return v.value, v0.value, G
+
     # -- packing (Simulation::detectPacingNodes, calculatePackingForcesImplicit3D / Jacobian3D) --
     def set_packing(self, node_placement=None):
         """Turn packing on with node_placement[N] (0 basal, 1 apical, 2 other), or off with None."""
