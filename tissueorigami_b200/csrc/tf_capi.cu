@@ -149,7 +149,7 @@ struct tf_ctx {
     std::vector<int32_t> h_slot_agg, h_agg_slot_ptr;  // host copies of the last coarse_space_upload's slots
     DevBuf ml_leaf_ptr_d, ml_leaf_nodes_d, ml_cen_d, ml_w_d, ml_top_d, ml_top_work, ml_info_d, ml_leaf_m_d, ml_part_d,
         ml_pstart_d, ml_first_cta_d, ml_slot_a_d, ml_out_ptr_d, ml_out_slots_d, ml_out_set_d, ml_out_col_d, ml_out_dst_d,
-        ml_pairs_d;
+        ml_pairs_d, ml_pos_leaf_d;
 
     // multicolour block ILU(0) (precond == TF_PRECOND_ILU0)
     std::vector<int32_t> ilu_colour_ptr;
@@ -789,6 +789,7 @@ BatchPlan make_plan(tf_ctx* c) {
     p.ml_part = dptr<double>(c->ml_part_d);
     p.ml_pstart = dptr<int32_t>(c->ml_pstart_d);
     p.ml_first_cta = dptr<int32_t>(c->ml_first_cta_d);
+    p.ml_pos_leaf = dptr<int32_t>(c->ml_pos_leaf_d);
     p.n_tissues = c->T;
     p.n_cta = (int32_t)c->plan_list_ptr.size() - 1;
     p.cta_list_ptr = dptr<int32_t>(c->plan_list_ptr_d);
@@ -1468,6 +1469,10 @@ int build_ml(tf_ctx* ctx) {
         return e;
     };
     const int n6 = 6 * n_top;
+    std::vector<int32_t> pos_leaf(N);
+    for (int a = 0; a < n_leaf; ++a)
+        for (int k = leaf_ptr[a]; k < leaf_ptr[a + 1]; ++k) pos_leaf[k] = a;
+    TF_CK(up(ctx->ml_pos_leaf_d, pos_leaf.data(), sizeof(int32_t) * pos_leaf.size()));
     TF_CK(up(ctx->ml_leaf_ptr_d, leaf_ptr.data(), sizeof(int32_t) * leaf_ptr.size()));
     TF_CK(up(ctx->ml_leaf_nodes_d, leaf_nodes.data(), sizeof(int32_t) * leaf_nodes.size()));
     TF_CK(up(ctx->ml_cen_d, cen.data(), sizeof(double) * cen.size()));
@@ -2404,7 +2409,7 @@ void tf_destroy(tf_ctx* ctx) {
     DevBuf* mlb[] = {&ctx->ml_leaf_ptr_d, &ctx->ml_leaf_nodes_d, &ctx->ml_cen_d, &ctx->ml_w_d, &ctx->ml_top_d,
                      &ctx->ml_top_work, &ctx->ml_info_d, &ctx->ml_leaf_m_d, &ctx->ml_part_d, &ctx->ml_pstart_d,
                      &ctx->ml_first_cta_d, &ctx->ml_slot_a_d, &ctx->ml_out_ptr_d, &ctx->ml_out_slots_d,
-                     &ctx->ml_out_set_d, &ctx->ml_out_col_d, &ctx->ml_out_dst_d, &ctx->ml_pairs_d};
+                     &ctx->ml_out_set_d, &ctx->ml_out_col_d, &ctx->ml_out_dst_d, &ctx->ml_pairs_d, &ctx->ml_pos_leaf_d};
     for (DevBuf* b : mlb) dfree(*b);
     if (ctx->h_coarse_info) cudaFreeHost(ctx->h_coarse_info);
     if (ctx->h_active) cudaFreeHost(ctx->h_active);

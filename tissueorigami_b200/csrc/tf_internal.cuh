@@ -196,6 +196,7 @@ struct BatchPlan {
     double* ml_part;             // [partials][6] per-CTA partial moments of the sets of levels >= 2
     const int32_t* ml_pstart;    // [sets+1] first partial of each set (levels >= 2)
     const int32_t* ml_first_cta; // [sets] first CTA of the group whose leaves overlap the set
+    const int32_t* ml_pos_leaf;  // [N] the leaf of each position of the leaf node list (agg_nodes)
 };
 
 constexpr int kMaxAggPerCta = 4;

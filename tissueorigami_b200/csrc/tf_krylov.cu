@@ -898,12 +898,25 @@ __device__ __forceinline__ void ml_or_batch_range(const BatchPlan& plan, int t, 
 // numbering in C and D. Every sum has a fixed order.
 template <int PH>
 __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, int l0, int l1, double alpha,
-                           double beta, double omega, GridBarrier* bar, int nct, double* cs) {
+                           double beta, double omega, GridBarrier* bar, int nct, double* cs, double* dots) {
     double* vin = phase_in<PH>(w);
     double* out = phase_out<PH>(w);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int G = plan.group, L = plan.ml_levels;
-    // A
+    const int kb = plan.agg_ptr[l0], ke = l1 > l0 ? plan.agg_ptr[l1] : kb;  // the CTA's span of the leaf node list
+    // A1 (node blocks): the smoother on every node of the CTA's leaves, one node per thread
+    if (G == 1)
+        for (int k = kb + threadIdx.x; k < ke; k += blockDim.x) {
+            const int n = plan.agg_nodes[k];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                vin[d] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+            }
+            apply_dinv(w.dinv, n, vin, out);
+        }
+    __syncthreads();  // vin of the CTA's nodes, written by other warps
+    // A2: the leaf moments, one warp per leaf (column blocks: the smoother too, per leaf)
     for (int a = l0 + warp; a < l1; a += nw) {
         const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -934,16 +947,9 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
         }
         for (int k = k0 + lane; G == 1 && k < k1; k += 32) {
             const int n = plan.agg_nodes[k];
-            double u[3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int d = n * 3 + i;
-                u[i] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
-                vin[d] = u[i];
-            }
-            apply_dinv(w.dinv, n, vin, out);
             const int mk = plan.node_mask[n];
-            const double u0 = (mk & 1) ? u[0] : 0.0, u1 = (mk & 2) ? u[1] : 0.0, u2 = (mk & 4) ? u[2] : 0.0;
+            const double u0 = (mk & 1) ? vin[n * 3] : 0.0, u1 = (mk & 2) ? vin[n * 3 + 1] : 0.0,
+                         u2 = (mk & 4) ? vin[n * 3 + 2] : 0.0;
             const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
             acc[0] += u0;
             acc[1] += u1;
@@ -1046,9 +1052,9 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
         }
     }
     __syncthreads();
-    // D
-    for (int a = l0 + warp; a < l1; a += nw) {
-        const double* ma = plan.ml_leaf_m + 6 * (size_t)a;
+    // D1: each leaf's motion, one thread per leaf, over the leaf's moment in ml_leaf_m
+    for (int a = l0 + (int)threadIdx.x; a < l1; a += blockDim.x) {
+        double* ma = plan.ml_leaf_m + 6 * (size_t)a;
         const double* Wa = plan.ml_w + 36 * (size_t)a;
         double m[6], y[6];
 #pragma unroll
@@ -1076,27 +1082,49 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
             y[5] += yS[5];
             jb += s1 - s0 + 1;
         }
-        const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
-        for (int k = k0 + lane; k < k1; k += 32) {
-            const int n = plan.agg_nodes[k];
-            const int mk = plan.node_mask[n];
-            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
-            if (mk & 1) out[n * 3] += y[0] + y[4] * dz - y[5] * dy;
-            if (mk & 2) out[n * 3 + 1] += y[1] + y[5] * dx - y[3] * dz;
-            if (mk & 4) out[n * 3 + 2] += y[2] + y[3] * dy - y[4] * dx;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) ma[q] = y[q];  // the moment is not needed again: the motion replaces it
+    }
+    __syncthreads();
+    // D2: the prolongation, one node per thread (the leaf of each list position in ml_pos_leaf);
+    // conjugate gradients' (r, z) and (r, r) over the same nodes on the way
+    double rz = 0.0, rr = 0.0;
+    for (int k = kb + threadIdx.x; k < ke; k += blockDim.x) {
+        const int n = plan.agg_nodes[k];
+        const double* y = plan.ml_leaf_m + 6 * (size_t)plan.ml_pos_leaf[k];
+        const int mk = plan.node_mask[n];
+        const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
+        double z0 = out[n * 3], z1 = out[n * 3 + 1], z2 = out[n * 3 + 2];
+        if (mk & 1) z0 += y[0] + y[4] * dz - y[5] * dy;
+        if (mk & 2) z1 += y[1] + y[5] * dx - y[3] * dz;
+        if (mk & 4) z2 += y[2] + y[3] * dy - y[4] * dx;
+        out[n * 3] = z0;
+        out[n * 3 + 1] = z1;
+        out[n * 3 + 2] = z2;
+        if (PH == 2) {
+            const double q0 = w.r[n * 3], q1 = w.r[n * 3 + 1], q2 = w.r[n * 3 + 2];
+            rz += q0 * z0 + q1 * z1 + q2 * z2;
+            rr += q0 * q0 + q1 * q1 + q2 * q2;
         }
+    }
+    if (dots) {
+        dots[0] = rz;
+        dots[1] = rr;
     }
     return true;
 }
 
 template <int PH>
+// dots (multilevel space, PH 2 only): this CTA's partial (r, z) and (r, r) over its leaves' nodes,
+// formed on the way (the caller then skips precond_rows_dots)
 __device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, int t, int lc, int r0, int r1, int ba0,
                                     int ba1, double alpha, double beta, double omega, GridBarrier* bar, int nct,
-                                    double* red, double* ys, double* cs, const float* cinv_s, const double* Ms) {
+                                    double* red, double* ys, double* cs, const float* cinv_s, const double* Ms,
+                                    double* dots = nullptr) {
     if (plan.agg_per_cta > 0)
         return precond_phase<PH>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms);
     if (plan.batch_coarse) return precond_batch<PH>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs);
-    if (plan.ml) return precond_ml<PH>(w, plan, lc, ba0, ba1, alpha, beta, omega, bar, nct, cs);
+    if (plan.ml) return precond_ml<PH>(w, plan, lc, ba0, ba1, alpha, beta, omega, bar, nct, cs, dots);
     double* vin = phase_in<PH>(w);
     double* out = phase_out<PH>(w);
     if (plan.group > 1) {
@@ -1379,10 +1407,11 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
     int it = 0;
     int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
     if (status == KS_RUNNING) {  // z = M^-1 r, (r, z)
-        if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, 0.0, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms))
+        double dd[2] = {0.0, 0.0};
+        if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, 0.0, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms, dd))
             return false;
-        double d0 = 0.0, d1 = 0.0;
-        precond_rows_dots(w, plan, r0, r1, ba0, ba1, d0, d1);
+        double d0 = dd[0], d1 = dd[1];
+        if (!plan.ml) precond_rows_dots(w, plan, r0, r1, ba0, ba1, d0, d1);
         double v2[2] = {d0, d1};
         write_partials<2>(v2, part[pb], lc, smem);
         if (!group_barrier(bar, nct, w.dflags)) return false;
@@ -1392,14 +1421,20 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         if (!isfinite(rz)) status = KS_NONFINITE;
         else if (!(rz > 0.0)) indefinite = true;
     }
+    bool pending = false;  // x += alpha p of the last iteration, applied with the next p update
     while (status == KS_RUNNING && !indefinite) {
-        // p = z + beta p on the contiguous rows (z of every row is final after the last barrier)
+        // x += alpha p_old (deferred); p = z + beta p_old on the contiguous rows (z of every row is
+        // final after the last barrier)
+        const double a_old = pending ? alpha : 0.0;
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const int d = n * 3 + i;
-                w.p[d] = w.phat[d] + beta * w.p[d];
+                const double po = w.p[d];
+                if (pending) w.x[d] += a_old * po;
+                w.p[d] = w.phat[d] + beta * po;
             }
+        pending = false;
         if (!group_barrier(bar, nct, w.dflags)) return false;
         // q = J p, (p, q)
         double d0 = 0.0, d1 = 0.0;
@@ -1413,18 +1448,15 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         if (!isfinite(pq)) { status = KS_NONFINITE; break; }
         if (!(pq > 0.0)) { indefinite = true; break; }
         alpha = rz / pq;
-        // x += alpha p; r -= alpha q; z = M^-1 r; (r, z), (r, r)
-        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int d = n * 3 + i;
-                w.x[d] += alpha * w.p[d];
-            }
-        if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms))
+        pending = true;  // x += alpha p: with the next p update, or after the loop
+        // r -= alpha q; z = M^-1 r; (r, z), (r, r)
+        double dd2[2] = {0.0, 0.0};
+        if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms,
+                                    dd2))
             return false;
-        d0 = 0.0;
-        d1 = 0.0;
-        precond_rows_dots(w, plan, r0, r1, ba0, ba1, d0, d1);
+        d0 = dd2[0];
+        d1 = dd2[1];
+        if (!plan.ml) precond_rows_dots(w, plan, r0, r1, ba0, ba1, d0, d1);
         double v2[2] = {d0, d1};
         write_partials<2>(v2, part[pb], lc, smem);
         if (!group_barrier(bar, nct, w.dflags)) return false;
@@ -1444,6 +1476,10 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         beta = rz_new / rz;
         rz = rz_new;
     }
+    if (pending)  // the last iteration's x += alpha p (x and r stay consistent for a warm start)
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) w.x[n * 3 + i] += alpha * w.p[n * 3 + i];
     if (indefinite) status = KS_INDEFINITE;  // the host solves the tissue again with BiCGStab
     if (lc == 0 && threadIdx.x == 0) {
         KrylovScalars* sc = plan.scalars + t;
