@@ -869,6 +869,32 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
 // for a batch tissue with the two-level preconditioner): PH 0 p = r + beta (p - omega v),
 // phat = M^-1 p; PH 1 s = r - alpha v, shat = M^-1 s (BiCGStab); PH 2 r = r - alpha q (q in v),
 // z = M^-1 r (z in phat; conjugate gradients). Returns false when a group barrier timed out.
+// The phase's vector update and block-Jacobi smoother on the contiguous rows [r0, r1) (node
+// blocks one node per thread; column blocks one DoF per lane).
+template <int PH>
+__device__ __forceinline__ void smooth_rows(const KrylovWork& w, const BatchPlan& plan, int r0, int r1, double alpha,
+                                            double beta, double omega) {
+    double* vin = phase_in<PH>(w);
+    double* out = phase_out<PH>(w);
+    if (plan.group > 1) {
+        const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
+        const int g1 = r1 / plan.group;
+        for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
+            const bool valid = gl < gpw && gc + gl < g1;
+            group_dof_update_apply<PH>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, beta, omega, vin, out);
+        }
+        return;
+    }
+    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            vin[d] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+        }
+        apply_dinv(w.dinv, n, vin, out);
+    }
+}
+
 // The aggregates of tissue t a CTA of its group preconditions (batch two-level space), or its
 // leaves (multilevel space of a single tissue).
 __device__ __forceinline__ void ml_or_batch_range(const BatchPlan& plan, int t, int lc, int nct, int& b0, int& b1) {
@@ -897,55 +923,23 @@ __device__ __forceinline__ void ml_or_batch_range(const BatchPlan& plan, int t, 
 // Jobs (level, set) are numbered in level order and dealt to the warps round-robin, the same
 // numbering in C and D. Every sum has a fixed order.
 template <int PH>
-__device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, int l0, int l1, double alpha,
-                           double beta, double omega, GridBarrier* bar, int nct, double* cs, double* dots) {
+__device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, int l0, int l1,
+                           double alpha, double beta, double omega, GridBarrier* bar, int nct, double* cs,
+                           double* dots) {
     double* vin = phase_in<PH>(w);
     double* out = phase_out<PH>(w);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int G = plan.group, L = plan.ml_levels;
+    const int L = plan.ml_levels;
     const int kb = plan.agg_ptr[l0], ke = l1 > l0 ? plan.agg_ptr[l1] : kb;  // the CTA's span of the leaf node list
-    // A1 (node blocks): the smoother on every node of the CTA's leaves, one node per thread
-    if (G == 1)
-        for (int k = kb + threadIdx.x; k < ke; k += blockDim.x) {
-            const int n = plan.agg_nodes[k];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int d = n * 3 + i;
-                vin[d] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
-            }
-            apply_dinv(w.dinv, n, vin, out);
-        }
-    __syncthreads();  // vin of the CTA's nodes, written by other warps
-    // A2: the leaf moments, one warp per leaf (column blocks: the smoother too, per leaf)
+    // A1: the smoother on the CTA's contiguous rows (coalesced); the leaves' nodes lie in other
+    // CTAs' rows as well, hence the group barrier before their moments
+    smooth_rows<PH>(w, plan, r0, r1, alpha, beta, omega);
+    if (!group_barrier(bar, nct, w.dflags)) return false;
+    // A2: the leaf moments from the updated vector, one warp per leaf
     for (int a = l0 + warp; a < l1; a += nw) {
         const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (G > 1) {  // whole smoother groups, each group's nodes consecutive: one DoF per lane
-            const int n3 = 3 * G, gpw = 32 / n3, gl = lane / n3, rr = lane - gl * n3;
-            const int ng = (k1 - k0) / G;
-            for (int q = 0; q < ng; q += gpw) {
-                const bool valid = gl < gpw && q + gl < ng;
-                const int g = plan.agg_nodes[k0 + (valid ? q + gl : q) * G] / G;
-                const double u = group_dof_update_apply<PH>(w, g, rr, n3, valid, alpha, beta, omega, vin, out);
-                if (valid) {
-                    const int n = g * G + rr / 3, i = rr % 3;
-                    const double ui = ((plan.node_mask[n] >> i) & 1) ? u : 0.0;
-                    const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
-                    acc[i] += ui;
-                    if (i == 0) {
-                        acc[4] += dz * ui;
-                        acc[5] -= dy * ui;
-                    } else if (i == 1) {
-                        acc[3] -= dz * ui;
-                        acc[5] += dx * ui;
-                    } else {
-                        acc[3] += dy * ui;
-                        acc[4] -= dx * ui;
-                    }
-                }
-            }
-        }
-        for (int k = k0 + lane; G == 1 && k < k1; k += 32) {
+        for (int k = k0 + lane; k < k1; k += 32) {
             const int n = plan.agg_nodes[k];
             const int mk = plan.node_mask[n];
             const double u0 = (mk & 1) ? vin[n * 3] : 0.0, u1 = (mk & 2) ? vin[n * 3 + 1] : 0.0,
@@ -1124,26 +1118,8 @@ __device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, 
     if (plan.agg_per_cta > 0)
         return precond_phase<PH>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms);
     if (plan.batch_coarse) return precond_batch<PH>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs);
-    if (plan.ml) return precond_ml<PH>(w, plan, lc, ba0, ba1, alpha, beta, omega, bar, nct, cs, dots);
-    double* vin = phase_in<PH>(w);
-    double* out = phase_out<PH>(w);
-    if (plan.group > 1) {
-        const int n3 = 3 * plan.group, gpw = 32 / n3, lane = threadIdx.x & 31, gl = lane / n3;
-        const int g1 = r1 / plan.group;
-        for (int gc = r0 / plan.group + (threadIdx.x >> 5) * gpw; gc < g1; gc += (blockDim.x >> 5) * gpw) {
-            const bool valid = gl < gpw && gc + gl < g1;
-            group_dof_update_apply<PH>(w, valid ? gc + gl : gc, lane - gl * n3, n3, valid, alpha, beta, omega, vin, out);
-        }
-        return true;
-    }
-    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const int d = n * 3 + i;
-            vin[d] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
-        }
-        apply_dinv(w.dinv, n, vin, out);
-    }
+    if (plan.ml) return precond_ml<PH>(w, plan, lc, r0, r1, ba0, ba1, alpha, beta, omega, bar, nct, cs, dots);
+    smooth_rows<PH>(w, plan, r0, r1, alpha, beta, omega);
     return true;
 }
 
@@ -1421,20 +1397,14 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         if (!isfinite(rz)) status = KS_NONFINITE;
         else if (!(rz > 0.0)) indefinite = true;
     }
-    bool pending = false;  // x += alpha p of the last iteration, applied with the next p update
     while (status == KS_RUNNING && !indefinite) {
-        // x += alpha p_old (deferred); p = z + beta p_old on the contiguous rows (z of every row is
-        // final after the last barrier)
-        const double a_old = pending ? alpha : 0.0;
+        // p = z + beta p on the contiguous rows (z of every row is final after the last barrier)
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const int d = n * 3 + i;
-                const double po = w.p[d];
-                if (pending) w.x[d] += a_old * po;
-                w.p[d] = w.phat[d] + beta * po;
+                w.p[d] = w.phat[d] + beta * w.p[d];
             }
-        pending = false;
         if (!group_barrier(bar, nct, w.dflags)) return false;
         // q = J p, (p, q)
         double d0 = 0.0, d1 = 0.0;
@@ -1448,8 +1418,14 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         if (!isfinite(pq)) { status = KS_NONFINITE; break; }
         if (!(pq > 0.0)) { indefinite = true; break; }
         alpha = rz / pq;
-        pending = true;  // x += alpha p: with the next p update, or after the loop
-        // r -= alpha q; z = M^-1 r; (r, z), (r, r)
+        // x += alpha p (p is still in L2 from the SpMV's gathers); r -= alpha q; z = M^-1 r;
+        // (r, z), (r, r)
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.x[d] += alpha * w.p[d];
+            }
         double dd2[2] = {0.0, 0.0};
         if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, alpha, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms,
                                     dd2))
@@ -1476,10 +1452,6 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         beta = rz_new / rz;
         rz = rz_new;
     }
-    if (pending)  // the last iteration's x += alpha p (x and r stay consistent for a warm start)
-        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) w.x[n * 3 + i] += alpha * w.p[n * 3 + i];
     if (indefinite) status = KS_INDEFINITE;  // the host solves the tissue again with BiCGStab
     if (lc == 0 && threadIdx.x == 0) {
         KrylovScalars* sc = plan.scalars + t;
