@@ -886,12 +886,23 @@ __device__ __forceinline__ void smooth_rows(const KrylovWork& w, const BatchPlan
         return;
     }
     for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+        // every load of the node before its first store (the vectors may alias as far as the
+        // compiler knows): one round trip to memory per node
+        double u[3], D[9];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const int d = n * 3 + i;
-            vin[d] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
+            const double rv = w.r[d], vv = w.v[d];
+            u[i] = PH == 0 ? rv + beta * (w.p[d] - omega * vv) : rv - alpha * vv;
         }
-        apply_dinv(w.dinv, n, vin, out);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) D[k] = __ldg(w.dinv + (size_t)n * 9 + k);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int d = n * 3 + i;
+            vin[d] = u[i];
+            out[d] = D[3 * i] * u[0] + D[3 * i + 1] * u[1] + D[3 * i + 2] * u[2];
+        }
     }
 }
 
@@ -1418,8 +1429,8 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         if (!isfinite(pq)) { status = KS_NONFINITE; break; }
         if (!(pq > 0.0)) { indefinite = true; break; }
         alpha = rz / pq;
-        // x += alpha p (p is still in L2 from the SpMV's gathers); r -= alpha q; z = M^-1 r;
-        // (r, z), (r, r)
+        // x += alpha p (p is still in L2 from the SpMV's gathers; a separate pass: folded into
+        // the smoother's, its live registers spill); r -= alpha q; z = M^-1 r; (r, z), (r, r)
         for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
