@@ -460,6 +460,17 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
     for (int rb = r0; rb < r1; rb += groups) {
         const int row = rb + threadIdx.x / kGroup;
         double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+        // the row's entries of the dot products' other vectors, loaded by the reducing lane ahead
+        // of the row product so that their latency overlaps it
+        double a[3] = {0.0, 0.0, 0.0}, b[3] = {0.0, 0.0, 0.0};
+        if (row < r1 && gl == 0) {
+            const double* av = KIND == 1 ? w.rhat : (KIND == 3 || KIND == 4 ? w.p : w.s);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) a[i] = av[row * 3 + i];
+            if (KIND == 4)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) b[i] = w.r[row * 3 + i];
+        }
         if (row < r1) {
             row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
             row_aux<kGroup>(w, row, gl, xin, y0, y1, y2);
@@ -474,17 +485,13 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
             yout[row * 3 + 0] = y0;
             yout[row * 3 + 1] = y1;
             yout[row * 3 + 2] = y2;
-            if (KIND == 1) {
-                d0 += w.rhat[row * 3] * y0 + w.rhat[row * 3 + 1] * y1 + w.rhat[row * 3 + 2] * y2;
-            } else if (KIND == 3) {
-                d0 += w.p[row * 3] * y0 + w.p[row * 3 + 1] * y1 + w.p[row * 3 + 2] * y2;
-            } else if (KIND == 4) {  // MINRES: (v, A v) and (v, r1), v in p, r1 in r
-                d0 += w.p[row * 3] * y0 + w.p[row * 3 + 1] * y1 + w.p[row * 3 + 2] * y2;
-                d1 += w.p[row * 3] * w.r[row * 3] + w.p[row * 3 + 1] * w.r[row * 3 + 1] + w.p[row * 3 + 2] * w.r[row * 3 + 2];
-            } else {
-                d0 += w.s[row * 3] * y0 + w.s[row * 3 + 1] * y1 + w.s[row * 3 + 2] * y2;
+            // KIND 1: (rhat, y); 3: (p, y); 4 (MINRES): (v, A v) and (v, r1), v in p, r1 in r;
+            // 2: (s, y) and (y, y)
+            d0 += a[0] * y0 + a[1] * y1 + a[2] * y2;
+            if (KIND == 4)
+                d1 += a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+            else if (KIND == 2)
                 d1 += y0 * y0 + y1 * y1 + y2 * y2;
-            }
         }
     }
 }
@@ -1100,6 +1107,12 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
         const int mk = plan.node_mask[n];
         const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
         double z0 = out[n * 3], z1 = out[n * 3 + 1], z2 = out[n * 3 + 2];
+        double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+        if (PH == 2) {  // loaded before the stores below, in the same round trip
+            q0 = w.r[n * 3];
+            q1 = w.r[n * 3 + 1];
+            q2 = w.r[n * 3 + 2];
+        }
         if (mk & 1) z0 += y[0] + y[4] * dz - y[5] * dy;
         if (mk & 2) z1 += y[1] + y[5] * dx - y[3] * dz;
         if (mk & 4) z2 += y[2] + y[3] * dy - y[4] * dx;
@@ -1107,7 +1120,6 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
         out[n * 3 + 1] = z1;
         out[n * 3 + 2] = z2;
         if (PH == 2) {
-            const double q0 = w.r[n * 3], q1 = w.r[n * 3 + 1], q2 = w.r[n * 3 + 2];
             rz += q0 * z0 + q1 * z1 + q2 * z2;
             rr += q0 * q0 + q1 * q1 + q2 * q2;
         }
