@@ -99,13 +99,17 @@ __device__ __forceinline__ void apply_dinv(const double* dinv, int n, const doub
 template <int G>
 __device__ __forceinline__ void row_dot(const KrylovWork& w, int k0, int k1, const double* __restrict__ xin,
                                         double& y0, double& y1, double& y2) {
+    // the next block's column index is loaded one iteration ahead, so that the x gathers of a
+    // block do not wait for its column index
+    int c = k0 < k1 ? __ldg(w.colidx + k0) : 0;
     for (int k = k0; k < k1; k += G) {
-        const int c = __ldg(w.colidx + k);
+        const int cn = k + G < k1 ? __ldg(w.colidx + k + G) : 0;
         const double* B = w.vals + (size_t)k * 9;
         const double x0 = __ldcg(xin + c * 3), x1 = __ldcg(xin + c * 3 + 1), x2 = __ldcg(xin + c * 3 + 2);
         y0 += __ldg(B + 0) * x0 + __ldg(B + 1) * x1 + __ldg(B + 2) * x2;
         y1 += __ldg(B + 3) * x0 + __ldg(B + 4) * x1 + __ldg(B + 5) * x2;
         y2 += __ldg(B + 6) * x0 + __ldg(B + 7) * x1 + __ldg(B + 8) * x2;
+        c = cn;
     }
 }
 
@@ -457,8 +461,13 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
                                           double* __restrict__ yout, double& d0, double& d1) {
     const int gl = threadIdx.x & (kGroup - 1);
     const int groups = blockDim.x / kGroup;
+    // the block range of the thread's next row is loaded one row ahead
+    int row_n = r0 + threadIdx.x / kGroup;
+    int ka = row_n < r1 ? __ldg(w.rowptr + row_n) : 0, kz = row_n < r1 ? __ldg(w.rowptr + row_n + 1) : 0;
     for (int rb = r0; rb < r1; rb += groups) {
         const int row = rb + threadIdx.x / kGroup;
+        row_n = row + groups;
+        const int ka_n = row_n < r1 ? __ldg(w.rowptr + row_n) : 0, kz_n = row_n < r1 ? __ldg(w.rowptr + row_n + 1) : 0;
         double y0 = 0.0, y1 = 0.0, y2 = 0.0;
         // the row's entries of the dot products' other vectors, loaded by the reducing lane ahead
         // of the row product so that their latency overlaps it
@@ -472,9 +481,11 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
                 for (int i = 0; i < 3; ++i) b[i] = w.r[row * 3 + i];
         }
         if (row < r1) {
-            row_dot<kGroup>(w, __ldg(w.rowptr + row) + gl, __ldg(w.rowptr + row + 1), xin, y0, y1, y2);
+            row_dot<kGroup>(w, ka + gl, kz, xin, y0, y1, y2);
             row_aux<kGroup>(w, row, gl, xin, y0, y1, y2);
         }
+        ka = ka_n;
+        kz = kz_n;
 #pragma unroll
         for (int off = kGroup / 2; off > 0; off >>= 1) {
             y0 += __shfl_xor_sync(0xffffffffu, y0, off);
