@@ -954,7 +954,7 @@ __device__ __forceinline__ void ml_or_batch_range(const BatchPlan& plan, int t, 
 template <int PH>
 __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, int r0, int r1, int l0, int l1,
                            double alpha, double beta, double omega, GridBarrier* bar, int nct, double* cs,
-                           double* dots) {
+                           double* red, double* dots) {
     double* vin = phase_in<PH>(w);
     double* out = phase_out<PH>(w);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -964,22 +964,39 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
     // CTAs' rows as well, hence the group barrier before their moments
     smooth_rows<PH>(w, plan, r0, r1, alpha, beta, omega);
     if (!group_barrier(bar, nct, w.dflags)) return false;
-    // A2: the leaf moments from the updated vector, one warp per leaf
+    // A2: the leaf moments from the updated vector, one warp per leaf; a lane takes two list
+    // positions at a time with every load issued first, and the next leaf's range is loaded one
+    // leaf ahead
+    int ka = l0 + warp < l1 ? plan.agg_ptr[l0 + warp] : 0, kz = l0 + warp < l1 ? plan.agg_ptr[l0 + warp + 1] : 0;
     for (int a = l0 + warp; a < l1; a += nw) {
-        const int k0 = plan.agg_ptr[a], k1 = plan.agg_ptr[a + 1];
+        const int k0 = ka, k1 = kz;
+        ka = a + nw < l1 ? plan.agg_ptr[a + nw] : 0;
+        kz = a + nw < l1 ? plan.agg_ptr[a + nw + 1] : 0;
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int k = k0 + lane; k < k1; k += 32) {
-            const int n = plan.agg_nodes[k];
-            const int mk = plan.node_mask[n];
-            const double u0 = (mk & 1) ? vin[n * 3] : 0.0, u1 = (mk & 2) ? vin[n * 3 + 1] : 0.0,
-                         u2 = (mk & 4) ? vin[n * 3 + 2] : 0.0;
-            const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
-            acc[0] += u0;
-            acc[1] += u1;
-            acc[2] += u2;
-            acc[3] += dy * u2 - dz * u1;
-            acc[4] += dz * u0 - dx * u2;
-            acc[5] += dx * u1 - dy * u0;
+        for (int k = k0 + lane; k < k1; k += 64) {
+            const bool two = k + 32 < k1;
+            int n[2];
+            n[0] = plan.agg_nodes[k];
+            n[1] = two ? plan.agg_nodes[k + 32] : n[0];
+            double u[2][3], d[2][3];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int mk = (h == 0 || two) ? plan.node_mask[n[h]] : 0;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    u[h][i] = ((mk >> i) & 1) ? vin[n[h] * 3 + i] : 0.0;
+                    d[h][i] = plan.node_d[n[h] * 3 + i];
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                acc[0] += u[h][0];
+                acc[1] += u[h][1];
+                acc[2] += u[h][2];
+                acc[3] += d[h][1] * u[h][2] - d[h][2] * u[h][1];
+                acc[4] += d[h][2] * u[h][0] - d[h][0] * u[h][2];
+                acc[5] += d[h][0] * u[h][1] - d[h][1] * u[h][0];
+            }
         }
 #pragma unroll
         for (int q = 0; q < 6; ++q)
@@ -1035,13 +1052,13 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
     __syncthreads();
     double* ys = cs + n6;
     job = 0;
-    for (int lev = 2; lev <= L; ++lev) {
+    for (int lev = 2; lev < L; ++lev) {  // the levels below the top: one warp per set
         const int span = plan.ml_span[lev - 1];
         const int s0 = l0 / span, s1 = l1 > l0 ? (l1 - 1) / span : s0 - 1;  // none for an empty range
         for (int S = s0; S <= s1; ++S, ++job) {
             if (job % nw != warp) continue;
             const int gS = plan.ml_set0[lev - 1] + S;
-            if (lev < L) {
+            {
                 double mq = 0.0;
                 if (lane < 6)
                     for (int k = plan.ml_pstart[gS]; k < plan.ml_pstart[gS + 1]; ++k)
@@ -1056,10 +1073,24 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
                     for (int p = 0; p < 6; ++p) v += W[p] * m[p];
                     ys[6 * job + lane] = v;
                 }
-            } else {
-                const double* rows = plan.ml_top_inv + (size_t)(6 * S) * n6;
+            }
+        }
+    }
+    // the top sets the CTA's leaves overlap (jobs job, job + 1, ...): their rows of the dense top
+    // inverse times the top moments, every set's columns cut into kTopChunks chunks that the
+    // warps share (chunk sums in red, then added in chunk order)
+    {
+        constexpr int kTopChunks = 8, kTopSets = 4;  // red holds kTopSets x kTopChunks x 6 sums
+        const int span = plan.ml_span[L - 1];
+        const int s0 = l0 / span, ntop = l1 > l0 ? (l1 - 1) / span - s0 + 1 : 0;
+        for (int base = 0; base < ntop; base += kTopSets) {
+            const int nb = min(kTopSets, ntop - base);
+            for (int item = warp; item < nb * kTopChunks; item += nw) {
+                const int jt = item / kTopChunks, ch = item % kTopChunks;
+                const double* rows = plan.ml_top_inv + (size_t)(6 * (s0 + base + jt)) * n6;
+                const int c0 = n6 * ch / kTopChunks, c1 = n6 * (ch + 1) / kTopChunks;
                 double y[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                for (int c = lane; c < n6; c += 32) {
+                for (int c = c0 + lane; c < c1; c += 32) {
                     const double x = cs[c];
 #pragma unroll
                     for (int q = 0; q < 6; ++q) y[q] += __ldg(rows + (size_t)q * n6 + c) * x;
@@ -1070,8 +1101,16 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
                     for (int off = 16; off > 0; off >>= 1) y[q] += __shfl_xor_sync(0xffffffffu, y[q], off);
 #pragma unroll
                 for (int q = 0; q < 6; ++q)
-                    if (lane == q) ys[6 * job + q] = y[q];
+                    if (lane == q) red[(jt * kTopChunks + ch) * 6 + q] = y[q];
             }
+            __syncthreads();
+            for (int e = threadIdx.x; e < nb * 6; e += blockDim.x) {
+                const int jt = e / 6, q = e % 6;
+                double v = 0.0;
+                for (int ch = 0; ch < kTopChunks; ++ch) v += red[(jt * kTopChunks + ch) * 6 + q];
+                ys[6 * (job + base + jt) + q] = v;
+            }
+            __syncthreads();  // red is written again by the next sets
         }
     }
     __syncthreads();
@@ -1112,9 +1151,14 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
     // D2: the prolongation, one node per thread (the leaf of each list position in ml_pos_leaf);
     // conjugate gradients' (r, z) and (r, r) over the same nodes on the way
     double rz = 0.0, rr = 0.0;
+    // the next position's node and leaf are loaded one iteration ahead
+    int n_nx = kb + (int)threadIdx.x < ke ? plan.agg_nodes[kb + threadIdx.x] : 0;
+    int lf_nx = kb + (int)threadIdx.x < ke ? plan.ml_pos_leaf[kb + threadIdx.x] : 0;
     for (int k = kb + threadIdx.x; k < ke; k += blockDim.x) {
-        const int n = plan.agg_nodes[k];
-        const double* y = plan.ml_leaf_m + 6 * (size_t)plan.ml_pos_leaf[k];
+        const int n = n_nx;
+        const double* y = plan.ml_leaf_m + 6 * (size_t)lf_nx;
+        n_nx = k + (int)blockDim.x < ke ? plan.agg_nodes[k + blockDim.x] : 0;
+        lf_nx = k + (int)blockDim.x < ke ? plan.ml_pos_leaf[k + blockDim.x] : 0;
         const int mk = plan.node_mask[n];
         const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
         double z0 = out[n * 3], z1 = out[n * 3 + 1], z2 = out[n * 3 + 2];
@@ -1152,7 +1196,7 @@ __device__ bool update_precondition(const KrylovWork& w, const BatchPlan& plan, 
     if (plan.agg_per_cta > 0)
         return precond_phase<PH>(w, plan, lc, r0, r1, alpha, beta, omega, bar, nct, red, ys, cs, cinv_s, Ms);
     if (plan.batch_coarse) return precond_batch<PH>(w, plan, t, ba0, ba1, alpha, beta, omega, bar, nct, cs);
-    if (plan.ml) return precond_ml<PH>(w, plan, lc, r0, r1, ba0, ba1, alpha, beta, omega, bar, nct, cs, dots);
+    if (plan.ml) return precond_ml<PH>(w, plan, lc, r0, r1, ba0, ba1, alpha, beta, omega, bar, nct, cs, red, dots);
     smooth_rows<PH>(w, plan, r0, r1, alpha, beta, omega);
     return true;
 }
