@@ -94,8 +94,11 @@ __device__ __forceinline__ void apply_dinv(const double* dinv, int n, const doub
     out[n * 3 + 2] = D[6] * a + D[7] * b + D[8] * c;
 }
 
-// Partial row product of one lane: blocks k0, k0+G, ... of the row. x is read through L2
-// (ld.cg): inside a persistent kernel it was written by other CTAs.
+// Partial row product of one lane: blocks k0, k0+G, ... of the row. x is read with ordinary
+// L1-cached loads (ld.ca; consecutive rows share most of their columns): inside a persistent
+// kernel it was written by other CTAs before the group barrier, whose fence makes those writes
+// visible to these loads. Never the read-only path (ld.global.nc), which assumes data that does
+// not change during the kernel.
 template <int G>
 __device__ __forceinline__ void row_dot(const KrylovWork& w, int k0, int k1, const double* __restrict__ xin,
                                         double& y0, double& y1, double& y2) {
@@ -105,7 +108,7 @@ __device__ __forceinline__ void row_dot(const KrylovWork& w, int k0, int k1, con
     for (int k = k0; k < k1; k += G) {
         const int cn = k + G < k1 ? __ldg(w.colidx + k + G) : 0;
         const double* B = w.vals + (size_t)k * 9;
-        const double x0 = __ldcg(xin + c * 3), x1 = __ldcg(xin + c * 3 + 1), x2 = __ldcg(xin + c * 3 + 2);
+        const double x0 = __ldca(xin + c * 3), x1 = __ldca(xin + c * 3 + 1), x2 = __ldca(xin + c * 3 + 2);
         y0 += __ldg(B + 0) * x0 + __ldg(B + 1) * x1 + __ldg(B + 2) * x2;
         y1 += __ldg(B + 3) * x0 + __ldg(B + 4) * x1 + __ldg(B + 5) * x2;
         y2 += __ldg(B + 6) * x0 + __ldg(B + 7) * x1 + __ldg(B + 8) * x2;
@@ -122,7 +125,7 @@ __device__ __forceinline__ void row_aux(const KrylovWork& w, int row, int gl, co
     for (int k = w.pk_ptr[row] + gl; k < w.pk_ptr[row + 1]; k += G) {
         const int c = w.pk_col[k];
         const double* B = w.pk_vals + (size_t)w.pk_blk[k] * 9;
-        const double x0 = __ldcg(xin + c * 3), x1 = __ldcg(xin + c * 3 + 1), x2 = __ldcg(xin + c * 3 + 2);
+        const double x0 = __ldca(xin + c * 3), x1 = __ldca(xin + c * 3 + 1), x2 = __ldca(xin + c * 3 + 2);
         y0 += B[0] * x0 + B[1] * x1 + B[2] * x2;
         y1 += B[3] * x0 + B[4] * x1 + B[5] * x2;
         y2 += B[6] * x0 + B[7] * x1 + B[8] * x2;
