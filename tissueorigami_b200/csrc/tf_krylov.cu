@@ -1010,20 +1010,25 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
             if (lane == q) plan.ml_leaf_m[6 * (size_t)a + q] = acc[q];
     }
     __syncthreads();
-    // B
+    // B: this CTA's partial moment of every set of levels >= 2 its leaves overlap, level after
+    // level, one thread per set, each from its children's partials one level down (the leaves for
+    // level 2) moved to the set's centroid; children in index order
     int job = 0;
     for (int lev = 2; lev <= L; ++lev) {
-        const int span = plan.ml_span[lev - 1];
-        const int s0 = l0 / span, s1 = l1 > l0 ? (l1 - 1) / span : s0 - 1;  // none for an empty range
-        for (int S = s0; S <= s1; ++S, ++job) {
-            if (job % nw != warp) continue;
+        const int span = plan.ml_span[lev - 1], cspan = plan.ml_span[lev - 2], fan = span / cspan;
+        const int s0 = l0 / span, s1 = l1 > l0 ? (l1 - 1) / span : s0 - 1;    // none for an empty range
+        const int c0 = l0 / cspan, c1 = l1 > l0 ? (l1 - 1) / cspan : c0 - 1;  // the children's range
+        for (int S = s0 + (int)threadIdx.x; S <= s1; S += blockDim.x) {
             const int gS = plan.ml_set0[lev - 1] + S;
             const double* cS = plan.ml_cen + 3 * (size_t)gS;
-            const int a0 = max(l0, S * span), a1 = min(l1, (S + 1) * span);
             double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            for (int a = a0 + lane; a < a1; a += 32) {
-                const double* m = plan.ml_leaf_m + 6 * (size_t)a;
-                const double* ca = plan.ml_cen + 3 * (size_t)a;
+            const int k0 = max(c0, S * fan), k1 = min(c1, S * fan + fan - 1);
+#pragma unroll 4
+            for (int Sc = k0; Sc <= k1; ++Sc) {
+                const int gC = plan.ml_set0[lev - 2] + Sc;
+                const double* m = lev == 2 ? plan.ml_leaf_m + 6 * (size_t)Sc
+                                           : plan.ml_part + 6 * (size_t)(plan.ml_pstart[gC] + lc - plan.ml_first_cta[gC]);
+                const double* ca = plan.ml_cen + 3 * (size_t)gC;
                 const double dx = ca[0] - cS[0], dy = ca[1] - cS[1], dz = ca[2] - cS[2];
                 const double f0 = m[0], f1 = m[1], f2 = m[2];
                 acc[0] += f0;
@@ -1033,15 +1038,11 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
                 acc[4] += m[4] + dz * f0 - dx * f2;
                 acc[5] += m[5] + dx * f1 - dy * f0;
             }
-#pragma unroll
-            for (int q = 0; q < 6; ++q)
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
             double* dst = plan.ml_part + 6 * (size_t)(plan.ml_pstart[gS] + lc - plan.ml_first_cta[gS]);
 #pragma unroll
-            for (int q = 0; q < 6; ++q)
-                if (lane == q) dst[q] = acc[q];
+            for (int q = 0; q < 6; ++q) dst[q] = acc[q];
         }
+        __syncthreads();  // the next level reads these partials
     }
     if (!group_barrier(bar, nct, w.dflags)) return false;
     // C
