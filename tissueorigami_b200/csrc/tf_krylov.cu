@@ -510,6 +510,18 @@ __device__ __forceinline__ void spmv_rows(const KrylovWork& w, int r0, int r1, c
     }
 }
 
+// The persistent solve keeps a node block's 3x3 inverse in FP32 at dinv32(w) + 9 n (it only
+// preconditions: the residual and the stopping test stay FP64); products are formed in FP64.
+__device__ __forceinline__ float* dinv32(const KrylovWork& w) { return reinterpret_cast<float*>(w.dinv); }
+
+__device__ __forceinline__ void apply_dinv32(const KrylovWork& w, int n, const double* in, double* out) {
+    const float* D = dinv32(w) + (size_t)n * 9;
+    const double a = in[n * 3], b = in[n * 3 + 1], c = in[n * 3 + 2];
+    out[n * 3 + 0] = (double)D[0] * a + (double)D[1] * b + (double)D[2] * c;
+    out[n * 3 + 1] = (double)D[3] * a + (double)D[4] * b + (double)D[5] * c;
+    out[n * 3 + 2] = (double)D[6] * a + (double)D[7] * b + (double)D[8] * c;
+}
+
 // |D_n|^-1 = V |Lambda|^-1 V^T of the symmetric part of node n's diagonal block (cyclic Jacobi
 // rotations): a symmetric positive definite block preconditioner for an indefinite symmetric J
 // (MINRES). An eigenvalue below 1e-300 in magnitude is taken as 1.
@@ -555,12 +567,13 @@ __device__ __forceinline__ void block_abs_inverse_row(const KrylovWork& w, int n
         const double l = fabs(A[k * 4]);
         inv[k] = (l > 1e-300 && isfinite(l)) ? 1.0 / l : 1.0;
     }
-    double* D = w.dinv + (size_t)n * 9;
+    float* D = dinv32(w) + (size_t)n * 9;
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            D[r * 3 + c] = V[r * 3] * V[c * 3] * inv[0] + V[r * 3 + 1] * V[c * 3 + 1] * inv[1] + V[r * 3 + 2] * V[c * 3 + 2] * inv[2];
+            D[r * 3 + c] = (float)(V[r * 3] * V[c * 3] * inv[0] + V[r * 3 + 1] * V[c * 3 + 1] * inv[1] +
+                                   V[r * 3 + 2] * V[c * 3 + 2] * inv[2]);
 }
 
 __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
@@ -569,22 +582,22 @@ __device__ __forceinline__ void block_jacobi_row(const KrylovWork& w, int n) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) m[k] = B[k];
     const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
-    double* D = w.dinv + (size_t)n * 9;
+    float* D = dinv32(w) + (size_t)n * 9;
     if (det == 0.0 || !isfinite(det)) {
         atomicOr(w.dflags, DF_SINGULAR_DIAG);
-        for (int k = 0; k < 9; ++k) D[k] = (k % 4 == 0) ? 1.0 : 0.0;
+        for (int k = 0; k < 9; ++k) D[k] = (k % 4 == 0) ? 1.0f : 0.0f;
         return;
     }
     const double id = 1.0 / det;
-    D[0] = (m[4] * m[8] - m[5] * m[7]) * id;
-    D[1] = (m[2] * m[7] - m[1] * m[8]) * id;
-    D[2] = (m[1] * m[5] - m[2] * m[4]) * id;
-    D[3] = (m[5] * m[6] - m[3] * m[8]) * id;
-    D[4] = (m[0] * m[8] - m[2] * m[6]) * id;
-    D[5] = (m[2] * m[3] - m[0] * m[5]) * id;
-    D[6] = (m[3] * m[7] - m[4] * m[6]) * id;
-    D[7] = (m[1] * m[6] - m[0] * m[7]) * id;
-    D[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+    D[0] = (float)((m[4] * m[8] - m[5] * m[7]) * id);
+    D[1] = (float)((m[2] * m[7] - m[1] * m[8]) * id);
+    D[2] = (float)((m[1] * m[5] - m[2] * m[4]) * id);
+    D[3] = (float)((m[5] * m[6] - m[3] * m[8]) * id);
+    D[4] = (float)((m[0] * m[8] - m[2] * m[6]) * id);
+    D[5] = (float)((m[2] * m[3] - m[0] * m[5]) * id);
+    D[6] = (float)((m[3] * m[7] - m[4] * m[6]) * id);
+    D[7] = (float)((m[1] * m[6] - m[0] * m[7]) * id);
+    D[8] = (float)((m[0] * m[4] - m[1] * m[3]) * id);
 }
 
 // The vector a phase updates and the one its preconditioner writes: BiCGStab's p / phat (PH 0)
@@ -683,10 +696,10 @@ __device__ bool precond_phase(const KrylovWork& w, const BatchPlan& plan, int lc
                 u[i] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
                 vin[d] = u[i];
             }
-            const double* D = w.dinv + (size_t)n * 9;
-            out[n * 3 + 0] = D[0] * u[0] + D[1] * u[1] + D[2] * u[2];
-            out[n * 3 + 1] = D[3] * u[0] + D[4] * u[1] + D[5] * u[2];
-            out[n * 3 + 2] = D[6] * u[0] + D[7] * u[1] + D[8] * u[2];
+            const float* D = dinv32(w) + (size_t)n * 9;
+            out[n * 3 + 0] = (double)D[0] * u[0] + (double)D[1] * u[1] + (double)D[2] * u[2];
+            out[n * 3 + 1] = (double)D[3] * u[0] + (double)D[4] * u[1] + (double)D[5] * u[2];
+            out[n * 3 + 2] = (double)D[6] * u[0] + (double)D[7] * u[1] + (double)D[8] * u[2];
             const int mk = plan.node_mask[n];
             const double u0 = (mk & 1) ? u[0] : 0.0, u1 = (mk & 2) ? u[1] : 0.0, u2 = (mk & 4) ? u[2] : 0.0;
             const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
@@ -818,10 +831,10 @@ __device__ bool precond_batch(const KrylovWork& w, const BatchPlan& plan, int t,
                 u[i] = PH == 0 ? w.r[d] + beta * (w.p[d] - omega * w.v[d]) : w.r[d] - alpha * w.v[d];
                 vin[d] = u[i];
             }
-            const double* D = w.dinv + (size_t)n * 9;
-            out[n * 3 + 0] = D[0] * u[0] + D[1] * u[1] + D[2] * u[2];
-            out[n * 3 + 1] = D[3] * u[0] + D[4] * u[1] + D[5] * u[2];
-            out[n * 3 + 2] = D[6] * u[0] + D[7] * u[1] + D[8] * u[2];
+            const float* D = dinv32(w) + (size_t)n * 9;
+            out[n * 3 + 0] = (double)D[0] * u[0] + (double)D[1] * u[1] + (double)D[2] * u[2];
+            out[n * 3 + 1] = (double)D[3] * u[0] + (double)D[4] * u[1] + (double)D[5] * u[2];
+            out[n * 3 + 2] = (double)D[6] * u[0] + (double)D[7] * u[1] + (double)D[8] * u[2];
             const int mk = plan.node_mask[n];
             const double u0 = (mk & 1) ? u[0] : 0.0, u1 = (mk & 2) ? u[1] : 0.0, u2 = (mk & 4) ? u[2] : 0.0;
             const double dx = plan.node_d[n * 3], dy = plan.node_d[n * 3 + 1], dz = plan.node_d[n * 3 + 2];
@@ -917,7 +930,7 @@ __device__ __forceinline__ void smooth_rows(const KrylovWork& w, const BatchPlan
             u[i] = PH == 0 ? rv + beta * (w.p[d] - omega * vv) : rv - alpha * vv;
         }
 #pragma unroll
-        for (int k = 0; k < 9; ++k) D[k] = __ldg(w.dinv + (size_t)n * 9 + k);
+        for (int k = 0; k < 9; ++k) D[k] = (double)__ldg(dinv32(w) + (size_t)n * 9 + k);
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const int d = n * 3 + i;
@@ -1584,7 +1597,7 @@ __device__ bool solve_tissue_minres(const KrylovWork& w, const BatchPlan& plan, 
             w.shat[d] = 0.0;
             v2[0] += b * b;
         }
-        apply_dinv(w.dinv, n, w.rhat, w.phat);
+        apply_dinv32(w, n, w.rhat, w.phat);
 #pragma unroll
         for (int i = 0; i < 3; ++i) v2[1] += w.rhat[n * 3 + i] * w.phat[n * 3 + i];
     }
@@ -1627,7 +1640,7 @@ __device__ bool solve_tissue_minres(const KrylovWork& w, const BatchPlan& plan, 
                 w.r[d] = w.rhat[d];
                 w.rhat[d] = y;
             }
-            apply_dinv(w.dinv, n, w.rhat, w.phat);
+            apply_dinv32(w, n, w.rhat, w.phat);
 #pragma unroll
             for (int i = 0; i < 3; ++i) e1[0] += w.rhat[n * 3 + i] * w.phat[n * 3 + i];
         }
