@@ -358,15 +358,15 @@ def run_b200(args) -> None:
     # persistent solve: per BiCGStab iteration two SpMVs (each also reads one dot vector)
     # and three node-wise phases (p/phat: r,p,v,D -> p,phat; s/shat: r,v,D -> s,shat;
     # x/r: x,phat,shat,s,t,rhat -> x,r); plus one setup pass (diagonal inverses, r, rhat, p, v)
-    # D^-1 is 72 G bytes per node with blocks of G nodes (a prism column's 3G x 3G inverse); with
-    # G > 1 it is set up by a separate kernel before the launch. Per conjugate-gradient iteration
+    # D^-1 is FP32, 36 G bytes per node with blocks of G nodes (a node's 3x3 inverse, or a prism
+    # column's 3G x 3G inverse); with G > 1 it is set up by a separate kernel before the launch. Per conjugate-gradient iteration
     # one SpMV (plus the p re-read of its dot) and three node-wise phases (p = z + beta p:
     # z,p -> p; x += alpha p: x,p -> x; r -= alpha q, z = D^-1 r with (r,z), (r,r): r,q,D -> r,z
     # and the two dot vectors re-read).
     G = sched.get("smoother_block_nodes", 1)
-    per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 72 * G + 4 * 24 + 72 * G + 8 * 24)
-    per_iter_cg = bytes_spmv + 24.0 * N + N * (3 * 24 + 3 * 24 + 4 * 24 + 72 * G + 2 * 24)
-    per_setup = N * ((72.0 + 72 if G == 1 else 0.0) + 24 + 4 * 24)
+    per_iter = 2.0 * (bytes_spmv + 24.0 * N) + N * (5 * 24 + 36 * G + 4 * 24 + 36 * G + 8 * 24)
+    per_iter_cg = bytes_spmv + 24.0 * N + N * (3 * 24 + 3 * 24 + 4 * 24 + 36 * G + 2 * 24)
+    per_setup = N * ((72.0 + 36 if G == 1 else 0.0) + 24 + 4 * 24)
     if sched.get("precond_effective") == "two_level" and sched.get("coarse_unknowns", 0) > 0:
         # two applications of the coarse correction per iteration, each reading the node modes
         # (d_i, mask) in the restriction and the prolongation and updating the preconditioned
