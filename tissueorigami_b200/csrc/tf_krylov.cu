@@ -1068,30 +1068,35 @@ __device__ bool precond_ml(const KrylovWork& w, const BatchPlan& plan, int lc, i
     }
     __syncthreads();
     double* ys = cs + n6;
+    // the levels below the top: one thread per (set, component), jobs numbered level by level;
+    // each thread sums its set's partial moments in CTA order and applies its row of W_S
     job = 0;
-    for (int lev = 2; lev < L; ++lev) {  // the levels below the top: one warp per set
+    for (int lev = 2; lev < L; ++lev) {
         const int span = plan.ml_span[lev - 1];
-        const int s0 = l0 / span, s1 = l1 > l0 ? (l1 - 1) / span : s0 - 1;  // none for an empty range
-        for (int S = s0; S <= s1; ++S, ++job) {
-            if (job % nw != warp) continue;
-            const int gS = plan.ml_set0[lev - 1] + S;
-            {
-                double mq = 0.0;
-                if (lane < 6)
-                    for (int k = plan.ml_pstart[gS]; k < plan.ml_pstart[gS + 1]; ++k)
-                        mq += __ldcg(plan.ml_part + 6 * (size_t)k + lane);
-                double m[6];
-#pragma unroll
-                for (int p = 0; p < 6; ++p) m[p] = __shfl_sync(0xffffffffu, mq, p);
-                if (lane < 6) {
-                    const double* W = plan.ml_w + 36 * (size_t)gS + 6 * lane;
-                    double v = 0.0;
-#pragma unroll
-                    for (int p = 0; p < 6; ++p) v += W[p] * m[p];
-                    ys[6 * job + lane] = v;
-                }
+        job += l1 > l0 ? (l1 - 1) / span - l0 / span + 1 : 0;
+    }
+    for (int e = threadIdx.x; e < 6 * job; e += blockDim.x) {
+        const int jg = e / 6, q = e - 6 * jg;
+        int jl = jg, lev = 2, S = 0;
+        for (; lev < L; ++lev) {  // the job's level and set (l1 > l0 here)
+            const int span = plan.ml_span[lev - 1];
+            const int s0 = l0 / span, ns = (l1 - 1) / span - s0 + 1;
+            if (jl < ns) {
+                S = s0 + jl;
+                break;
             }
+            jl -= ns;
         }
+        const int gS = plan.ml_set0[lev - 1] + S;
+        double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int k = plan.ml_pstart[gS]; k < plan.ml_pstart[gS + 1]; ++k)
+#pragma unroll
+            for (int p = 0; p < 6; ++p) m[p] += __ldcg(plan.ml_part + 6 * (size_t)k + p);
+        const double* W = plan.ml_w + 36 * (size_t)gS + 6 * q;
+        double v = 0.0;
+#pragma unroll
+        for (int p = 0; p < 6; ++p) v += W[p] * m[p];
+        ys[6 * jg + q] = v;
     }
     // the top sets the CTA's leaves overlap (jobs job, job + 1, ...): their rows of the dense top
     // inverse times the top moments, every set's columns cut into kTopChunks chunks that the
