@@ -69,9 +69,11 @@ extern "C" {
 #define TF_KRYLOV_CG 2        /* preconditioned conjugate gradients; a tissue whose J turns */
                               /* out indefinite is solved again with BiCGStab              */
 
-#define TF_SCATTER_AUTO 0     /* pick by the autotuner's cached choice                   */
+#define TF_SCATTER_AUTO 0     /* the autotuner's choice once tf_autotune ran, else ATOMIC */
 #define TF_SCATTER_ATOMIC 1   /* FP64 atomics into the fixed BSR3 pattern                */
 #define TF_SCATTER_COLOURED 2 /* greedy element colouring, plain read-modify-write       */
+#define TF_SCATTER_STAGED 3   /* FP64 atomics from a shared-memory stage, one block's    */
+                              /* entries on consecutive threads (fewer L2 sectors)       */
 
 typedef struct tf_ctx tf_ctx;
 
@@ -130,7 +132,7 @@ typedef struct tf_step_stats {
 } tf_step_stats;
 
 /* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), Krylov rtol
- * 1e-12 with cap 20000, the two-level preconditioner (TF_PRECOND_TWO_LEVEL), autotuned scatter,
+ * 1e-12 with cap 20000, the two-level preconditioner (TF_PRECOND_TWO_LEVEL), TF_SCATTER_AUTO,
  * device 0, graphs on, persistent solve on, smoother block chosen from the mesh, no refinement,
  * TF_KRYLOV_AUTO. */
 void tf_default_params(tf_params* p);

@@ -44,7 +44,9 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("eta", [0.0, 4.0])
 @pytest.mark.parametrize("scatter,teams", [(capi.TF_SCATTER_ATOMIC, 16), (capi.TF_SCATTER_COLOURED, 8),
-                                           (capi.TF_SCATTER_ATOMIC, 32), (capi.TF_SCATTER_COLOURED, 32)])
+                                           (capi.TF_SCATTER_ATOMIC, 32), (capi.TF_SCATTER_COLOURED, 32),
+                                           (capi.TF_SCATTER_STAGED, 8), (capi.TF_SCATTER_STAGED, 16),
+                                           (capi.TF_SCATTER_STAGED, 32)])
 def test_assembly_matches_oracle(eta, scatter, teams):
     t, uk, un, inv = _state(mesh.small_rectangle(nx=9, ny=6), eta=eta)
     vs = O.viscosity_surfaces(t, uk)
@@ -298,7 +300,7 @@ def test_schedule_and_autotune():
         sch = s.schedule()
         assert sch["n_colours"] > 0
         tuned = s.autotune(t.x, t.dt)
-        assert tuned["scatter"] in (capi.TF_SCATTER_ATOMIC, capi.TF_SCATTER_COLOURED)
+        assert tuned["scatter"] in (capi.TF_SCATTER_ATOMIC, capi.TF_SCATTER_COLOURED, capi.TF_SCATTER_STAGED)
         assert tuned["elems_per_block"] in (8, 16, 32)
         me, ms = s.time_kernels(5)
         assert me > 0 and ms > 0

@@ -37,6 +37,7 @@ TF_KRYLOV_CG = 2
 TF_SCATTER_AUTO = 0
 TF_SCATTER_ATOMIC = 1
 TF_SCATTER_COLOURED = 2
+TF_SCATTER_STAGED = 3
 
 STATUS_NAMES = {
     0: "ok", 1: "newton_not_converged", 2: "krylov_max_iters", 3: "krylov_breakdown",

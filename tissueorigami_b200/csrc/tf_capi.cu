@@ -828,7 +828,7 @@ cudaError_t launch_elements(tf_ctx* c, double dt, int scatter, int teams) {
         return cudaSuccess;
     }
     c->launches += 1;
-    return launch_element_assemble(a, teams, c->has_visc, 0, c->stream);
+    return launch_element_assemble(a, teams, c->has_visc, scatter == TF_SCATTER_STAGED ? 2 : 0, c->stream);
 }
 
 // One Newton iteration's system: J (BSR3) and g in the context's buffers.
@@ -2292,6 +2292,7 @@ static int create_ctx(const tf_mesh_desc* mesh, const tf_params* params, int32_t
         ctx->persistent_grid_max == 0)
         ctx->params.precond = TF_PRECOND_BLOCK_JACOBI;
     ctx->h_fixmask.assign(N, 0);
+    if (ctx->params.scatter < TF_SCATTER_AUTO || ctx->params.scatter > TF_SCATTER_STAGED) return TF_ERR_ARGUMENT;
     if (ctx->params.scatter == TF_SCATTER_COLOURED && ctx->n_colours == 0) return TF_ERR_UNSUPPORTED;
     ctx->scatter = ctx->params.scatter == TF_SCATTER_AUTO ? TF_SCATTER_ATOMIC : ctx->params.scatter;
     ctx->teams = ctx->params.elems_per_block > 0 ? ctx->params.elems_per_block : 16;
@@ -3077,7 +3078,7 @@ int tf_autotune(tf_ctx* ctx, const double* x_n, double dt) {
     const int teams_opts[3] = {8, 16, 32};
     float best = 1e30f;
     int best_sc = TF_SCATTER_ATOMIC, best_t = 32;
-    for (int sc = TF_SCATTER_ATOMIC; sc <= TF_SCATTER_COLOURED; ++sc) {
+    for (int sc = TF_SCATTER_ATOMIC; sc <= TF_SCATTER_STAGED; ++sc) {
         if (sc == TF_SCATTER_COLOURED && ctx->n_colours == 0) continue;
         if (ctx->params.scatter != TF_SCATTER_AUTO && sc != ctx->params.scatter) continue;
         for (int t : teams_opts) {

@@ -9,6 +9,9 @@
 //   phase 2  the six threads split the 21 symmetric 3x3 blocks (36 when internal viscosity
 //            is on) and the 6 nodal forces, sum the Gauss points and scatter straight into
 //            the BSR3 Jacobian and the residual - no 18x18 element matrix ever reaches HBM.
+//   phase 3  (staged scatter only) the blocks wait in shared memory and the whole CTA adds
+//            them to J with consecutive threads on consecutive entries of one block, so a
+//            warp's FP64 reductions reach L2 as ~12 sectors instead of 32.
 //
 // Closed-form tangent. For the neo-Hookean law of Prism.cpp:793-794 the reference's D81
 // contraction (ShapeBase.cpp:3010-3062) pushes forward to
@@ -78,13 +81,21 @@ __constant__ int8_t c_pairA[36] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4, 
 __constant__ int8_t c_pairB[36] = {1, 2, 3, 4, 5, 2, 3, 4, 5, 3, 4, 5, 4, 5, 5, 0, 1, 2, 3, 4, 5,
                                    0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4};
 
+// Scatter modes of k_element_assemble: each lane adds its own blocks with FP64 atomics (0), adds
+// them with plain read-modify-writes inside one element colour (1), or stages them in shared
+// memory for a CTA-wide pass of atomics laid out entry by entry (2).
+constexpr int kScatterAtomic = 0, kScatterColoured = 1, kScatterStaged = 2;
+
 template <int MODE>
 __device__ __forceinline__ void add_entry(double* p, double v) {
-    if (MODE == 0)
-        atomicAdd(p, v);
-    else
+    if (MODE == kScatterColoured)
         *p += v;
+    else
+        atomicAdd(p, v);
 }
+
+// Position in the pair order above of the off-diagonal pair (a, b), a < b.
+__device__ __forceinline__ int upper_pair(int a, int b) { return a * 5 - (a * (a - 1)) / 2 + (b - a - 1); }
 
 __device__ int find_block(const int32_t* rowptr, const int32_t* colidx, int row, int col) {
     int lo = rowptr[row], hi = rowptr[row + 1] - 1;
@@ -119,7 +130,11 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
     double(*s_x)[18] = reinterpret_cast<double(*)[18]>(smem_dyn + TEAMS * kElemWords);
     double(*s_v)[18] = reinterpret_cast<double(*)[18]>(smem_dyn + TEAMS * (kElemWords + 18));
     double(*s_gp)[6][GPW] = reinterpret_cast<double(*)[6][GPW]>(smem_dyn + TEAMS * (kElemWords + (VISC ? 36 : 18)));
-    int(*s_fix)[6] = reinterpret_cast<int(*)[6]>(smem_dyn + TEAMS * (kElemWords + (VISC ? 36 : 18) + 6 * GPW));
+    constexpr int NB = VISC ? 36 : 21;  // blocks a team computes (21 symmetric pairs without viscosity)
+    double(*s_K)[NB][9] = reinterpret_cast<double(*)[NB][9]>(smem_dyn + TEAMS * (kElemWords + (VISC ? 36 : 18) + 6 * GPW));
+    int(*s_fix)[6] = reinterpret_cast<int(*)[6]>(smem_dyn + TEAMS * (kElemWords + (VISC ? 36 : 18) + 6 * GPW +
+                                                                   (MODE == kScatterStaged ? NB * 9 : 0)));
+    int* s_go = reinterpret_cast<int*>(s_fix + TEAMS);  // staged scatter: team active and not routed
 
     const int team = threadIdx.x / 6;
     const int lane = threadIdx.x - team * 6;
@@ -224,12 +239,13 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
         }
     }
     __syncthreads();
-    if (!active) return;
+    if (MODE != kScatterStaged && !active) return;
 
-    const bool routed = (R.flags & 1) != 0;
+    const bool routed = active && (R.flags & 1) != 0;
+    if (MODE == kScatterStaged && lane == 0) s_go[team] = active && !routed;
 
     // ---- phase 2a: nodal forces, node a = lane ---------------------------------------------
-    {
+    if (active) {
         const int a = lane;
         double f0 = 0.0, f1 = 0.0, f2 = 0.0;
 #pragma unroll
@@ -258,8 +274,7 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
     }
 
     // ---- phase 2b: tangent blocks ----------------------------------------------------------
-    constexpr int NB = VISC ? 36 : 21;
-    for (int pb = lane; pb < NB; pb += 6) {
+    for (int pb = lane; active && pb < NB; pb += 6) {
         const int a = c_pairA[pb], b = c_pairB[pb];
         double K[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
@@ -301,6 +316,13 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
                         K[i][j] += cv * (ab * P[i * 3 + j] + bv[i] * Pta[j]) + Sva[i] * bv[j] - Svb[i] * av[j];
             }
         }
+        if (MODE == kScatterStaged && !routed) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) s_K[team][pb][i * 3 + k] = K[i][k];
+            continue;
+        }
         const int fa = s_fix[team][a], fb = s_fix[team][b];
         if (routed) {
             const int na = R.conn[a], nb = R.conn[b];
@@ -327,6 +349,47 @@ __global__ void __launch_bounds__(TEAMS * 6) k_element_assemble(AssembleArgs A) 
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
                     if (!((fa >> i) & 1) && !((fb >> k) & 1)) add_entry<MODE>(blkT + k * 3 + i, K[i][k]);
+        }
+    }
+
+    // ---- phase 3 (staged scatter): the CTA's 36 destination blocks per prism, one entry per
+    // thread, entries of a block on consecutive threads. The (block, entry) a thread adds is the
+    // same for every prism of the CTA, so it is decoded once: bits 0-8 source offset in the
+    // team's stage (< 36 * 9), 9-14 destination block p*6+q, 15-18 entry r*3+c, 19-21 p,
+    // 22-23 r, 24-26 q, 27-28 c.
+    if (MODE == kScatterStaged) {
+        constexpr int NT = TEAMS * 6, NJ = (324 + NT - 1) / NT;
+        int desc[NJ];
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const int rem = threadIdx.x + j * NT;
+            const int d = rem / 9, en = rem - d * 9;
+            const int p = d / 6, q = d - p * 6, r = en / 3, c = en - r * 3;
+            int src;
+            if (p == q)
+                src = (15 + p) * 9 + en;
+            else if (p < q)
+                src = upper_pair(p, q) * 9 + en;
+            else if (VISC)
+                src = (21 + upper_pair(q, p)) * 9 + en;
+            else
+                src = upper_pair(q, p) * 9 + c * 3 + r;
+            desc[j] = rem < 324 ? src | d << 9 | en << 15 | p << 19 | r << 22 | q << 24 | c << 27 : -1;
+        }
+        __syncthreads();
+        for (int tm = 0; tm < TEAMS; ++tm) {
+            if (!s_go[tm]) continue;
+            const ElemRecord& Rt = *reinterpret_cast<const ElemRecord*>(&s_rec[tm][0]);
+            const double* stage = &s_K[tm][0][0];
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                const int dj = desc[j];
+                if (dj < 0) continue;
+                if (((s_fix[tm][(dj >> 19) & 7] >> ((dj >> 22) & 3)) & 1) ||
+                    ((s_fix[tm][(dj >> 24) & 7] >> ((dj >> 27) & 3)) & 1))
+                    continue;
+                atomicAdd(A.vals + (size_t)Rt.slots[(dj >> 9) & 63] * 9 + ((dj >> 15) & 15), stage[dj & 511]);
+            }
         }
     }
 }
@@ -606,15 +669,17 @@ __global__ void k_viscosity_surface(const ElemRecord* elems, int32_t n_elems, co
     }
 }
 
-template <int TEAMS, bool VISC>
+template <int TEAMS, bool VISC, int MODE>
 constexpr size_t element_smem_bytes() {
-    return sizeof(double) * TEAMS * (kElemWords + (VISC ? 36 : 18) + 6 * (VISC ? 42 : 26)) + sizeof(int) * TEAMS * 6;
+    return sizeof(double) * TEAMS *
+               (kElemWords + (VISC ? 36 : 18) + 6 * (VISC ? 42 : 26) + (MODE == kScatterStaged ? (VISC ? 36 : 21) * 9 : 0)) +
+           sizeof(int) * TEAMS * 7;
 }
 
 template <int TEAMS, bool VISC, int MODE>
 cudaError_t launch_t(const AssembleArgs& a, cudaStream_t s) {
     static bool attr_set = false;
-    constexpr size_t smem = element_smem_bytes<TEAMS, VISC>();
+    constexpr size_t smem = element_smem_bytes<TEAMS, VISC, MODE>();
     if (!attr_set) {
         cudaError_t err = cudaFuncSetAttribute(k_element_assemble<TEAMS, VISC, MODE>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -627,10 +692,18 @@ cudaError_t launch_t(const AssembleArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int TEAMS, bool VISC>
+cudaError_t launch_modes(const AssembleArgs& a, int mode, cudaStream_t s) {
+    switch (mode) {
+        case kScatterColoured: return launch_t<TEAMS, VISC, kScatterColoured>(a, s);
+        case kScatterStaged: return launch_t<TEAMS, VISC, kScatterStaged>(a, s);
+        default: return launch_t<TEAMS, VISC, kScatterAtomic>(a, s);
+    }
+}
+
 template <int TEAMS>
 cudaError_t launch_teams(const AssembleArgs& a, bool visc, int mode, cudaStream_t s) {
-    if (visc) return mode == 0 ? launch_t<TEAMS, true, 0>(a, s) : launch_t<TEAMS, true, 1>(a, s);
-    return mode == 0 ? launch_t<TEAMS, false, 0>(a, s) : launch_t<TEAMS, false, 1>(a, s);
+    return visc ? launch_modes<TEAMS, true>(a, mode, s) : launch_modes<TEAMS, false>(a, mode, s);
 }
 
 bool g_table_ready = false;

@@ -209,7 +209,8 @@ constexpr int kMaxCoarse = 2048;  // coarse unknowns the persistent solve stages
 constexpr int kCoarseSmemBytes = 96 * 1024;
 
 // --- element assembly (tf_element.cu) ---------------------------------------------------
-// mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class)
+// mode: 0 = atomic scatter, 1 = plain read-modify-write (caller guarantees a colour class),
+// 2 = atomics from a shared-memory stage, a block's entries on consecutive threads
 cudaError_t launch_element_assemble(const AssembleArgs& a, int teams, bool visc, int mode,
                                     cudaStream_t s);
 cudaError_t launch_node_terms(const NodeArgs& a, cudaStream_t s);
