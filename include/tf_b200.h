@@ -108,6 +108,11 @@ typedef struct tf_params {
                               /* Newton iteration corrects the previous one's solve error    */
     int32_t krylov_method;    /* TF_KRYLOV_*; the persistent solve only (the graph-replayed */
                               /* and allocation-free paths run BiCGStab)                    */
+    int32_t krylov_warm_start; /* 1: in the Newton loop of a single tissue, conjugate       */
+                              /* gradients start from the previous step's solution of the   */
+                              /* same Newton iteration (x0, r0 = g - J x0; from zero if that */
+                              /* residual is not below ||g||); 0: every solve from zero.    */
+                              /* Same stopping rule either way; the adjoint runs cold       */
 } tf_params;
 
 typedef struct tf_step_stats {

@@ -72,7 +72,7 @@ class Params(ctypes.Structure):
                 ("elems_per_block", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("use_graphs", ctypes.c_int32), ("persistent", ctypes.c_int32),
                 ("smoother_nodes", ctypes.c_int32), ("krylov_refine", ctypes.c_int32),
-                ("krylov_method", ctypes.c_int32)]
+                ("krylov_method", ctypes.c_int32), ("krylov_warm_start", ctypes.c_int32)]
 
 
 class GridGrowth(ctypes.Structure):

@@ -35,6 +35,7 @@ constexpr int kMlLeafCols = 16;      // prism columns per leaf of the multilevel
 constexpr int kMlTopMax = 160;       // sets of the multilevel space's densely inverted top level
 constexpr int kMlAutoNodes = 100000; // single tissues from this size take the multilevel space
 constexpr int kMlTopMaxAge = 8;      // solves between refreshes of the multilevel top inverse
+constexpr int kWarmSlots = 8;        // Newton iterations whose solutions are kept for warm starts
 
 struct DevBuf {
     void* p = nullptr;
@@ -50,6 +51,13 @@ T* dptr(DevBuf& b) {
 
 struct tf_ctx {
     tf_params params{};
+    // Warm starts of the Newton loop's solves (single tissue, conjugate gradients): the solution
+    // of Newton iteration k of the last step that reached it, and the iteration the current
+    // solve belongs to (-1 outside the Newton loop).
+    std::vector<DevBuf> warm_hist;
+    std::vector<char> warm_valid;
+    int warm_k = -1;
+    bool warm_call = false;  // the current call is a time step of the public API (not the adjoint's)
     int device = 0;
     cudaStream_t stream = nullptr;
     int32_t N = 0, E = 0;
@@ -1695,7 +1703,23 @@ int krylov_solve(tf_ctx* ctx) {
                 if (top) ctx->ml_top_fresh = true;
             }
         }
-        const BatchPlan plan = make_plan(ctx);
+        BatchPlan plan = make_plan(ctx);
+        // Warm start (tf_params.krylov_warm_start): inside the Newton loop of a single tissue,
+        // conjugate gradients start from the solution of the same Newton iteration of the last
+        // step that reached it, with its true residual r0 = g - J x0 (the kernel falls back to
+        // x0 = 0 when ||r0|| is not below ||g||). Consecutive steps grow the tissue by similar
+        // increments, so ||r0|| is typically a tenth of ||g||. Not for the lumen's second solve
+        // (another right-hand side) or MINRES.
+        const size_t bytes3 = sizeof(double) * 3 * (size_t)ctx->N;
+        const int wk = ctx->warm_k;
+        const bool warm_slot = ctx->params.krylov_warm_start && ctx->T == 1 && plan.cg && !plan.minres &&
+                               !ctx->reuse_precond && wk >= 0 && wk < kWarmSlots;
+        if (warm_slot && wk < (int)ctx->warm_valid.size() && ctx->warm_valid[wk]) {
+            TF_CK(cudaMemcpyAsync(ctx->du.p, ctx->warm_hist[wk].p, bytes3, cudaMemcpyDeviceToDevice, ctx->stream));
+            TF_CK(launch_residual(w, dptr<double>(ctx->du), dptr<double>(ctx->g), dptr<double>(ctx->r), ctx->stream));
+            ctx->launches += 1;
+            plan.warm = 1;
+        }
         if (plan.group > 1) {
             TF_CK(launch_group_jacobi_setup(w, plan.group, ctx->stream));
             ctx->launches += 1;
@@ -1769,6 +1793,18 @@ int krylov_solve(tf_ctx* ctx) {
             }
         }
         *ctx->h_sc = ctx->h_tsc[0];
+        if (warm_slot && ctx->h_tsc[0].status == KS_CONVERGED) {
+            if ((int)ctx->warm_hist.size() <= wk) {
+                ctx->warm_hist.resize(wk + 1);
+                ctx->warm_valid.resize(wk + 1, 0);
+            }
+            if (dalloc(ctx->warm_hist[wk], bytes3) == cudaSuccess) {
+                TF_CK(cudaMemcpyAsync(ctx->warm_hist[wk].p, ctx->du.p, bytes3, cudaMemcpyDeviceToDevice, ctx->stream));
+                ctx->warm_valid[wk] = 1;
+            } else {
+                (void)cudaGetLastError();  // no room for the history: this iteration keeps starting from zero
+            }
+        }
         for (int t = 0; t < ctx->T; ++t)
             if (ctx->T == 1 || ctx->h_active[t]) {
                 ctx->last_method = std::max(ctx->last_method, ctx->h_tsc[t].method);
@@ -1904,7 +1940,9 @@ int newton_core(tf_ctx* ctx, double dt, tf_step_stats* st) {
         int rc = assemble_system(ctx, dt);
         if (rc != TF_OK) return rc;
         TF_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+        ctx->warm_k = ctx->warm_call && T == 1 ? ctx->t_iters[0] : -1;
         rc = newton_solve(ctx);
+        ctx->warm_k = -1;
         if (rc != TF_OK) return rc;
         KrylovWork w = make_work(ctx);
         if (persistent) {
@@ -2129,6 +2167,7 @@ void tf_default_params(tf_params* p) {
     p->smoother_nodes = 0;
     p->krylov_refine = 0;
     p->krylov_method = TF_KRYLOV_AUTO;
+    p->krylov_warm_start = 1;
 }
 
 const char* tf_version(void) { return "tissueorigami_b200 0.1 (sm_100a, FP64)"; }
@@ -2385,7 +2424,7 @@ void tf_destroy(tf_ctx* ctx) {
     DevBuf* batch[] = {&ctx->plan_queue_d, &ctx->queue_head_d, &ctx->node_tissue_d, &ctx->plan_list_ptr_d,
                        &ctx->plan_list_d, &ctx->plan_cta0_d, &ctx->plan_ncta_d, &ctx->plan_row0_d, &ctx->active_d, &ctx->tbarriers, &ctx->tscalars, &ctx->tdu2};
     for (DevBuf* b : batch) dfree(*b);
-    for (auto* v : {&ctx->cp_x, &ctx->cp_fg, &ctx->seg_x, &ctx->seg_fg})
+    for (auto* v : {&ctx->cp_x, &ctx->cp_fg, &ctx->seg_x, &ctx->seg_fg, &ctx->warm_hist})
         for (DevBuf& b : *v) dfree(b);
     DevBuf* adj[] = {&ctx->abar, &ctx->abar2, &ctx->mubar, &ctx->dLdr, &ctx->qbuf, &ctx->ilu_cnodes, &ctx->ilu_lo_ptr,
                      &ctx->ilu_lo_idx, &ctx->ilu_up_ptr, &ctx->ilu_up_idx, &ctx->ilu_lu, &ctx->ilu_uinv, &ctx->ilu_y};
@@ -2727,7 +2766,9 @@ static int step_entry(tf_ctx* ctx, const double* x_n, double dt, double* x_out, 
         rc = prologue(ctx, dt);
         if (rc != TF_OK) return rc;
     }
+    ctx->warm_call = true;
     rc = newton_core(ctx, dt, st);
+    ctx->warm_call = false;
     if (rc < 0) return rc;
     if (grow) ctx->sim_time += dt;  // runOneStep ends with currSimTimeSec += dt
     TF_CK(cudaMemcpyAsync(x_out, ctx->uk.p, bytes, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));

@@ -1457,31 +1457,53 @@ __device__ bool solve_tissue_cg(const KrylovWork& w, const BatchPlan& plan, int 
         for (int i = threadIdx.x; i < 36 * plan.agg_per_cta; i += blockDim.x)
             Ms[i] = plan.agg_m[(size_t)lc * plan.agg_per_cta * 36 + i];
     }
-    // set-up: block-Jacobi inverses, x = 0, r = b, p = q = 0, ||b||^2
-    double v1[1] = {0.0};
-    for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
-        if (plan.group == 1) block_jacobi_row(w, n);
+    // set-up: block-Jacobi inverses, x = 0, r = b, p = q = 0, ||b||^2; warm start (plan.warm):
+    // x0 and r0 = b - J x0 given by the host, ||r0||^2 beside ||b||^2
+    double v1[1] = {0.0}, t1[1], t2[2];
+    {
+        double v0[2] = {0.0, 0.0};
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x) {
+            if (plan.group == 1) block_jacobi_row(w, n);
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const int d = n * 3 + i;
-            const double b = w.b[d];
-            w.x[d] = 0.0;
-            w.r[d] = b;
-            w.p[d] = 0.0;
-            w.v[d] = 0.0;
-            v1[0] += b * b;
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                const double b = w.b[d];
+                double r = b;
+                if (plan.warm)
+                    r = w.r[d];
+                else
+                    w.x[d] = 0.0;
+                w.r[d] = r;
+                w.p[d] = 0.0;
+                w.v[d] = 0.0;
+                v0[0] += b * b;
+                v0[1] += r * r;
+            }
         }
+        write_partials<2>(v0, part[pb], lc, smem);
     }
-    write_partials<1>(v1, part[pb], lc, smem);
     if (!group_barrier(bar, nct, w.dflags)) return false;
-    double t1[1], t2[2];
-    sum_partials<1>(part[pb], nct, t1, smem, sb);
+    sum_partials<2>(part[pb], nct, t2, smem, sb);
     pb ^= 1;
-    const double bb = t1[0];
+    const double bb = t2[0];
+    double rr = t2[1];
+    if (plan.warm && !(rr < bb)) {
+        // the guess is no better than zero (or not finite): every CTA of the group sees the same
+        // sums and takes this branch; start from x = 0 and wait until every row is reset
+        for (int n = r0 + threadIdx.x; n < r1; n += blockDim.x)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int d = n * 3 + i;
+                w.x[d] = 0.0;
+                w.r[d] = w.b[d];
+            }
+        rr = bb;
+        if (!group_barrier(bar, nct, w.dflags)) return false;
+    }
     const double tol2 = rtol * rtol * bb;
-    double rr = bb, rz = 0.0, alpha = 0.0, beta = 0.0;
+    double rz = 0.0, alpha = 0.0, beta = 0.0;
     int it = 0;
-    int status = !isfinite(bb) ? KS_NONFINITE : (bb == 0.0 ? KS_CONVERGED : KS_RUNNING);
+    int status = !isfinite(bb) ? KS_NONFINITE : (rr <= tol2 ? KS_CONVERGED : KS_RUNNING);
     if (status == KS_RUNNING) {  // z = M^-1 r, (r, z)
         double dd[2] = {0.0, 0.0};
         if (!update_precondition<2>(w, plan, t, lc, r0, r1, ba0, ba1, 0.0, 0.0, 0.0, bar, nct, red, ys, cs, cinv_s, Ms, dd))
