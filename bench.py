@@ -347,11 +347,15 @@ def run_b200(args) -> None:
     # the committed captures are of the default sizes: a reduced slab has no entry
     traffic_key = t.name if (t.name != "large_slab" or args.slab_grid == "1000x500") else None
 
-    def roof(name, b, t_ms):
+    def roof(name, b, t_ms, iters=None):
         ach = b / (t_ms * 1e-3) / 1e9
+        tr, tr_iters = traffic.get((name, traffic_key), (None, None))
+        if tr is not None and tr_iters and iters:
+            # a solve's DRAM traffic grows with its Krylov iterations: the capture's bytes per
+            # launch scaled from its iteration count to this run's
+            tr *= iters / tr_iters
         return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "peak_source": peak_src, "algorithmic_bytes": b, "ms_per_launch": t_ms,
-                "traffic": traffic.get((name, traffic_key))}
+                "peak_source": peak_src, "algorithmic_bytes": b, "ms_per_launch": t_ms, "traffic": tr}
 
     r_el = roof("element_assemble", bytes_asm, ms_el)
     r_sp = roof("bsr3_spmv", bytes_spmv, ms_spmv)
@@ -384,7 +388,7 @@ def run_b200(args) -> None:
     kry_bi = kry - kry_cg
     if solve_launches > 0:
         bytes_solve = (kry_bi * per_iter + kry_cg * per_iter_cg + solve_launches * per_setup) / solve_launches
-        r_solve = roof("bicgstab_persistent", bytes_solve, solve_ms / solve_launches)
+        r_solve = roof("bicgstab_persistent", bytes_solve, solve_ms / solve_launches, kry / solve_launches)
         r_solve["krylov_iterations_per_launch"] = kry / solve_launches
         r_solve["cg_iterations_per_launch"] = kry_cg / solve_launches
         # the element kernel's own bound is FP64, not HBM: the closed-form tangent costs ~15.2 k
@@ -650,7 +654,8 @@ def run_adjoint(args) -> None:
 
 def load_traffic():
     """Per-launch DRAM bytes from committed ncu summaries (profiles/traffic.tsv:
-    kernel<TAB>workload<TAB>bytes_per_launch); missing entries read as null."""
+    kernel<TAB>workload<TAB>bytes_per_launch[<TAB>Krylov iterations per launch of the capture]);
+    missing entries read as null. Returns {(kernel, workload): (bytes, iterations or None)}."""
     out = {}
     p = os.path.join(ROOT, "profiles", "traffic.tsv")
     if os.path.exists(p):
@@ -658,7 +663,7 @@ def load_traffic():
             f = ln.strip().split("\t")
             if len(f) >= 3 and not ln.startswith("#"):
                 try:
-                    out[(f[0], f[1])] = float(f[2])
+                    out[(f[0], f[1])] = (float(f[2]), float(f[3]) if len(f) >= 4 else None)
                 except ValueError:
                     pass
     return out

@@ -139,7 +139,7 @@ typedef struct tf_step_stats {
 /* Fill p with defaults: the reference's Newton cap (20) and threshold (1e-8), Krylov rtol
  * 1e-12 with cap 20000, the two-level preconditioner (TF_PRECOND_TWO_LEVEL), TF_SCATTER_AUTO,
  * device 0, graphs on, persistent solve on, smoother block chosen from the mesh, no refinement,
- * TF_KRYLOV_AUTO. */
+ * TF_KRYLOV_AUTO, warm starts on. */
 void tf_default_params(tf_params* p);
 
 /* Library version string. */
