@@ -156,3 +156,34 @@ def test_wing_disc_shape():
     assert t.n_nodes == 3 * (t.n_nodes // 3)
     assert 7000 < t.n_elems < 9000  # 2 layers of ~3.9k triangles
     assert int(t.fixed.sum()) > 0
+
+
+def test_previous_step_solution_is_a_warm_start():
+    """The premise of the Newton loop's warm-started solves (tf_params.krylov_warm_start): for
+    Newton iteration k of step n, the solution of iteration k of step n - 1 leaves a residual
+    ||g - J du_prev|| well below ||g|| on the first iterations (consecutive steps grow the
+    tissue by similar increments). Oracle systems of a 40 x 20 slab, steps 2-3."""
+    t = mesh.large_slab(nx=40, ny=20)
+    x = np.array(t.x, dtype=np.float64, copy=True)
+    fg = np.array(t.fg, dtype=np.float64, copy=True)
+    rowptr, colidx = O.block_pattern(t)
+    prev, ratios = {}, []
+    for step in range(3):
+        fg, inv, _, _ = O.grow(t, x, fg)
+        vs = O.viscosity_surfaces(t, x)
+        un = x.reshape(-1, 3).copy()
+        uk, cur = un.copy(), {}
+        for k in range(20):
+            vals, g = O.assemble_bsr(t, uk, un, vs, inv, rowptr, colidx)
+            J = O.bsr_to_scipy(rowptr, colidx, vals, t.n_nodes)
+            du = O.sparse_direct_solve(J, g)
+            cur[k] = du
+            if k in prev and k < 3:
+                ratios.append(np.linalg.norm(g - J @ prev[k]) / np.linalg.norm(g))
+            uk = uk + du.reshape(-1, 3)
+            if np.linalg.norm(du) <= t.newton_tol:
+                break
+        prev = cur
+        x = uk.reshape(x.shape)
+    assert len(ratios) >= 4
+    assert max(ratios) < 0.7, ratios
