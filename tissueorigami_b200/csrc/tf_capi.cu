@@ -1708,8 +1708,8 @@ int krylov_solve(tf_ctx* ctx) {
         // conjugate gradients start from the solution of the same Newton iteration of the last
         // step that reached it, with its true residual r0 = g - J x0 (the kernel falls back to
         // x0 = 0 when ||r0|| is not below ||g||). Consecutive steps grow the tissue by similar
-        // increments, so ||r0|| is typically a tenth of ||g||. Not for the lumen's second solve
-        // (another right-hand side) or MINRES.
+        // increments, so ||r0|| is 0.06-0.5 of ||g|| on the first three Newton iterations of a
+        // slab. Not for the lumen's second solve (another right-hand side) or MINRES.
         const size_t bytes3 = sizeof(double) * 3 * (size_t)ctx->N;
         const int wk = ctx->warm_k;
         const bool warm_slot = ctx->params.krylov_warm_start && ctx->T == 1 && plan.cg && !plan.minres &&
