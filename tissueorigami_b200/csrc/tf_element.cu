@@ -678,13 +678,18 @@ constexpr size_t element_smem_bytes() {
 
 template <int TEAMS, bool VISC, int MODE>
 cudaError_t launch_t(const AssembleArgs& a, cudaStream_t s) {
-    static bool attr_set = false;
+    // the shared-memory opt-in is a per-device attribute of the kernel: set once per device
+    constexpr int kDevices = 64;
+    static bool attr_set[kDevices] = {};
     constexpr size_t smem = element_smem_bytes<TEAMS, VISC, MODE>();
-    if (!attr_set) {
+    int dev = 0;
+    cudaError_t derr = cudaGetDevice(&dev);
+    if (derr != cudaSuccess) return derr;
+    if (dev < 0 || dev >= kDevices || !attr_set[dev]) {
         cudaError_t err = cudaFuncSetAttribute(k_element_assemble<TEAMS, VISC, MODE>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
-        attr_set = true;
+        if (dev >= 0 && dev < kDevices) attr_set[dev] = true;
     }
     if (a.e_count <= 0) return cudaSuccess;
     const int grid = (a.e_count + TEAMS - 1) / TEAMS;
